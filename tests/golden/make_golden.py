@@ -1,0 +1,322 @@
+"""Generate the golden fixtures under tests/golden/.
+
+The reference (Fortran on PSBLAS/MLD2P4) cannot be built in this
+environment and ships no golden vectors, so these fixtures come from an
+independent pure-Python restatement of the reference algorithm, written
+separately from the C oracle and following the Fortran line by line:
+
+  - maxval scaling and d = weight/p   src/impl/mld_d_ainv_bld.F90:115-184
+  - left-looking biconjugation        src/impl/mld_dsparse_biconjg_llk.F90:35-366
+  - SYM-LLK (W = Z)                   src/impl/mld_dsparse_biconjg_s_llk.F90:246
+  - LLK without the alpha test        src/impl/mld_dsparse_biconjg_llk_noth.F90
+  - sparsify (diag + nzrmax-1 largest, PSBLAS magnitude-heap tie order)
+                                      src/impl/mld_d_sparsify.f90:35-149
+  - Z CSC->CSR, W CSC->transpose      src/mld_d_biconjg_mod.F90:131-135
+  - apply 'N' / 'T'                   src/impl/mld_d_base_ainv_solver_apply_vect.f90:112-127
+
+Cases are tiny (pure-Python loops).  Run:  python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import heapq
+import math
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+EPSTOL = 1.1e-16
+
+
+# ---------------------------------------------------------------- inputs --
+def pde3d(idim, kind, beta):
+    """7-point operator, x fastest; kind 'poisson' (6/-1) or 'convdiff'."""
+    m = idim
+    h = 1.0 / (idim + 1)
+    ih2 = 1.0 / (h * h)
+    if kind == "poisson":
+        lo = [-1.0] * 3
+        up = [-1.0] * 3
+        diag = 6.0
+    else:
+        lo, up = [0.0] * 3, [0.0] * 3
+        diag = 6.0 * ih2
+        for a in range(3):
+            lo[a] = -ih2 - (beta[a] if beta[a] > 0 else 0.0) / h
+            up[a] = -ih2 + (beta[a] if beta[a] < 0 else 0.0) / h
+            diag += abs(beta[a]) / h
+    rows = []
+    for iz in range(m):
+        for iy in range(m):
+            for ix in range(m):
+                r = ix + m * (iy + m * iz)
+                e = []
+                if iz > 0: e.append((r - m * m, lo[2]))
+                if iy > 0: e.append((r - m, lo[1]))
+                if ix > 0: e.append((r - 1, lo[0]))
+                e.append((r, diag))
+                if ix < m - 1: e.append((r + 1, up[0]))
+                if iy < m - 1: e.append((r + m, up[1]))
+                if iz < m - 1: e.append((r + m * m, up[2]))
+                rows.append(e)
+    return rows
+
+
+def rows_to_csr(rows):
+    irp = [0]
+    ja, va = [], []
+    for e in rows:
+        for c, v in e:
+            ja.append(c)
+            va.append(v)
+        irp.append(len(ja))
+    return (np.array(irp, np.int32), np.array(ja, np.int32), np.array(va, np.float64))
+
+
+# ------------------------------------------------ PSBLAS magnitude heap --
+class MagHeapDown:
+    """psb_d_idx_heap with dir=psb_asort_down_ (1-based binary heap)."""
+
+    def __init__(self):
+        self.k = [None]
+        self.i = [None]
+
+    def insert(self, key, idx):
+        self.k.append(key)
+        self.i.append(idx)
+        c = len(self.k) - 1
+        while c > 1:
+            p = c // 2
+            if abs(self.k[c]) <= abs(self.k[p]):
+                break
+            self.k[c], self.k[p] = self.k[p], self.k[c]
+            self.i[c], self.i[p] = self.i[p], self.i[c]
+            c = p
+
+    def get_first(self):
+        last = len(self.k) - 1
+        if last <= 0:
+            return None
+        key, idx = self.k[1], self.i[1]
+        self.k[1], self.i[1] = self.k[last], self.i[last]
+        self.k.pop()
+        self.i.pop()
+        last -= 1
+        c = 1
+        while c <= last // 2:
+            if 2 * c == last or abs(self.k[2 * c]) > abs(self.k[2 * c + 1]):
+                j = 2 * c
+            else:
+                j = 2 * c + 1
+            if abs(self.k[c]) < abs(self.k[j]):
+                self.k[c], self.k[j] = self.k[j], self.k[c]
+                self.i[c], self.i[j] = self.i[j], self.i[c]
+                c = j
+            else:
+                break
+        return key, idx
+
+
+def sparsify(idiag, nzrmax, thresh, zw, nzset):
+    xw = [0.0]
+    xwid = [idiag]
+    h = MagHeapDown()
+    for i in sorted(nzset):
+        if i == idiag:
+            xw[0] = zw[i]
+        elif abs(zw[i]) >= thresh:
+            h.insert(zw[i], i)
+        zw[i] = 0.0
+    k = 1
+    while k != nzrmax:
+        got = h.get_first()
+        if got is None:
+            break
+        xw.append(got[0])
+        xwid.append(got[1])
+        k += 1
+    order = sorted(range(len(xwid)), key=lambda t: xwid[t])
+    return [xwid[t] for t in order], [xw[t] for t in order]
+
+
+# --------------------------------------------------------- biconjugation --
+def biconjg_half(n, dot_rows, cand_rows, nzrmax, thresh, piv0, noth):
+    """dot_rows[j]: list of (k, a) giving the dot vector j; cand_rows[kr]:
+    indices j whose dot vector touches position kr; the starting candidates
+    for column i are cand_rows[i] filtered to j < i."""
+    piv = [0.0] * n
+    piv[0] = piv0
+    cols = [([0], [1.0])]
+    zw = [0.0] * n
+    for i in range(1, n):
+        zw[i] = 1.0
+        nzset = {i}
+        rh = []
+        flagged = set()
+        for j in cand_rows[i]:
+            if j < i:
+                heapq.heappush(rh, j)
+                flagged.add(j)
+        lastj = -1
+        while True:
+            j = None
+            while rh:
+                c = heapq.heappop(rh)
+                if c > lastj:
+                    lastj = c
+                    j = c
+                    break
+            if j is None:
+                break
+            flagged.discard(j)
+            if j >= i:
+                continue
+            s = 0.0
+            for k, a in dot_rows[j]:
+                s = s + zw[k] * a
+            alpha = -s / piv[j]
+            if noth or abs(alpha) > thresh:
+                ci, cv = cols[j]
+                for kr, v in zip(ci, cv):
+                    zw[kr] = zw[kr] + alpha * v
+                    if kr not in nzset:
+                        nzset.add(kr)
+                        for nj in cand_rows[kr]:
+                            if nj not in flagged and j < nj < i:
+                                heapq.heappush(rh, nj)
+                                flagged.add(nj)
+        s = 0.0
+        for k, a in dot_rows[i]:
+            s = s + zw[k] * a
+        if abs(s) < EPSTOL:
+            s = 1.0e-3
+        piv[i] = s
+        cols.append(sparsify(i, nzrmax, thresh, zw, nzset))
+    return piv, cols
+
+
+def ainv_build(rows, alg, nzrmax, thresh):
+    n = len(rows)
+    mx = max(abs(v) for e in rows for _, v in e)
+    w = 1.0 / mx
+    srows = [[(c, v * w) for c, v in e if 0 <= c < n] for e in rows]
+    scols = [[] for _ in range(n)]
+    for r, e in enumerate(srows):
+        for c, v in e:
+            scols[c].append((r, v))
+    a11 = 0.0
+    for c, v in srows[0]:
+        if c == 0:
+            a11 = v
+            break
+    if abs(a11) < EPSTOL:
+        a11 = 1.0e-3
+    col_idx = [[r for r, _ in e] for e in scols]
+    row_idx = [[c for c, _ in e] for e in srows]
+    noth = alg == "LLK-NOTH"
+    p, zcols = biconjg_half(n, srows, col_idx, nzrmax, thresh, a11, noth)
+    if alg == "SYM-LLK":
+        wcols = zcols
+    else:
+        _, wcols = biconjg_half(n, scols, row_idx, nzrmax, thresh, a11, noth)
+    d = np.array([(1.0 if abs(v) < EPSTOL else 1.0 / v) * w for v in p])
+    # Wt CSR: row i = column w_i
+    wt = rows_to_csr([list(zip(ci, cv)) for ci, cv in wcols])
+    # Z CSR: transpose of the CSC columns
+    zrows = [[] for _ in range(n)]
+    for c, (ci, cv) in enumerate(zcols):
+        for r, v in zip(ci, cv):
+            zrows[r].append((c, v))
+    z = rows_to_csr(zrows)
+    return wt, z, d
+
+
+def csr_mv(csr, x, trans="N"):
+    irp, ja, va = csr
+    n = len(irp) - 1
+    y = [0.0] * n
+    if trans == "N":
+        for i in range(n):
+            s = 0.0
+            for k in range(irp[i], irp[i + 1]):
+                s = s + va[k] * x[ja[k]]
+            y[i] = s
+    else:
+        for r in range(n):
+            for k in range(irp[r], irp[r + 1]):
+                y[ja[k]] = y[ja[k]] + va[k] * x[r]
+    return y
+
+
+def apply(wt, z, d, x, trans, alpha, beta, y0):
+    if trans == "N":
+        t = csr_mv(wt, x)
+        t = [d[i] * t[i] for i in range(len(t))]
+        u = csr_mv(z, t)
+    else:
+        t = csr_mv(z, x, "T")
+        t = [d[i] * t[i] for i in range(len(t))]
+        u = csr_mv(wt, t, "T")
+    return np.array([alpha * u[i] + beta * y0[i] for i in range(len(u))])
+
+
+def splitmix_uniform(seed, n, lo=-1.0, hi=1.0):
+    M = (1 << 64) - 1
+    out = np.empty(n)
+    for i in range(n):
+        x = ((seed << 40) + i) & M
+        x = (x + 0x9E3779B97F4A7C15) & M
+        x = ((x ^ (x >> 30)) * 0xBF58476D1CE4E5B9) & M
+        x = ((x ^ (x >> 27)) * 0x94D049BB133111EB) & M
+        x = x ^ (x >> 31)
+        out[i] = lo + (hi - lo) * ((x >> 11) * (1.0 / 9007199254740992.0))
+    return out
+
+
+# ---------------------------------------------------------------- cases --
+CASES = [
+    # name, grid, kind, beta, alg, fill_in, thresh
+    ("poisson5_llk", 5, "poisson", (0, 0, 0), "LLK", 20, 0.1),
+    ("poisson5_cap3", 5, "poisson", (0, 0, 0), "LLK", 3, 0.01),
+    ("poisson4_exact", 4, "poisson", (0, 0, 0), "LLK", 64, 0.0),
+    ("convdiff6_llk", 6, "convdiff", (40.0, -25.0, 10.0), "LLK", 20, 0.1),
+    ("convdiff6_cap4", 6, "convdiff", (40.0, -25.0, 10.0), "LLK", 4, 0.02),
+    ("convdiff5_noth", 5, "convdiff", (30.0, 30.0, 30.0), "LLK-NOTH", 6, 0.05),
+    ("convdiff5_sym", 5, "convdiff", (5.0, 5.0, 5.0), "SYM-LLK", 8, 0.05),
+]
+
+HAND_4x4 = [  # small nonsymmetric case worked by hand in the test
+    [(0, 4.0), (1, -1.0), (3, -0.5)],
+    [(0, -2.0), (1, 5.0), (2, -1.0)],
+    [(1, -1.0), (2, 6.0), (3, -2.0)],
+    [(0, -1.0), (2, -3.0), (3, 7.0)],
+]
+
+
+def main():
+    cases = [(c[0], pde3d(c[1], c[2], c[3]), c) for c in CASES]
+    cases.append(("hand4", HAND_4x4, ("hand4", 0, "hand", (0, 0, 0), "LLK", 4, 0.0)))
+    for name, rows, c in cases:
+        alg, fill, thr = c[4], c[5], c[6]
+        a = rows_to_csr(rows)
+        wt, z, d = ainv_build(rows, alg, fill, thr)
+        n = len(rows)
+        x = splitmix_uniform(7, n)
+        y0 = splitmix_uniform(8, n)
+        yN = apply(wt, z, d, x, "N", 1.5, 0.5, y0)
+        yT = apply(wt, z, d, x, "T", -0.75, 2.0, y0)
+        np.savez_compressed(
+            os.path.join(HERE, f"{name}.npz"),
+            a_irp=a[0], a_ja=a[1], a_val=a[2],
+            wt_irp=wt[0], wt_ja=wt[1], wt_val=wt[2],
+            z_irp=z[0], z_ja=z[1], z_val=z[2], d=d,
+            x=x, y0=y0, yN=yN, yT=yT,
+            meta=np.array([c[1], {"poisson": 0, "convdiff": 1, "hand": 2}[c[2]],
+                           fill], np.int64),
+            beta=np.array(c[3], np.float64), thresh=np.array(thr),
+            alg=np.array(alg), kind=np.array(c[2]))
+        print(f"{name}: n={n} nnzA={len(a[1])} nnzWt={len(wt[1])} nnzZ={len(z[1])}")
+
+
+if __name__ == "__main__":
+    main()
