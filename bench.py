@@ -1,0 +1,425 @@
+#!/usr/bin/env python
+"""Benchmark: AINV preconditioner apply GB/s on one B200 (or N replicas).
+
+Workload (one step = one apply y = Z * D^-1 * W^T * x, trans 'N', FP64):
+3-D convection-diffusion -Lap(u) + b.grad(u), 200^3 unit-cube grid
+(n = 8,000,000, nnz(A) = 55,760,000), central diffusion, first-order upwind
+convection, b = 10*(1,1,1)/sqrt(3); AINV factors from the left-looking
+biconjugation with drop tolerance 0.1 and fill cap 20 per column.  Synthetic
+input x ~ U(-1,1) (splitmix64, seed 0).  L2 (126 MB) is flushed between
+timed steps by writing a 256 MB buffer outside the timed events.
+
+value = algorithmic bytes of one apply (nnz_wt*12 + nnz_z*12 + 2*(n+1)*4
++ n*8 [x] + n*8 [D^-1] + 2*n*8 [t write+read] + n*8 [y]) / device time.
+e2e   = the same bytes / time of the host-array entry point
+        (ainv_gpu_apply_host: H2D of x, apply, D2H of y; pinned buffers).
+
+--impl reference times the CPU restatement of the reference apply (the
+oracle; the Fortran reference cannot be built here) on the host cores.
+Multi-GPU: independent replicas, one per rank ("replicas only"), no
+data-path collective; value = sum of bytes over ranks / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "mld-ainv_b200"))
+
+IDIM = 200
+BETA = (10 / np.sqrt(3),) * 3
+FILL, THRESH = 20, 0.1
+WORKLOAD = "convdiff3d_200_upwind_ainv_llk_drop0.1_fill20_apply_N"
+METRIC = "AINV apply GB/s (% HBM peak)"
+
+
+def apply_bytes(n, nnz_wt, nnz_z, vsize=8, isize=4, tsize=8, beta_nonzero=False):
+    """Algorithmic bytes of one 'N' apply (unfused minimum)."""
+    b = nnz_wt * (vsize + isize) + nnz_z * (vsize + isize) + 2 * (n + 1) * 4
+    b += n * 8 + n * vsize + 2 * n * tsize + n * 8
+    if beta_nonzero:
+        b += n * 8
+    return b
+
+
+def stage_bytes(n, nnz, vsize=8, isize=4, tsize=8):
+    """Per-sweep split of apply_bytes: sweep 1 (W^T, reads x and D^-1, writes t),
+    sweep 2 (Z, reads t, writes y)."""
+    s1 = nnz[0] * (vsize + isize) + (n + 1) * 4 + n * 8 + n * vsize + n * tsize
+    s2 = nnz[1] * (vsize + isize) + (n + 1) * 4 + n * tsize + n * 8
+    return s1, s2
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def recorded_traffic(kernel: str):
+    """DRAM bytes per launch from a committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_convdiff3d_200.txt")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """NVML sampling of SM clock and throttle reasons while the timed loop runs."""
+
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown",
+               0x4: "sw_power_cap", 0x80: "hw_power_brake_slowdown", 0x1: "gpu_idle"}
+
+    def __init__(self, index: int, period_s: float = 0.005):
+        self.index, self.period = index, period_s
+        self.samples, self.reasons = [], set()
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._t = None
+        self.ok = False
+
+    def __enter__(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+            self._nv, self._h = pynvml, h
+            self.ok = True
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        except Exception:
+            self.ok = False
+        return self
+
+    def _run(self):
+        nv, h = self._nv, self._h
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                for bit, name in self.REASONS.items():
+                    if r & bit and name != "gpu_idle":
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(self.period)
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._t:
+            self._t.join()
+
+    def summary(self):
+        if not self.ok or not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"]}
+        return {"sm_mhz": float(statistics.median(self.samples)), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+def build_workload(idim=IDIM):
+    import ainv
+    irp, ja, val = ainv.pde.gen_pde3d(idim, "convdiff", BETA)
+    sv = ainv.mld_d_ainv_solver_type()
+    sv.csetc("AINV_ALG", "LLK")
+    sv.cseti("SUB_FILLIN", FILL)
+    sv.csetr("SUB_ILUTHRS", THRESH)
+    sv.check()
+    info = sv.build(irp, ja, val)
+    if info != 0:
+        raise RuntimeError(f"factor build failed: {ainv.last_error()}")
+    return (irp, ja, val), sv
+
+
+def cpu_baseline_apply(f, n, budget_s=10.0, max_reps=200):
+    """Oracle apply ('N') on all host cores for a bounded sample."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    of = O.Factors(O.CSR(n, f["wt_irp"], f["wt_ja"], f["wt_val"]),
+                   O.CSR(n, f["z_irp"], f["z_ja"], f["z_val"]), f["d"])
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    x = np.ascontiguousarray(np.random.default_rng(0).uniform(-1, 1, n))
+    O.ainv_apply(of, x)  # warm
+    t0, reps = time.perf_counter(), 0
+    while reps < max_reps and time.perf_counter() - t0 < budget_s:
+        O.ainv_apply(of, x)
+        reps += 1
+    dt = (time.perf_counter() - t0) / reps
+    return dt, reps, O.get_threads()
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    import ainv
+    irp, ja, val = ainv.pde.gen_pde3d(IDIM, "convdiff", BETA)
+    n = len(irp) - 1
+    of = O.ainv_build(O.CSR(n, irp, ja, val), "LLK", FILL, THRESH)
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    x = O.rand_uniform(0, n)
+    for _ in range(max(args.warmup, 1)):
+        O.ainv_apply(of, x)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        O.ainv_apply(of, x)
+        times.append(time.perf_counter() - t0)
+    ms = 1e3 * sum(times) / len(times)
+    B = apply_bytes(n, of.wt.nnz, of.z.nnz)
+    gbs = B / (ms * 1e-3) / 1e9
+    out = {"impl": "reference", "metric": METRIC, "value": round(gbs, 3), "unit": "GB/s",
+           "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": WORKLOAD, "n": n, "nnz_A": int(len(ja)),
+                      "nnz_wt": of.wt.nnz, "nnz_z": of.z.nnz, "bytes_per_apply": B},
+           "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": O.get_threads(),
+                            "kind": "port",
+                            "sample": f"{args.steps} full 200^3 applies, CPU restatement of "
+                                      "the reference apply (OpenMP over rows); the Fortran "
+                                      "reference cannot be built here"},
+           "e2e": {"value": round(gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-extras", action="store_true", help="skip solves/s and mixed legs")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--idim", type=int, default=IDIM,
+                    help="grid side (default 200; smaller sizes for profiler captures)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+    import ainv
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def allmax(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    (irp, ja, val), sv = build_workload(args.idim)
+    n = len(irp) - 1
+    f = sv.factors()
+    assert sv.cnv("FP64") == 0, ainv.last_error()
+    df = sv.device
+    nnz = (len(f["wt_ja"]), len(f["z_ja"]))
+    B = apply_bytes(n, *nnz)
+    dev = torch.device("cuda", local)
+    x = torch.from_numpy(ainv.pde.rand_uniform(0, n)).to(dev)
+    y = torch.zeros(n, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream()
+
+    for _ in range(args.warmup):
+        df.apply(x, y, 1.0, 0.0, "N", stream)
+    torch.cuda.synchronize()
+
+    K = args.steps
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(K)]
+    with ClockSampler(local) as clk:
+        barrier()
+        torch.cuda.synchronize()
+        for k in range(K):
+            flush.zero_()
+            ev[k][0].record(stream)
+            df.apply(x, y, 1.0, 0.0, "N", stream)
+            ev[k][1].record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    ms = sum(a.elapsed_time(b) for a, b in ev) / K
+    ms = allmax(ms)
+    value = B * world / (ms * 1e-3) / 1e9
+
+    # per-sweep timing (roofline of the dominant kernel)
+    K2 = min(K, 100)
+    st = {1: [], 2: []}
+    for stage in (1, 2):
+        for _ in range(K2):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            df.apply_stage(stage, x=x, y=y, alpha=1.0, beta=0.0, trans="N", stream=stream)
+            b.record(stream)
+            st[stage].append((a, b))
+    torch.cuda.synchronize()
+    st_ms = {s: sum(a.elapsed_time(b) for a, b in st[s]) / K2 for s in st}
+    sb = stage_bytes(n, nnz)
+    dom = max((1, 2), key=lambda s: st_ms[s])
+    dom_name = {1: "k_sweep_dscale", 2: "k_sweep_axpby"}[dom]
+    peak, peak_kind = measured_peaks()
+    achieved = sb[dom - 1] / (st_ms[dom] * 1e-3) / 1e9
+    traffic = recorded_traffic(dom_name)
+
+    # end to end through the host-array entry point (pinned buffers)
+    xh = torch.from_numpy(ainv.pde.rand_uniform(0, n)).pin_memory()
+    yh = torch.zeros(n, dtype=torch.float64).pin_memory()
+    import ctypes as C
+    lib = ainv.lib()
+    Ke = min(K, 50)
+    for _ in range(3):
+        lib.ainv_gpu_apply_host(df.handle, b"N", 1.0, C.c_void_p(xh.data_ptr()), 0.0,
+                                C.c_void_p(yh.data_ptr()))
+    torch.cuda.synchronize()
+    barrier()
+    legacy = torch.cuda.default_stream()  # the entry point runs on the legacy stream
+    t_e2e = []
+    for _ in range(Ke):
+        flush.zero_()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(legacy)
+        info = lib.ainv_gpu_apply_host(df.handle, b"N", 1.0, C.c_void_p(xh.data_ptr()), 0.0,
+                                       C.c_void_p(yh.data_ptr()))
+        b.record(legacy)
+        assert info == 0, ainv.last_error()
+        t_e2e.append((a, b))
+    torch.cuda.synchronize()
+    e2e_ms = allmax(sum(a.elapsed_time(b) for a, b in t_e2e) / Ke)
+    e2e = {"value": round(B * world / (e2e_ms * 1e-3) / 1e9, 3), "unit": "GB/s",
+           "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
+           "ms_per_step": round(e2e_ms, 4)}
+
+    extras = {}
+    if not args.no_extras:
+        extras = run_extras(ainv, torch, dev, irp, ja, val, f, sv, flush, stream)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        dt, reps, cores = cpu_baseline_apply(f, n)
+        cpu = {"value": round(B / dt / 1e9, 3), "unit": "GB/s", "cores": cores, "kind": "port",
+               "sample": f"{reps} full 200^3 applies ({dt * 1e3:.1f} ms each) of the CPU "
+                         "restatement of the reference apply, OpenMP over rows"}
+
+    if rank == 0:
+        out = {"metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world,
+               "steps": K, "warmup": args.warmup, "ms_per_step": round(ms, 5),
+               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+               "data": "synthetic",
+               "config": {"workload": WORKLOAD if args.idim == IDIM else
+                          WORKLOAD.replace("_200_", f"_{args.idim}_"), "n": n, "nnz_A": int(len(ja)),
+                          "nnz_wt": nnz[0], "nnz_z": nnz[1], "bytes_per_apply": B,
+                          "layout": "SELL-32", "l2": "flushed between steps (256 MB write)",
+                          "parallelism": f"replicas{world}",
+                          "pct_of_hbm_peak": round(100 * value / world / peak, 2)},
+               "roofline": {"bound": "hbm", "kernel": dom_name,
+                            "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
+                            "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                            "traffic": traffic, "algorithmic_bytes": sb[dom - 1],
+                            "stage_ms": {"k_sweep_dscale": round(st_ms[1], 5),
+                                         "k_sweep_axpby": round(st_ms[2], 5)}},
+               "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
+               "gpu_launches": 2 * K}
+        out.update(extras)
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def run_extras(ainv, torch, dev, irp, ja, val, f, sv, flush, stream):
+    """Mixed-precision apply GB/s and BiCGSTAB solves/s (FP64 vs FP32 factors)."""
+    n = len(irp) - 1
+    nnz = (len(f["wt_ja"]), len(f["z_ja"]))
+    out = {"mixed": {}, "solve": {}}
+    x = torch.from_numpy(ainv.pde.rand_uniform(0, n)).to(dev)
+    y = torch.zeros(n, dtype=torch.float64, device=dev)
+    for prec, vs in [("FP32", 4), ("BF16", 2)]:
+        df = ainv.DeviceFactors((f["wt_irp"], f["wt_ja"], f["wt_val"]),
+                                (f["z_irp"], f["z_ja"], f["z_val"]), f["d"], prec=prec)
+        for _ in range(5):
+            df.apply(x, y, 1.0, 0.0, "N", stream)
+        evs = []
+        for _ in range(50):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            df.apply(x, y, 1.0, 0.0, "N", stream)
+            b.record(stream)
+            evs.append((a, b))
+        torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in evs) / len(evs)
+        Bm = apply_bytes(n, *nnz, vsize=vs, tsize=4)
+        out["mixed"][prec] = {"ms": round(ms, 5), "GB/s": round(Bm / (ms * 1e-3) / 1e9, 2),
+                              "bytes": Bm}
+        df.close()
+    # BiCGSTAB to 1e-9, b = A x*, x* ~ U(-1,1) seed 0
+    A = ainv.DeviceOperator(irp, ja, val)
+    xs = torch.from_numpy(ainv.pde.rand_uniform(0, n)).to(dev)
+    b = torch.zeros(n, dtype=torch.float64, device=dev)
+    A.spmv(xs, b, 1.0, 0.0, stream)
+    bn = float(torch.linalg.vector_norm(b))
+    for prec in ["FP64", "FP32"]:
+        if prec != "FP64":
+            sv.cnv(prec)
+        df = sv.device
+        res = None
+        times = []
+        for rep in range(3):
+            xx = torch.zeros(n, dtype=torch.float64, device=dev)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            res = A.solve(b, xx, df, "BICGSTAB", 1e-9, 2000, stream)
+            times.append(time.perf_counter() - t0)
+        r = torch.empty_like(b)
+        A.spmv(xx, r, 1.0, 0.0, stream)
+        true_rel = float(torch.linalg.vector_norm(b - r)) / bn
+        err_x = float((xx - xs).abs().max())
+        out["solve"][prec] = {"iters": res.iter, "info": res.info, "relres": res.err,
+                              "true_relres": true_rel, "max_err_vs_xstar": err_x,
+                              "s_per_solve": round(min(times), 5),
+                              "solves_per_s": round(1.0 / min(times), 3)}
+    sv.cnv("FP64")
+    A.close()
+    return out
+
+
+if __name__ == "__main__":
+    sys.exit(main())

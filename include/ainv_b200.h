@@ -1,0 +1,182 @@
+/*
+ * ainv_b200 -- B200 (sm_100a) application phase of the MLD2P4 AINV plugin.
+ *
+ * C-ABI boundary.  Plain pointers and sizes only; no exceptions cross it.
+ * Every entry point returns 0 (AINV_SUCCESS, the reference's psb_success_)
+ * or a nonzero status; ainv_last_error() gives a message for the calling
+ * thread.  Device pointers are CUDA global-memory addresses on the current
+ * device; `stream` is a cudaStream_t passed as void* (NULL = legacy
+ * default stream).  Host arrays passed to *_create are copied and not
+ * retained.  A handle is not thread-safe; one stream per call.
+ *
+ * Reference interfaces replaced (paths inside sfilippone/mld-ainv):
+ *   ainv_gpu_create      mold conversion of the factors:
+ *                        src/impl/mld_d_ainv_solver_bld.f90:71-82 and
+ *                        src/impl/mld_d_base_ainv_solver_cnv.f90:56-60
+ *   ainv_gpu_apply       mld_d_base_ainv_solver_apply_vect
+ *                        src/impl/mld_d_base_ainv_solver_apply_vect.f90:35-166
+ *   ainv_gpu_apply_host  mld_d_base_ainv_solver_apply (array form)
+ *                        src/impl/mld_d_base_ainv_solver_apply.f90:35-152
+ *   ainv_gpu_destroy     mld_d_base_ainv_solver_free / clear_data
+ *                        src/impl/mld_d_base_ainv_solver_free.f90:35-60,
+ *                        src/impl/mld_d_base_ainv_solver_clear_data.f90:35-70
+ *   ainv_gpu_sizeof      d_base_ainv_solver_sizeof src/mld_d_base_ainv_mod.F90:194-207
+ *   ainv_gpu_get_nzeros  d_base_ainv_get_nzeros    src/mld_d_base_ainv_mod.F90:179-192
+ *   ainv_csr_* / ainv_gpu_solve
+ *                        psb_spmm(A) and psb_krylov('CG'|'BICGSTAB', ..., istop=2)
+ *                        as called at tests/pdegen/ppde3d.f90:280-281 (PSBLAS)
+ *   mld_d_solver_*       the solver types mld_d_ainv_solver_type
+ *                        (src/mld_d_ainv_solver.F90:46-67), mld_d_invk_solver_type
+ *                        (src/mld_d_invk_solver.f90:47-57), mld_d_invt_solver_type
+ *                        (src/mld_d_invt_solver.f90:46-58) with their
+ *                        build / cseti / csetr / csetc / check / default / descr /
+ *                        clone / clone_settings / free / sizeof / get_nzeros /
+ *                        get_wrksz / dump procedures.
+ */
+#ifndef AINV_B200_H
+#define AINV_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes --------------------------------------------------- */
+#define AINV_SUCCESS          0    /* psb_success_                        */
+#define AINV_ERR_ARG          30   /* invalid argument (bad trans, sizes)  */
+#define AINV_ERR_ALLOC        4025 /* allocation request refused            */
+#define AINV_ERR_INTERNAL     4000 /* internal error / inconsistent state   */
+#define AINV_ERR_CUDA         4100 /* a CUDA runtime call failed            */
+#define AINV_ERR_NOT_BUILT    4101 /* solver has no factors yet             */
+#define AINV_ERR_BREAKDOWN    4102 /* Krylov breakdown (rho, sigma or omega = 0) */
+#define AINV_ERR_NONFINITE    4103 /* non-finite residual in the Krylov loop */
+#define AINV_ERR_NOCONV       4104 /* itmax reached before the tolerance    */
+#define AINV_ERR_UNSUPPORTED  4105 /* option not built into this library   */
+
+/* ---- factor storage precision (values of W^T, Z and D^-1) ------------- */
+#define AINV_PREC_FP64 0
+#define AINV_PREC_FP32 1
+#define AINV_PREC_BF16 2
+
+/* ---- Krylov methods --------------------------------------------------- */
+#define AINV_KRYLOV_CG       0
+#define AINV_KRYLOV_BICGSTAB 1
+
+/* ---- AINV_ALG values (cseti), in the order of src/mld_base_ainv_mod.F90:50-55;
+ * csetc accepts 'LLK', 'SYM-LLK', 'STAB-LLK', 'MLK'. ------------------------ */
+#define MLD_AINV_LLK       0
+#define MLD_AINV_S_LLK     1
+#define MLD_AINV_S_FT_LLK  2
+#define MLD_AINV_LLK_NOTH  3
+#define MLD_AINV_MLK       4
+
+typedef struct ainv_handle ainv_handle; /* device factors W^T, Z, D^-1    */
+typedef struct ainv_csr ainv_csr;       /* device sparse operator A        */
+typedef struct mld_d_solver mld_d_solver; /* host solver type (AINV/INVK/INVT) */
+
+const char *ainv_last_error(void);
+/* Library version string. */
+const char *ainv_version(void);
+
+/* ---- device factors: upload / apply / release ------------------------ */
+/* Upload W^T (CSR, lower, row i = column w_i), Z (CSR, upper) and
+ * dinv = D^-1 into the device layout, stored in precision `prec`.
+ * one_based != 0 accepts Fortran 1-based irp/ja. */
+int ainv_gpu_create(ainv_handle **h, int n,
+                    const int *wt_irp, const int *wt_ja, const double *wt_val,
+                    const int *z_irp, const int *z_ja, const double *z_val,
+                    const double *dinv, int prec, int one_based);
+/* y = alpha * Z * D^-1 * W^T * x + beta * y   (trans 'N')
+ * y = alpha * W * D^-1 * Z^T * x + beta * y   (trans 'T' or 'C')
+ * x_dev, y_dev: n doubles on the device.  beta == 0 ignores y's contents. */
+int ainv_gpu_apply(ainv_handle *h, char trans, double alpha, const double *x_dev,
+                   double beta, double *y_dev, void *stream);
+/* One sweep of the apply, for overlapping the two sweeps with other work
+ * or timing them apart: stage 1 computes the handle's intermediate
+ * t = D^-1 * (W^T x) ('N') or D^-1 * (Z^T x) ('T'); stage 2 computes
+ * y = alpha * Z t + beta * y ('N') or alpha * W t + beta * y ('T') from the
+ * t left by the last stage 1 on this handle (x is ignored in stage 2). */
+int ainv_gpu_apply_stage(ainv_handle *h, char trans, int stage, double alpha,
+                         const double *x_dev, double beta, double *y_dev, void *stream);
+/* Same on host arrays: copies x in and y out (pinned staging owned by h). */
+int ainv_gpu_apply_host(ainv_handle *h, char trans, double alpha, const double *x,
+                        double beta, double *y);
+int ainv_gpu_destroy(ainv_handle *h);
+size_t ainv_gpu_sizeof(const ainv_handle *h);
+long long ainv_gpu_get_nzeros(const ainv_handle *h);
+int ainv_gpu_get_n(const ainv_handle *h);
+int ainv_gpu_get_prec(const ainv_handle *h);
+/* Nonzeros and device bytes of the apply's two sweeps for trans 'N'
+ * (W^T then Z): nnz_wt, nnz_z, stored (padded) slots of each. */
+int ainv_gpu_layout_info(const ainv_handle *h, long long *nnz_wt, long long *nnz_z,
+                         long long *slots_wt, long long *slots_z);
+
+/* ---- operator A and the Krylov loop ---------------------------------- */
+int ainv_csr_create(ainv_csr **a, int n, const int *irp, const int *ja,
+                    const double *val, int one_based);
+/* y = alpha * A * x + beta * y on device vectors. */
+int ainv_csr_spmv(const ainv_csr *a, double alpha, const double *x_dev, double beta,
+                  double *y_dev, void *stream);
+int ainv_csr_destroy(ainv_csr *a);
+/* Preconditioned CG / BiCGSTAB with istop=2 (||r||_2 <= eps*||b||_2).
+ * x_dev holds x0 on entry and the solution on exit; h may be NULL (no
+ * preconditioner).  Returns AINV_SUCCESS on convergence, AINV_ERR_NOCONV
+ * at itmax, AINV_ERR_BREAKDOWN / AINV_ERR_NONFINITE on breakdown; *iter and
+ * *err (relative residual) are set in every case. */
+int ainv_gpu_solve(ainv_handle *h, const ainv_csr *a, const double *b_dev,
+                   double *x_dev, int method, double eps, int itmax, int *iter,
+                   double *err, void *stream);
+
+/* ---- host solver types (mirror of the Fortran plugin types) ----------- */
+/* type: "AINV", "INVK" or "INVT".  default() is applied on creation. */
+int mld_d_solver_create(mld_d_solver **sv, const char *type);
+int mld_d_solver_destroy(mld_d_solver *sv);
+int mld_d_solver_default(mld_d_solver *sv);
+/* String-keyed setters; keys as in the reference: SUB_FILLIN, AINV_ALG,
+ * SUB_ILUTHRS, INV_FILLIN, INV_THRESH.  Unknown keys are ignored with
+ * success, as the base-solver fallthrough does. */
+int mld_d_solver_cseti(mld_d_solver *sv, const char *what, int val);
+int mld_d_solver_csetr(mld_d_solver *sv, const char *what, double val);
+int mld_d_solver_csetc(mld_d_solver *sv, const char *what, const char *val);
+/* Validate the parameters like mld_check_def: an illegal value is reset to
+ * its default with a warning on stderr (fill_in >= 1 for AINV, levels >= 0
+ * for INVK/INVT, thresholds >= 0); returns AINV_SUCCESS. */
+int mld_d_solver_check(mld_d_solver *sv);
+/* Host factor construction from A (n x n CSR; entries outside the local
+ * n x n block are clipped).  When a device precision has been set with
+ * mld_d_solver_cnv, the factors are uploaded at the end of build, as the
+ * reference converts them when amold/vmold are present. */
+int mld_d_solver_build(mld_d_solver *sv, int n, const int *irp, const int *ja,
+                       const double *val, int one_based);
+/* Convert (upload) the built factors to the device in precision prec. */
+int mld_d_solver_cnv(mld_d_solver *sv, int prec);
+int mld_d_solver_apply(mld_d_solver *sv, double alpha, const double *x_dev,
+                       double beta, double *y_dev, char trans, void *stream);
+/* Host-array form of the apply (apply_a). */
+int mld_d_solver_apply_host(mld_d_solver *sv, double alpha, const double *x,
+                            double beta, double *y, char trans);
+/* Device handle owned by sv (NULL before cnv). */
+ainv_handle *mld_d_solver_handle(mld_d_solver *sv);
+/* Copy the host factors out.  Call with NULL arrays to get the sizes. */
+int mld_d_solver_get_factors(const mld_d_solver *sv, int *n, long long *nnz_wt,
+                             long long *nnz_z, int *wt_irp, int *wt_ja,
+                             double *wt_val, int *z_irp, int *z_ja, double *z_val,
+                             double *d);
+int mld_d_solver_clone(const mld_d_solver *sv, mld_d_solver **out);
+int mld_d_solver_clone_settings(const mld_d_solver *sv, mld_d_solver *out);
+int mld_d_solver_free(mld_d_solver *sv);       /* drop host and device data */
+size_t mld_d_solver_sizeof(const mld_d_solver *sv);
+long long mld_d_solver_get_nzeros(const mld_d_solver *sv);
+int mld_d_solver_get_wrksz(void);              /* 2, like get_wrksz */
+/* Human-readable description into buf (always NUL-terminated). */
+int mld_d_solver_descr(const mld_d_solver *sv, char *buf, size_t len);
+/* MatrixMarket dump of W^T, D^-1 and Z as <prefix>_wmat.mtx,
+ * <prefix>_diag.mtx, <prefix>_zmat.mtx. */
+int mld_d_solver_dump(const mld_d_solver *sv, const char *prefix);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AINV_B200_H */

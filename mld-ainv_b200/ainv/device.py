@@ -1,0 +1,157 @@
+"""Device objects: the converted factors (W^T, Z, D^-1) and the operator A.
+
+Vectors passed to the device entry points are CUDA tensors (torch is used
+only as the owner of device memory and streams); host entry points take
+numpy arrays.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import KRYLOV, PREC, SUCCESS, check, lib, last_error
+
+
+def _np(a, dtype):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+def dptr(t) -> C.c_void_p:
+    """Device address of a CUDA tensor (float64, contiguous)."""
+    if not t.is_cuda or not t.is_contiguous():
+        raise ValueError("expected a contiguous CUDA tensor")
+    return C.c_void_p(t.data_ptr())
+
+
+def _stream(s):
+    if s is None:
+        return None
+    return C.c_void_p(getattr(s, "cuda_stream", s))
+
+
+class DeviceFactors:
+    """W^T (lower CSR), Z (upper CSR) and D^-1 uploaded to the device layout."""
+
+    def __init__(self, wt, z, d, prec: str = "FP64", one_based: bool = False, *, _borrow=None):
+        self._own = _borrow is None
+        if _borrow is not None:
+            self._h = _borrow
+            return
+        self._keep = [_np(wt[0], np.int32), _np(wt[1], np.int32), _np(wt[2], np.float64),
+                      _np(z[0], np.int32), _np(z[1], np.int32), _np(z[2], np.float64),
+                      _np(d, np.float64)]
+        n = len(self._keep[6])
+        h = C.c_void_p()
+        check(lib().ainv_gpu_create(C.byref(h), n, *[C.c_void_p(a.ctypes.data) for a in self._keep],
+                                    PREC[prec.upper()], 1 if one_based else 0))
+        self._h = h
+        del self._keep
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    @property
+    def n(self) -> int:
+        return lib().ainv_gpu_get_n(self._h)
+
+    @property
+    def prec(self) -> str:
+        p = lib().ainv_gpu_get_prec(self._h)
+        return {v: k for k, v in PREC.items()}[p]
+
+    def apply(self, x, y, alpha=1.0, beta=0.0, trans="N", stream=None) -> None:
+        """y = alpha * Z D^-1 W^T x + beta * y (trans 'N'), device tensors."""
+        check(lib().ainv_gpu_apply(self._h, trans.encode()[:1], alpha, dptr(x), beta, dptr(y),
+                                   _stream(stream)))
+
+    def apply_stage(self, stage, x=None, y=None, alpha=1.0, beta=0.0, trans="N", stream=None):
+        """Run sweep 1 (t = D^-1 W^T x) or sweep 2 (y = alpha Z t + beta y) alone."""
+        check(lib().ainv_gpu_apply_stage(self._h, trans.encode()[:1], int(stage), alpha,
+                                         dptr(x) if x is not None else None, beta,
+                                         dptr(y) if y is not None else None, _stream(stream)))
+
+    def apply_host(self, x, alpha=1.0, beta=0.0, y=None, trans="N") -> np.ndarray:
+        x = _np(x, np.float64)
+        y = np.zeros_like(x) if y is None else _np(y, np.float64).copy()
+        check(lib().ainv_gpu_apply_host(self._h, trans.encode()[:1], alpha,
+                                        C.c_void_p(x.ctypes.data), beta, C.c_void_p(y.ctypes.data)))
+        return y
+
+    def sizeof(self) -> int:
+        return int(lib().ainv_gpu_sizeof(self._h))
+
+    def get_nzeros(self) -> int:
+        return int(lib().ainv_gpu_get_nzeros(self._h))
+
+    def layout_info(self) -> dict:
+        v = [C.c_longlong() for _ in range(4)]
+        check(lib().ainv_gpu_layout_info(self._h, *[C.byref(x) for x in v]))
+        return dict(nnz_wt=v[0].value, nnz_z=v[1].value, slots_wt=v[2].value, slots_z=v[3].value)
+
+    def close(self) -> None:
+        if getattr(self, "_own", False) and self._h:
+            lib().ainv_gpu_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class SolveResult:
+    def __init__(self, info, iters, err):
+        self.info, self.iter, self.err = info, iters, err
+
+    @property
+    def converged(self) -> bool:
+        return self.info == SUCCESS
+
+    def __repr__(self):
+        return f"SolveResult(info={self.info}, iter={self.iter}, err={self.err:.3e})"
+
+
+class DeviceOperator:
+    """Sparse operator A (FP64) on the device, with the Krylov driver."""
+
+    def __init__(self, irp, ja, val, one_based: bool = False):
+        irp, ja, val = _np(irp, np.int32), _np(ja, np.int32), _np(val, np.float64)
+        self.n = len(irp) - 1
+        h = C.c_void_p()
+        check(lib().ainv_csr_create(C.byref(h), self.n, C.c_void_p(irp.ctypes.data),
+                                    C.c_void_p(ja.ctypes.data), C.c_void_p(val.ctypes.data),
+                                    1 if one_based else 0))
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def spmv(self, x, y, alpha=1.0, beta=0.0, stream=None) -> None:
+        check(lib().ainv_csr_spmv(self._h, alpha, dptr(x), beta, dptr(y), _stream(stream)))
+
+    def solve(self, b, x, factors: DeviceFactors | None = None, method="BICGSTAB", eps=1e-9,
+              itmax=1000, stream=None) -> SolveResult:
+        """psb_krylov(method, A, prec, b, x, eps, ..., istop=2) on the device.
+        Returns the status instead of raising for NOCONV / breakdown."""
+        it, err = C.c_int(0), C.c_double(0.0)
+        info = lib().ainv_gpu_solve(factors.handle if factors is not None else None, self._h,
+                                    dptr(b), dptr(x), KRYLOV[method.upper()], eps, itmax,
+                                    C.byref(it), C.byref(err), _stream(stream))
+        if info not in (SUCCESS, 4102, 4103, 4104):
+            check(info)
+        return SolveResult(info, it.value, err.value)
+
+    def close(self) -> None:
+        if self._h:
+            lib().ainv_csr_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

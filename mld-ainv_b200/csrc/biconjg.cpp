@@ -1,0 +1,276 @@
+// Host factor construction for the AINV solver (sparse left-looking
+// biconjugation), producing the Z / W^T patterns the device apply consumes.
+//
+// Algorithm: mld_d_ainv_bld (src/impl/mld_d_ainv_bld.F90:35-194) with the
+// maxval scaling the solver always requests (src/impl/mld_d_ainv_solver_bld.f90:68-69),
+// the left-looking biconjugation of src/impl/mld_dsparse_biconjg_llk.F90:35-366
+// (plus the SYM-LLK and no-alpha-test variants), and the column
+// sparsification of src/impl/mld_d_sparsify.f90:35-149.  Floating-point
+// operations happen in the reference's order with one rounding per
+// operation, so the factors are bit-identical to the reference algorithm.
+//
+// The Z and W halves of the biconjugation only share read-only data (A and
+// its transpose), so they run on two threads.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <queue>
+#include <thread>
+#include <vector>
+
+#include "host_build.h"
+
+namespace ainv {
+namespace {
+
+constexpr double kEpsTol = 1.1e-16;  // PSBLAS d_epstol
+constexpr double kTinyPivot = 1.0e-3;
+
+// Magnitude-ordered heap with the exact pop order of PSBLAS psb_d_idx_heap
+// in psb_asort_down_ mode: 1-based binary heap; an inserted key rises while
+// strictly larger in magnitude than its parent; the root's replacement sinks
+// toward the larger child (left child on ties, or when it is the last
+// element) while strictly smaller than it.  This order decides which
+// equal-magnitude entries survive the fill cap.
+class MagnitudeHeap {
+ public:
+  void clear() {
+    key_.resize(1);
+    idx_.resize(1);
+  }
+  bool empty() const { return key_.size() <= 1; }
+  void push(double k, int i) {
+    key_.push_back(k);
+    idx_.push_back(i);
+    size_t c = key_.size() - 1;
+    while (c > 1) {
+      const size_t p = c / 2;
+      if (std::fabs(key_[c]) <= std::fabs(key_[p])) break;
+      std::swap(key_[c], key_[p]);
+      std::swap(idx_[c], idx_[p]);
+      c = p;
+    }
+  }
+  void pop(double &k, int &i) {
+    k = key_[1];
+    i = idx_[1];
+    key_[1] = key_.back();
+    idx_[1] = idx_.back();
+    key_.pop_back();
+    idx_.pop_back();
+    const size_t last = key_.size() - 1;
+    size_t c = 1;
+    while (c <= last / 2) {
+      const size_t l = 2 * c;
+      const size_t j = (l == last || std::fabs(key_[l]) > std::fabs(key_[l + 1])) ? l : l + 1;
+      if (!(std::fabs(key_[c]) < std::fabs(key_[j]))) break;
+      std::swap(key_[c], key_[j]);
+      std::swap(idx_[c], idx_[j]);
+      c = j;
+    }
+  }
+
+ private:
+  std::vector<double> key_{0.0};
+  std::vector<int> idx_{0};
+};
+
+using MinQueue = std::priority_queue<int, std::vector<int>, std::greater<int>>;
+
+// Column-by-column builder of one unit upper triangular factor (Z, or W).
+// `dots` gives the sparse vector whose dot with the working column yields
+// the biconjugation coefficient for step j (rows of A for Z, columns of A
+// for W); `touch` maps a position kr to the steps j whose dot vector has a
+// nonzero at kr (columns of A for Z, rows of A for W).
+class HalfBuilder {
+ public:
+  HalfBuilder(const HostCsr &dots, const HostCsr &touch, int cap, double thresh,
+              bool alpha_test)
+      : dots_(dots), touch_(touch), n_(dots.n), cap_(cap), thresh_(thresh),
+        alpha_test_(alpha_test) {}
+
+  // piv receives the pivots; out gets the factor as CSC columns.
+  void run(double piv0, std::vector<double> &piv, HostCsr &out) {
+    piv.assign((size_t)n_, 0.0);
+    out.n = n_;
+    out.irp.assign((size_t)n_ + 1, 0);
+    out.ja.clear();
+    out.val.clear();
+    out.ja.reserve((size_t)n_ * 4);
+    out.val.reserve((size_t)n_ * 4);
+    work_.assign((size_t)n_, 0.0);
+    in_col_.assign((size_t)n_, 0);
+    queued_.assign((size_t)n_, 0);
+
+    piv[0] = piv0;
+    out.ja.push_back(0);
+    out.val.push_back(1.0);
+    out.irp[1] = 1;
+
+    for (int i = 1; i < n_; i++) {
+      std::vector<int> nz;  // positions set in work_, in insertion order
+      work_[i] = 1.0;
+      in_col_[i] = 1;
+      nz.push_back(i);
+      MinQueue steps;
+      for (int k = touch_.irp[i]; k < touch_.irp[i + 1]; k++) {
+        const int j = touch_.ja[k];
+        if (j < i) {
+          steps.push(j);
+          queued_[j] = 1;
+        }
+      }
+      int lastj = -1;
+      while (!steps.empty()) {
+        const int j = steps.top();
+        steps.pop();
+        if (j <= lastj) continue;  // repeated entry
+        lastj = j;
+        queued_[j] = 0;
+        if (j >= i) continue;
+        const double alpha = -dot_with(j) / piv[j];
+        if (alpha_test_ && !(std::fabs(alpha) > thresh_)) continue;
+        for (int k = out.irp[j]; k < out.irp[j + 1]; k++) {
+          const int kr = out.ja[k];
+          work_[kr] = work_[kr] + alpha * out.val[k];
+          if (!in_col_[kr]) {
+            in_col_[kr] = 1;
+            nz.push_back(kr);
+            for (int kc = touch_.irp[kr]; kc < touch_.irp[kr + 1]; kc++) {
+              const int nj = touch_.ja[kc];
+              if (!queued_[nj] && nj > j && nj < i) {
+                steps.push(nj);
+                queued_[nj] = 1;
+              }
+            }
+          }
+        }
+      }
+      double p = dot_with(i);
+      if (std::fabs(p) < kEpsTol) p = kTinyPivot;
+      piv[i] = p;
+      keep_column(i, nz, out);
+    }
+  }
+
+ private:
+  double dot_with(int j) const {
+    double s = 0.0;
+    for (int k = dots_.irp[j]; k < dots_.irp[j + 1]; k++) s = s + work_[dots_.ja[k]] * dots_.val[k];
+    return s;
+  }
+
+  // Diagonal plus at most cap-1 entries of largest magnitude >= thresh,
+  // offered to the heap in ascending index order; survivors sorted by index.
+  void keep_column(int i, std::vector<int> &nz, HostCsr &out) {
+    std::sort(nz.begin(), nz.end());
+    heap_.clear();
+    double diag = 0.0;
+    for (int r : nz) {
+      if (r == i)
+        diag = work_[r];
+      else if (std::fabs(work_[r]) >= thresh_)
+        heap_.push(work_[r], r);
+      work_[r] = 0.0;
+      in_col_[r] = 0;
+    }
+    kept_.clear();
+    kept_.push_back({i, diag});
+    while ((int)kept_.size() < cap_ && !heap_.empty()) {
+      double v;
+      int r;
+      heap_.pop(v, r);
+      kept_.push_back({r, v});
+    }
+    std::sort(kept_.begin(), kept_.end(),
+              [](const std::pair<int, double> &a, const std::pair<int, double> &b) {
+                return a.first < b.first;
+              });
+    for (const auto &e : kept_) {
+      out.ja.push_back(e.first);
+      out.val.push_back(e.second);
+    }
+    out.irp[(size_t)i + 1] = (int)out.ja.size();
+  }
+
+  const HostCsr &dots_;
+  const HostCsr &touch_;
+  const int n_, cap_;
+  const double thresh_;
+  const bool alpha_test_;
+  std::vector<double> work_;
+  std::vector<char> in_col_, queued_;
+  MagnitudeHeap heap_;
+  std::vector<std::pair<int, double>> kept_;
+};
+
+}  // namespace
+
+int ainv_biconjg_build(const HostCsr &a_in, int alg, int fill_in, double thresh,
+                       HostCsr &wt, HostCsr &z, std::vector<double> &d) {
+  if (fill_in < 1) {
+    set_error("AINV build: fill_in must be >= 1 (got %d)", fill_in);
+    return AINV_ERR_ARG;
+  }
+  if (alg != kAlgLLK && alg != kAlgSymLLK && alg != kAlgLLKNoth) {
+    set_error("AINV build: Invalid alg %d", alg);
+    return AINV_ERR_ARG;
+  }
+  const int n = a_in.n;
+  // clip to the local n x n block and scale by 1/max|a_ij|
+  HostCsr a;
+  a.n = n;
+  a.irp.assign((size_t)n + 1, 0);
+  for (int r = 0; r < n; r++) {
+    for (int k = a_in.irp[r]; k < a_in.irp[r + 1]; k++)
+      if (a_in.ja[k] >= 0 && a_in.ja[k] < n) {
+        a.ja.push_back(a_in.ja[k]);
+        a.val.push_back(a_in.val[k]);
+      }
+    a.irp[(size_t)r + 1] = (int)a.ja.size();
+  }
+  double mx = 0.0;
+  for (double v : a.val) mx = std::max(mx, std::fabs(v));
+  if (!(mx > 0.0)) {
+    set_error("AINV build: matrix has no nonzero entries");
+    return AINV_ERR_ARG;
+  }
+  const double weight = 1.0 / mx;
+  for (double &v : a.val) v = v * weight;
+  const HostCsr at = transpose(a);
+
+  double a11 = 0.0;
+  for (int k = a.irp[0]; k < a.irp[1]; k++)
+    if (a.ja[k] == 0) {
+      a11 = a.val[k];
+      break;
+    }
+  if (std::fabs(a11) < kEpsTol) a11 = kTinyPivot;
+
+  const bool alpha_test = alg != kAlgLLKNoth;
+  std::vector<double> p, q;
+  HostCsr zc, wc;
+  HalfBuilder zb(a, at, fill_in, thresh, alpha_test);   // dots: rows of A
+  if (alg == kAlgSymLLK) {
+    zb.run(a11, p, zc);
+    wc = zc;  // W = Z (src/impl/mld_dsparse_biconjg_s_llk.F90:246)
+  } else {
+    HalfBuilder wb(at, a, fill_in, thresh, alpha_test);  // dots: columns of A
+    std::thread th([&] { wb.run(a11, q, wc); });
+    zb.run(a11, p, zc);
+    th.join();
+  }
+  // W is held by columns; its CSC arrays are the CSR arrays of W^T
+  // (src/mld_d_biconjg_mod.F90:133-135).  Z goes CSC -> CSR (:131-132).
+  wt = std::move(wc);
+  z = transpose(zc);
+  d.resize((size_t)n);
+  for (int i = 0; i < n; i++) {
+    const double inv = (std::fabs(p[i]) < kEpsTol) ? 1.0 : 1.0 / p[i];
+    d[i] = inv * weight;  // src/impl/mld_d_ainv_bld.F90:161-173
+  }
+  return AINV_SUCCESS;
+}
+
+}  // namespace ainv

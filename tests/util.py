@@ -1,0 +1,32 @@
+"""Shared helpers for the GPU parity tests (oracle = CPU restatement)."""
+import numpy as np
+
+import ainv
+import oracle as O
+
+
+def build_factors(irp, ja, val, fill=20, thresh=0.1, alg="LLK"):
+    """Product host build (mld_d_ainv_solver_type) -> dict of CSR arrays."""
+    sv = ainv.mld_d_ainv_solver_type()
+    sv.csetc("AINV_ALG", alg)
+    sv.cseti("SUB_FILLIN", fill)
+    sv.csetr("SUB_ILUTHRS", thresh)
+    assert sv.build(irp, ja, val) == 0, ainv.last_error()
+    return sv.factors()
+
+
+def oracle_factors(f):
+    n = len(f["d"])
+    return O.Factors(O.CSR(n, f["wt_irp"], f["wt_ja"], f["wt_val"]),
+                     O.CSR(n, f["z_irp"], f["z_ja"], f["z_val"]), f["d"])
+
+
+def device_factors(f, prec="FP64"):
+    return ainv.DeviceFactors((f["wt_irp"], f["wt_ja"], f["wt_val"]),
+                              (f["z_irp"], f["z_ja"], f["z_val"]), f["d"], prec=prec)
+
+
+def relerr(y, ref):
+    """Norm-wise relative error ||y - ref||_inf / ||ref||_inf."""
+    y = np.asarray(y)
+    return float(np.abs(y - ref).max() / max(np.abs(ref).max(), 1e-300))
