@@ -113,6 +113,27 @@ int ainv_gpu_get_prec(const ainv_handle *h);
 int ainv_gpu_layout_info(const ainv_handle *h, long long *nnz_wt, long long *nnz_z,
                          long long *slots_wt, long long *slots_z);
 
+/* No counterpart in the reference.  The 'N' apply for callers that may not
+ * allocate device memory when they apply (a framework that owns all device
+ * memory through its own pool, or a latency-critical section where
+ * cudaMalloc/cudaFree and the synchronisation they can cause are not
+ * allowed).  Every argument is caller-owned device memory: W^T and Z as
+ * 0-based CSR (irp n+1, ja/val nnz), dinv, x and y (n doubles); columns
+ * outside [0, n) are skipped.  Computes y = alpha * Z * D^-1 * W^T * x +
+ * beta * y without allocating: the intermediate vector lives in a built-in
+ * device array of 2^20 doubles (8 MiB, held on each device where the
+ * library's module is loaded until the process exits), so n must be at most
+ * 1,048,576 (larger n returns AINV_ERR_ARG).  The first call on each device
+ * looks up that array's address (cudaGetSymbolAddress); make it before any
+ * stream capture.  All calls share the array: calls that overlap on the GPU
+ * race and must be serialised by the caller. */
+int ainv_gpu_apply_csr_noalloc(int n, const int *wt_irp, const int *wt_ja,
+                               const double *wt_val, long long nnz_wt,
+                               const int *z_irp, const int *z_ja, const double *z_val,
+                               long long nnz_z, const double *dinv, double alpha,
+                               const double *x_dev, double beta, double *y_dev,
+                               void *stream);
+
 /* ---- operator A and the Krylov loop ---------------------------------- */
 int ainv_csr_create(ainv_csr **a, int n, const int *irp, const int *ja,
                     const double *val, int one_based);

@@ -45,6 +45,8 @@ SIGNATURES = [
     ("ainv_gpu_get_n", _i, [_vp]),
     ("ainv_gpu_get_prec", _i, [_vp]),
     ("ainv_gpu_layout_info", _i, [_vp, _llp, _llp, _llp, _llp]),
+    ("ainv_gpu_apply_csr_noalloc", _i, [_i, _vp, _vp, _vp, _ll, _vp, _vp, _vp, _ll, _vp, _d,
+                                        _vp, _d, _vp, _vp]),
     ("ainv_csr_create", _i, [C.POINTER(_vp), _i, _vp, _vp, _vp, _i]),
     ("ainv_csr_spmv", _i, [_vp, _d, _vp, _d, _vp, _vp]),
     ("ainv_csr_destroy", _i, [_vp]),
