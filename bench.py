@@ -42,20 +42,20 @@ WORKLOAD = "convdiff3d_200_upwind_ainv_llk_drop0.1_fill20_apply_N"
 METRIC = "AINV apply GB/s (% HBM peak)"
 
 
-def apply_bytes(n, nnz_wt, nnz_z, vsize=8, isize=4, tsize=8, beta_nonzero=False):
-    """Algorithmic bytes of one 'N' apply (unfused minimum)."""
-    b = nnz_wt * (vsize + isize) + nnz_z * (vsize + isize) + 2 * (n + 1) * 4
-    b += n * 8 + n * vsize + 2 * n * tsize + n * 8
-    if beta_nonzero:
-        b += n * 8
-    return b
+def csr_apply_bytes(n, nnz_wt, nnz_z):
+    """FP64 CSR bytes of one 'N' apply (the reference format, int32 indices)."""
+    return 12 * nnz_wt + 12 * nnz_z + 2 * 4 * (n + 1) + 8 * n + 8 * n + 16 * n + 8 * n
 
 
-def stage_bytes(n, nnz, vsize=8, isize=4, tsize=8):
-    """Per-sweep split of apply_bytes: sweep 1 (W^T, reads x and D^-1, writes t),
-    sweep 2 (Z, reads t, writes y)."""
-    s1 = nnz[0] * (vsize + isize) + (n + 1) * 4 + n * 8 + n * vsize + n * tsize
-    s2 = nnz[1] * (vsize + isize) + (n + 1) * 4 + n * tsize + n * 8
+def layout_bytes(n, lay, vsize, tsize):
+    """Algorithmic bytes of the two 'N' sweeps for the device layout:
+    values (nnz * vsize) + stored index words (column offsets per slice, or
+    per-entry columns) + two slice pointers, plus the vectors each sweep
+    streams.  Returns (sweep1, sweep2)."""
+    def mat(m):
+        return m["nnz"] * vsize + 4 * m["nidx"] + 8 * (m["nslices"] + 1)
+    s1 = mat(lay["wt"]) + 8 * n + vsize * n + tsize * n      # x, D^-1, t write
+    s2 = mat(lay["z"]) + tsize * n + 8 * n                   # t read, y write
     return s1, s2
 
 
@@ -186,7 +186,7 @@ def run_reference(args):
         O.ainv_apply(of, x)
         times.append(time.perf_counter() - t0)
     ms = 1e3 * sum(times) / len(times)
-    B = apply_bytes(n, of.wt.nnz, of.z.nnz)
+    B = csr_apply_bytes(n, of.wt.nnz, of.z.nnz)
     gbs = B / (ms * 1e-3) / 1e9
     out = {"impl": "reference", "metric": METRIC, "value": round(gbs, 3), "unit": "GB/s",
            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -250,7 +250,10 @@ def main():
     assert sv.cnv("FP64") == 0, ainv.last_error()
     df = sv.device
     nnz = (len(f["wt_ja"]), len(f["z_ja"]))
-    B = apply_bytes(n, *nnz)
+    lay = {k: df.layout_info(k) for k in ("wt", "z")}
+    sb = layout_bytes(n, lay, 8, 8)
+    B = sb[0] + sb[1]
+    B_csr = csr_apply_bytes(n, *nnz)
     dev = torch.device("cuda", local)
     x = torch.from_numpy(ainv.pde.rand_uniform(0, n)).to(dev)
     y = torch.zeros(n, dtype=torch.float64, device=dev)
@@ -291,7 +294,6 @@ def main():
             st[stage].append((a, b))
     torch.cuda.synchronize()
     st_ms = {s: sum(a.elapsed_time(b) for a, b in st[s]) / K2 for s in st}
-    sb = stage_bytes(n, nnz)
     dom = max((1, 2), key=lambda s: st_ms[s])
     dom_name = {1: "k_sweep_dscale", 2: "k_sweep_axpby"}[dom]
     peak, peak_kind = measured_peaks()
@@ -329,12 +331,12 @@ def main():
 
     extras = {}
     if not args.no_extras:
-        extras = run_extras(ainv, torch, dev, irp, ja, val, f, sv, flush, stream)
+        extras = run_extras(ainv, torch, dev, irp, ja, val, f, sv, flush, stream, ms)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         dt, reps, cores = cpu_baseline_apply(f, n)
-        cpu = {"value": round(B / dt / 1e9, 3), "unit": "GB/s", "cores": cores, "kind": "port",
+        cpu = {"value": round(B_csr / dt / 1e9, 3), "unit": "GB/s", "cores": cores, "kind": "port",
                "sample": f"{reps} full 200^3 applies ({dt * 1e3:.1f} ms each) of the CPU "
                          "restatement of the reference apply, OpenMP over rows"}
 
@@ -346,7 +348,12 @@ def main():
                "config": {"workload": WORKLOAD if args.idim == IDIM else
                           WORKLOAD.replace("_200_", f"_{args.idim}_"), "n": n, "nnz_A": int(len(ja)),
                           "nnz_wt": nnz[0], "nnz_z": nnz[1], "bytes_per_apply": B,
-                          "layout": "SELL-32", "l2": "flushed between steps (256 MB write)",
+                          "csr_bytes_per_apply": B_csr,
+                          "csr_equivalent_GBps": round(B_csr * world / (ms * 1e-3) / 1e9, 1),
+                          "layout": "32-row slices, shared column offsets per slice",
+                          "offset_slices": [lay["wt"]["offset_slices"], lay["z"]["offset_slices"]],
+                          "nslices": lay["wt"]["nslices"],
+                          "l2": "flushed between steps (256 MB write)",
                           "parallelism": f"replicas{world}",
                           "pct_of_hbm_peak": round(100 * value / world / peak, 2)},
                "roofline": {"bound": "hbm", "kernel": dom_name,
@@ -364,7 +371,7 @@ def main():
     return 0
 
 
-def run_extras(ainv, torch, dev, irp, ja, val, f, sv, flush, stream):
+def run_extras(ainv, torch, dev, irp, ja, val, f, sv, flush, stream, fp64_ms):
     """Mixed-precision apply GB/s and BiCGSTAB solves/s (FP64 vs FP32 factors)."""
     n = len(irp) - 1
     nnz = (len(f["wt_ja"]), len(f["z_ja"]))
@@ -386,9 +393,10 @@ def run_extras(ainv, torch, dev, irp, ja, val, f, sv, flush, stream):
             evs.append((a, b))
         torch.cuda.synchronize()
         ms = sum(a.elapsed_time(b) for a, b in evs) / len(evs)
-        Bm = apply_bytes(n, *nnz, vsize=vs, tsize=4)
+        Bm = sum(layout_bytes(n, {k: df.layout_info(k) for k in ("wt", "z")}, vs, 4))
         out["mixed"][prec] = {"ms": round(ms, 5), "GB/s": round(Bm / (ms * 1e-3) / 1e9, 2),
-                              "bytes": Bm}
+                              "bytes": Bm,
+                              "speedup_vs_fp64": round(fp64_ms / ms, 3)}
         df.close()
     # BiCGSTAB to 1e-9, b = A x*, x* ~ U(-1,1) seed 0
     A = ainv.DeviceOperator(irp, ja, val)

@@ -54,6 +54,7 @@ extern "C" {
 #define AINV_ERR_NONFINITE    4103 /* non-finite residual in the Krylov loop */
 #define AINV_ERR_NOCONV       4104 /* itmax reached before the tolerance    */
 #define AINV_ERR_UNSUPPORTED  4105 /* option not built into this library   */
+#define AINV_ERR_TIMEOUT      4106 /* a device-side wait ran past its limit  */
 
 /* ---- factor storage precision (values of W^T, Z and D^-1) ------------- */
 #define AINV_PREC_FP64 0
@@ -104,14 +105,20 @@ int ainv_gpu_apply_stage(ainv_handle *h, char trans, int stage, double alpha,
 int ainv_gpu_apply_host(ainv_handle *h, char trans, double alpha, const double *x,
                         double beta, double *y);
 int ainv_gpu_destroy(ainv_handle *h);
+/* Synchronise and report whether any kernel working on h gave up a wait
+ * (the streaming kernels bound every wait to about 2 s); clears the flag.
+ * AINV_SUCCESS or AINV_ERR_TIMEOUT. */
+int ainv_gpu_check(const ainv_handle *h);
 size_t ainv_gpu_sizeof(const ainv_handle *h);
 long long ainv_gpu_get_nzeros(const ainv_handle *h);
 int ainv_gpu_get_n(const ainv_handle *h);
 int ainv_gpu_get_prec(const ainv_handle *h);
-/* Nonzeros and device bytes of the apply's two sweeps for trans 'N'
- * (W^T then Z): nnz_wt, nnz_z, stored (padded) slots of each. */
-int ainv_gpu_layout_info(const ainv_handle *h, long long *nnz_wt, long long *nnz_z,
-                         long long *slots_wt, long long *slots_z);
+/* Device layout of one operand: which = 0 W^T, 1 Z (the 'N' sweeps),
+ * 2 Z^T, 3 W (the 'T' sweeps).  nnz: entries; slots: stored values incl.
+ * padding; nidx: stored index words; nslices: 32-row slices;
+ * offset_slices: slices that share one column-offset list. */
+int ainv_gpu_layout_info(const ainv_handle *h, int which, long long *nnz, long long *slots,
+                         long long *nidx, int *nslices, int *offset_slices);
 
 /* No counterpart in the reference.  The 'N' apply for callers that may not
  * allocate device memory when they apply (a framework that owns all device
@@ -141,6 +148,8 @@ int ainv_csr_create(ainv_csr **a, int n, const int *irp, const int *ja,
 int ainv_csr_spmv(const ainv_csr *a, double alpha, const double *x_dev, double beta,
                   double *y_dev, void *stream);
 int ainv_csr_destroy(ainv_csr *a);
+/* As ainv_gpu_check, for kernels working on the operator A. */
+int ainv_csr_check(const ainv_csr *a);
 /* Preconditioned CG / BiCGSTAB with istop=2 (||r||_2 <= eps*||b||_2).
  * x_dev holds x0 on entry and the solution on exit; h may be NULL (no
  * preconditioner).  Returns AINV_SUCCESS on convergence, AINV_ERR_NOCONV
@@ -149,6 +158,10 @@ int ainv_csr_destroy(ainv_csr *a);
 int ainv_gpu_solve(ainv_handle *h, const ainv_csr *a, const double *b_dev,
                    double *x_dev, int method, double eps, int itmax, int *iter,
                    double *err, void *stream);
+/* Statistics of the last ainv_gpu_solve on a: how often the recurrence
+ * claimed convergence the true residual did not confirm, and how often the
+ * recurrence residual was replaced by b - A x. */
+int ainv_csr_solve_info(const ainv_csr *a, int *verify_fails, int *replacements);
 
 /* ---- host solver types (mirror of the Fortran plugin types) ----------- */
 /* type: "AINV", "INVK" or "INVT".  default() is applied on creation. */

@@ -23,6 +23,7 @@ ERR_BREAKDOWN = 4102
 ERR_NONFINITE = 4103
 ERR_NOCONV = 4104
 ERR_UNSUPPORTED = 4105
+ERR_TIMEOUT = 4106
 
 PREC = {"FP64": 0, "FP32": 1, "BF16": 2}
 KRYLOV = {"CG": 0, "BICGSTAB": 1}
@@ -40,16 +41,19 @@ SIGNATURES = [
     ("ainv_gpu_apply_stage", _i, [_vp, _c, _i, _d, _vp, _d, _vp, _vp]),
     ("ainv_gpu_apply_host", _i, [_vp, _c, _d, _vp, _d, _vp]),
     ("ainv_gpu_destroy", _i, [_vp]),
+    ("ainv_gpu_check", _i, [_vp]),
     ("ainv_gpu_sizeof", C.c_size_t, [_vp]),
     ("ainv_gpu_get_nzeros", _ll, [_vp]),
     ("ainv_gpu_get_n", _i, [_vp]),
     ("ainv_gpu_get_prec", _i, [_vp]),
-    ("ainv_gpu_layout_info", _i, [_vp, _llp, _llp, _llp, _llp]),
+    ("ainv_gpu_layout_info", _i, [_vp, _i, _llp, _llp, _llp, _ip, _ip]),
     ("ainv_gpu_apply_csr_noalloc", _i, [_i, _vp, _vp, _vp, _ll, _vp, _vp, _vp, _ll, _vp, _d,
                                         _vp, _d, _vp, _vp]),
     ("ainv_csr_create", _i, [C.POINTER(_vp), _i, _vp, _vp, _vp, _i]),
     ("ainv_csr_spmv", _i, [_vp, _d, _vp, _d, _vp, _vp]),
     ("ainv_csr_destroy", _i, [_vp]),
+    ("ainv_csr_check", _i, [_vp]),
+    ("ainv_csr_solve_info", _i, [_vp, _ip, _ip]),
     ("ainv_gpu_solve", _i, [_vp, _vp, _vp, _vp, _i, _d, _i, _ip, _dp, _vp]),
     ("mld_d_solver_create", _i, [C.POINTER(_vp), C.c_char_p]),
     ("mld_d_solver_destroy", _i, [_vp]),

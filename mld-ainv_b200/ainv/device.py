@@ -79,16 +79,24 @@ class DeviceFactors:
                                         C.c_void_p(x.ctypes.data), beta, C.c_void_p(y.ctypes.data)))
         return y
 
+    def check(self) -> None:
+        """Raise if a device-side wait of a kernel on these factors timed out."""
+        check(lib().ainv_gpu_check(self._h))
+
     def sizeof(self) -> int:
         return int(lib().ainv_gpu_sizeof(self._h))
 
     def get_nzeros(self) -> int:
         return int(lib().ainv_gpu_get_nzeros(self._h))
 
-    def layout_info(self) -> dict:
-        v = [C.c_longlong() for _ in range(4)]
-        check(lib().ainv_gpu_layout_info(self._h, *[C.byref(x) for x in v]))
-        return dict(nnz_wt=v[0].value, nnz_z=v[1].value, slots_wt=v[2].value, slots_z=v[3].value)
+    def layout_info(self, which: str = "wt") -> dict:
+        """Device layout of one operand: 'wt', 'z' (trans 'N'), 'zt', 'w' (trans 'T')."""
+        w = {"wt": 0, "z": 1, "zt": 2, "w": 3}[which]
+        ll = [C.c_longlong() for _ in range(3)]
+        ii = [C.c_int() for _ in range(2)]
+        check(lib().ainv_gpu_layout_info(self._h, w, *[C.byref(x) for x in ll + ii]))
+        return dict(nnz=ll[0].value, slots=ll[1].value, nidx=ll[2].value, nslices=ii[0].value,
+                    offset_slices=ii[1].value)
 
     def close(self) -> None:
         if getattr(self, "_own", False) and self._h:
@@ -103,15 +111,17 @@ class DeviceFactors:
 
 
 class SolveResult:
-    def __init__(self, info, iters, err):
+    def __init__(self, info, iters, err, verify_fails=0, replacements=0):
         self.info, self.iter, self.err = info, iters, err
+        self.verify_fails, self.replacements = verify_fails, replacements
 
     @property
     def converged(self) -> bool:
         return self.info == SUCCESS
 
     def __repr__(self):
-        return f"SolveResult(info={self.info}, iter={self.iter}, err={self.err:.3e})"
+        return (f"SolveResult(info={self.info}, iter={self.iter}, err={self.err:.3e}, "
+                f"verify_fails={self.verify_fails}, replacements={self.replacements})")
 
 
 class DeviceOperator:
@@ -130,6 +140,10 @@ class DeviceOperator:
     def handle(self):
         return self._h
 
+    def check(self) -> None:
+        """Raise if a device-side wait of a kernel on A timed out."""
+        check(lib().ainv_csr_check(self._h))
+
     def spmv(self, x, y, alpha=1.0, beta=0.0, stream=None) -> None:
         check(lib().ainv_csr_spmv(self._h, alpha, dptr(x), beta, dptr(y), _stream(stream)))
 
@@ -143,7 +157,9 @@ class DeviceOperator:
                                     C.byref(it), C.byref(err), _stream(stream))
         if info not in (SUCCESS, 4102, 4103, 4104):
             check(info)
-        return SolveResult(info, it.value, err.value)
+        vf, rp = C.c_int(0), C.c_int(0)
+        lib().ainv_csr_solve_info(self._h, C.byref(vf), C.byref(rp))
+        return SolveResult(info, it.value, err.value, vf.value, rp.value)
 
     def close(self) -> None:
         if self._h:

@@ -26,6 +26,7 @@ void destroy_handle(ainv_handle *h) {
   if (h->t) cudaFree(h->t);
   if (h->xs) cudaFree(h->xs);
   if (h->ys) cudaFree(h->ys);
+  if (h->status) cudaFree(h->status);
   delete h;
 }
 
@@ -87,6 +88,8 @@ int ainv_gpu_create(ainv_handle **hp, int n, const int *wt_irp, const int *wt_ja
   if (rc == AINV_SUCCESS) {
     const size_t ts = (prec == AINV_PREC_FP64) ? 8 : 4;
     cudaError_t e = cudaMalloc(&h->t, ts * (size_t)n);
+    if (e == cudaSuccess) e = cudaMalloc(&h->status, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(h->status, 0, sizeof(int));
     if (e != cudaSuccess) {
       ainv::set_error("ainv_gpu_create: scratch allocation failed: %s", cudaGetErrorString(e));
       rc = AINV_ERR_ALLOC;
@@ -121,8 +124,10 @@ int ainv_gpu_apply_stage(ainv_handle *h, char trans, int stage, double alpha,
     return AINV_ERR_ARG;
   }
   cudaStream_t s = (cudaStream_t)stream;
-  if (stage == 1) return ainv::launch_sweep_dscale(tr ? h->zt : h->wt, h->d, x_dev, h->t, s);
-  return ainv::launch_sweep_axpby(tr ? h->w : h->z, h->t, alpha, beta, y_dev, s);
+  if (stage == 1)
+    return ainv::launch_sweep_dscale(tr ? h->zt : h->wt, h->d, x_dev, h->t, s, nullptr, h->status);
+  return ainv::launch_sweep_axpby(tr ? h->w : h->z, h->t, alpha, beta, y_dev, s, nullptr,
+                                  h->status);
 }
 
 int ainv_gpu_apply_host(ainv_handle *h, char trans, double alpha, const double *x,
@@ -166,17 +171,43 @@ long long ainv_gpu_get_nzeros(const ainv_handle *h) {
 int ainv_gpu_get_n(const ainv_handle *h) { return h ? h->n : 0; }
 int ainv_gpu_get_prec(const ainv_handle *h) { return h ? h->prec : -1; }
 
-int ainv_gpu_layout_info(const ainv_handle *h, long long *nnz_wt, long long *nnz_z,
-                         long long *slots_wt, long long *slots_z) {
-  if (!h) {
-    ainv::set_error("ainv_gpu_layout_info: null handle");
+int ainv_gpu_layout_info(const ainv_handle *h, int which, long long *nnz, long long *slots,
+                         long long *nidx, int *nslices, int *offset_slices) {
+  if (!h || which < 0 || which > 3) {
+    ainv::set_error("ainv_gpu_layout_info: invalid argument");
     return AINV_ERR_ARG;
   }
-  if (nnz_wt) *nnz_wt = h->wt.nnz;
-  if (nnz_z) *nnz_z = h->z.nnz;
-  if (slots_wt) *slots_wt = h->wt.slots;
-  if (slots_z) *slots_z = h->z.slots;
+  const DevSell &m = which == 0 ? h->wt : which == 1 ? h->z : which == 2 ? h->zt : h->w;
+  if (nnz) *nnz = m.nnz;
+  if (slots) *slots = m.slots;
+  if (nidx) *nidx = m.nidx;
+  if (nslices) *nslices = m.nslices;
+  if (offset_slices) *offset_slices = m.offset_slices;
   return AINV_SUCCESS;
+}
+
+// Streaming kernels record a timed-out wait in the object's status word;
+// reading it synchronises the device and clears it.
+static int read_status(int *word, const char *what) {
+  if (!word) return AINV_SUCCESS;
+  int v = 0;
+  AINV_CUDA_TRY(cudaMemcpy(&v, word, sizeof(int), cudaMemcpyDeviceToHost));
+  if (v != 0) {
+    AINV_CUDA_TRY(cudaMemset(word, 0, sizeof(int)));
+    ainv::set_error("%s: a device wait ran past its time limit; results are incomplete", what);
+    return AINV_ERR_TIMEOUT;
+  }
+  return AINV_SUCCESS;
+}
+
+int ainv_gpu_check(const ainv_handle *h) {
+  if (!h) return AINV_ERR_ARG;
+  return read_status(h->status, "ainv_gpu_check");
+}
+
+int ainv_csr_check(const ainv_csr *a) {
+  if (!a) return AINV_ERR_ARG;
+  return read_status(a->status, "ainv_csr_check");
 }
 
 int ainv_csr_create(ainv_csr **ap, int n, const int *irp, const int *ja, const double *val,
@@ -195,7 +226,17 @@ int ainv_csr_create(ainv_csr **ap, int n, const int *irp, const int *ja, const d
   }
   m->n = n;
   int rc = ainv::upload_sell(a, AINV_PREC_FP64, m->a);
+  if (rc == AINV_SUCCESS) {
+    cudaError_t e = cudaMalloc(&m->status, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(m->status, 0, sizeof(int));
+    if (e != cudaSuccess) {
+      ainv::set_error("ainv_csr_create: status allocation failed: %s", cudaGetErrorString(e));
+      rc = AINV_ERR_ALLOC;
+    }
+  }
   if (rc != AINV_SUCCESS) {
+    ainv::free_sell(m->a);
+    if (m->status) cudaFree(m->status);
     delete m;
     return rc;
   }
@@ -209,13 +250,14 @@ int ainv_csr_spmv(const ainv_csr *a, double alpha, const double *x_dev, double b
     ainv::set_error("ainv_csr_spmv: null argument");
     return AINV_ERR_ARG;
   }
-  return ainv::launch_spmv(a->a, alpha, x_dev, beta, y_dev, (cudaStream_t)stream);
+  return ainv::launch_spmv(a->a, alpha, x_dev, beta, y_dev, (cudaStream_t)stream, a->status);
 }
 
 int ainv_csr_destroy(ainv_csr *a) {
   if (a) {
     ainv::destroy_ws(a->ws);
     ainv::free_sell(a->a);
+    if (a->status) cudaFree(a->status);
     delete a;
   }
   return AINV_SUCCESS;

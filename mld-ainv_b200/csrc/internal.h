@@ -47,21 +47,65 @@ int import_csr(int n, const int *irp, const int *ja, const double *val,
 HostCsr transpose(const HostCsr &a);
 
 // ------------------------------------------------------ device layout --
-// SELL-32: rows are taken 32 at a time ("slices"); a slice of width w holds
-// 32*w slots stored column-major, slot (k, lane) at sptr[s] + 32*k + lane.
-// Padding slots carry value 0 and the row's own index as column, so every
-// gather stays in bounds and lands next to data the warp already touches.
+// Sliced layout, 32 rows per slice, slots stored column-major: slot k of
+// lane l of slice s is value val[sptr[s] + 32*k + l].  Each slice picks the
+// cheaper of two index encodings:
+//   offset mode: the slice's rows share one sorted list of column offsets
+//     (col - row); the slice stores that list once (iptr[s+1]-iptr[s] == w
+//     entries) and slot k of every lane holds the value at offset idx[k], or
+//     0 where that row has no entry.  Stencil-derived factors are all in
+//     this mode, so almost no index bytes are streamed and the gathers of
+//     the 32 lanes are contiguous.
+//   column mode (SELL): one int32 column per slot (32*w entries); padding
+//     slots carry value 0 and the row's own index.
+// w is the slice width (slots per lane), a multiple of the pack P: the P
+// slots kP..kP+P-1 of one lane are adjacent in memory, so a lane reads them
+// with one vector load (slot k of lane l at sptr[s] + (k/P)*32P + l*P + k%P;
+// per-slot columns use the same arrangement).  P is chosen per matrix (up to
+// 16 bytes per load) as long as padding to a multiple of P costs <= 6%.
 constexpr int kSlice = 32;
+constexpr int kMaxOffsets = 64;  // offset mode only for slices with <= 64 offsets
+
+// A stage is stage_slices consecutive slices (kConsumerSlices per consumer
+// warp times a per-precision factor) streamed into shared memory by bulk
+// asynchronous copies: its descriptor, its slice pointers, values, index
+// words and, for uniform stages, the windows of the gathered vector.  A
+// stage is "uniform" when all its slices use offset mode with one identical
+// offset list of at most kStageMaxOffsets entries; its gathers then read
+// contiguous windows x[r0+o, r1+o) that are copied too.  Built on the host at
+// upload; consumed by the streaming kernels.
+constexpr int kConsumerSlices = 8;   // consumer warps per streaming block
+constexpr int kStageMaxOffsets = 8;
+constexpr int kMaxStageSlices = 32;
+struct alignas(16) StageDesc {
+  int s0, s1;          // slice range [s0, s1)
+  int vstart;          // first value (element index, = sptr[s0])
+  int vbytes;          // value bytes (multiple of 16)
+  long long ibyte0;    // first index byte copied (16-aligned)
+  int ibytes;          // index bytes copied (multiple of 16)
+  int noff;            // uniform: number of offsets, else 0
+  int off[kStageMaxOffsets];
+};
+static_assert(sizeof(StageDesc) == 64, "stage descriptor is one 64-byte copy");
 
 struct DevSell {
   int n = 0;
   int nslices = 0;
   long long nnz = 0;    // real entries
-  long long slots = 0;  // stored entries incl. padding
+  long long slots = 0;  // stored values incl. padding
+  long long nidx = 0;   // stored index words
+  int offset_slices = 0;
+  int pack = 1;  // P
   int prec = AINV_PREC_FP64;
-  int *sptr = nullptr;  // nslices+1 slot offsets
-  int *col = nullptr;   // slots
+  int *sptr = nullptr;  // nslices+1 value offsets (+16 bytes of tail padding)
+  int *iptr = nullptr;  // nslices+1 index offsets (+16 bytes of tail padding)
+  int *idx = nullptr;   // nidx offsets / columns (+16 bytes of tail padding)
   void *val = nullptr;  // slots, element type from prec
+  // streaming stages (see StageDesc); nstages = 0 when not streamable
+  int nstages = 0;
+  int stage_slices = 0;
+  int stage_vmax = 0, stage_imax = 0, stage_noff_max = 0;
+  StageDesc *stages = nullptr;
   size_t bytes() const;
 };
 
@@ -94,10 +138,12 @@ struct ainv_handle {
   void *t = nullptr;      // intermediate D^-1 W^T x (double for FP64, float otherwise)
   double *xs = nullptr;   // device staging for the host-array apply
   double *ys = nullptr;
+  int *status = nullptr;  // device word: nonzero after a streaming wait timed out
 };
 
 struct ainv_csr {
   int n = 0;
+  int *status = nullptr;  // device word: nonzero after a streaming wait timed out
   ainv::DevSell a;
   ainv::KrylovWs *ws = nullptr;  // Krylov vectors, state and captured graph
 };
@@ -107,14 +153,17 @@ namespace ainv {
 // t = d .* (M x) with M, d in prec; t is double (FP64) or float (mixed).
 // stop: optional device flag; when nonzero the kernel returns at once.
 int launch_sweep_dscale(const DevSell &m, const void *d, const double *x, void *t,
-                        cudaStream_t s, const int *stop = nullptr);
+                        cudaStream_t s, const int *stop = nullptr, int *status = nullptr);
 // y = alpha * M t + beta * y; t as produced by launch_sweep_dscale.
 int launch_sweep_axpby(const DevSell &m, const void *t, double alpha, double beta,
-                       double *y, cudaStream_t s, const int *stop = nullptr);
+                       double *y, cudaStream_t s, const int *stop = nullptr,
+                       int *status = nullptr);
 // y = alpha * A x + beta * y with an FP64 operator.
 int launch_spmv(const DevSell &a, double alpha, const double *x, double beta,
-                double *y, cudaStream_t s);
+                double *y, cudaStream_t s, int *status = nullptr);
 // Both sweeps of the apply for trans 'N' or 'T'/'C'.
+// status: device word for wait timeouts (the handle's own when null).
 int ainv_apply_async(const ainv_handle *h, char trans, double alpha, const double *x,
-                     double beta, double *y, cudaStream_t s, const int *stop = nullptr);
+                     double beta, double *y, cudaStream_t s, const int *stop = nullptr,
+                     int *status = nullptr);
 }  // namespace ainv

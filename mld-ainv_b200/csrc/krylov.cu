@@ -16,17 +16,23 @@
 // dot r.z share one kernel; x/r updates and the residual norm (plus rt.r
 // for BiCGSTAB) share one kernel.
 #include <atomic>
+#include <cstdint>
 #include <cmath>
 #include <cstdlib>
 #include <new>
 
-#include "sell_device.cuh"
+#include "stream.cuh"
 
 namespace ainv {
 
 struct KState {
   double rho, rho_old, alpha, beta, omega, rn2, bn2, eps;
-  int iter, itmax, done, status, replace_every, method;
+  int iter, itmax, done, status, check_every, method;
+  int verified;  // convergence confirmed on the true residual b - A x
+  int replace;   // r := b - A x pending (cleared by the next reduction kernel)
+  int fails;     // convergence claims the true residual did not confirm
+  int replacements;
+  int timeout;  // a streaming kernel gave up a bounded wait
   unsigned ticket[4];
 };
 
@@ -34,8 +40,10 @@ namespace {
 
 using namespace dev;
 
-enum { kCgSigma = 0, kBicgSigma = 1, kBicgOmega = 2, kReplace = 3, kInit = 4 };
-constexpr int kChunk = 8;  // iterations per captured graph launch
+enum { kCgSigma = 0, kBicgSigma = 1, kBicgOmega = 2, kTrueRes = 3, kInit = 4 };
+constexpr int kChunk = 8;         // iterations per captured graph launch
+constexpr double kDrift = 1e-6;   // replace r when ||(b - A x) - r|| > kDrift ||b - A x||
+constexpr int kMaxVerifyFails = 3;
 
 __device__ __forceinline__ void finish_iteration(KState *st, double rn2) {
   st->rn2 = rn2;
@@ -69,97 +77,83 @@ __device__ __forceinline__ void bicg_next_rho(KState *st, double rr) {
 // ||b||_2 (istop=2 denominator).
 __global__ void __launch_bounds__(kBlock)
     k_bnorm(int n, const double *__restrict__ b, KState *st, double *partials) {
-  const int i = blockIdx.x * kBlock + threadIdx.x;
   double pr[1] = {0.0};
-  if (i < n) pr[0] = b[i] * b[i];
+  for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock)
+    pr[0] += b[i] * b[i];
   if (grid_sum<1>(pr, partials, &st->ticket[0]) && threadIdx.x == 0) {
     const double bn = sqrt(pr[0]);
     st->bn2 = (bn == 0.0) ? 1.0 : bn;
   }
 }
 
-// y = A x with the reductions each caller needs (see MODE):
-//   kCgSigma:   sigma = x.y, alpha = rho/sigma               (q = A p)
-//   kBicgSigma: sigma = w1.y, alpha = rho/sigma              (v = A f, w1 = rt)
-//   kBicgOmega: omega = (y.w1)/(y.y)                         (t = A z, w1 = s)
-//   kReplace:   y = w1 - A x (true residual, w1 = b), every replace_every its
-//   kInit:      y = w1 - A x, optional copy into w2 (rt), initial norm/rho
+// Scalar bookkeeping done by the last block of an SpMV-with-dots kernel
+// (thread 0), from the grid totals pr.
 template <int MODE>
-__global__ void __launch_bounds__(kBlock)
-    k_spmv_dots(int n, int nslices, const int *__restrict__ sptr,
-                const int *__restrict__ col, const double *__restrict__ val,
-                const double *__restrict__ x, double *__restrict__ y,
-                const double *__restrict__ w1, double *__restrict__ w2, KState *st,
-                double *partials) {
-  if (st->done) return;
-  if (MODE == kReplace &&
-      (st->replace_every <= 0 || st->iter == 0 || st->iter % st->replace_every != 0))
-    return;
-  SliceCtx c;
-  double pr[2] = {0.0, 0.0};
-  if (slice_ctx(nslices, sptr, c)) {
-    const double acc = row_dot(col + c.beg + c.lane, val + c.beg + c.lane, x, c.w);
-    if (c.row < n) {
-      const int i = c.row;
-      if (MODE == kReplace || MODE == kInit) {
-        const double ri = w1[i] - acc;
-        y[i] = ri;
-        pr[0] = ri * ri;
-        if (w2) {
-          if (MODE == kInit) {
-            w2[i] = ri;
-            pr[1] = ri * ri;
-          } else {
-            pr[1] = w2[i] * ri;
-          }
-        }
-      } else {
-        y[i] = acc;
-        if (MODE == kCgSigma) pr[0] = x[i] * acc;
-        if (MODE == kBicgSigma) pr[0] = w1[i] * acc;
-        if (MODE == kBicgOmega) {
-          pr[0] = acc * acc;
-          pr[1] = acc * w1[i];
-        }
-      }
+__device__ __forceinline__ void finish_dots(KState *st, const double (&pr)[3], bool verify,
+                                            const double *w2) {
+  if (MODE == kCgSigma || MODE == kBicgSigma) {
+    if (MODE == kBicgSigma) st->replace = 0;
+    if (pr[0] == 0.0) {
+      st->status = AINV_ERR_BREAKDOWN;
+      st->done = 1;
+    } else {
+      st->alpha = st->rho / pr[0];
     }
-  }
-  if (grid_sum<2>(pr, partials, &st->ticket[1]) && threadIdx.x == 0) {
-    if (MODE == kCgSigma || MODE == kBicgSigma) {
-      if (pr[0] == 0.0) {
-        st->status = AINV_ERR_BREAKDOWN;
-        st->done = 1;
+  } else if (MODE == kBicgOmega) {
+    const double om = (pr[0] == 0.0) ? 0.0 : pr[1] / pr[0];
+    if (pr[0] == 0.0 || om == 0.0) {
+      st->status = AINV_ERR_BREAKDOWN;
+      st->done = 1;
+    } else {
+      st->omega = om;
+    }
+  } else if (MODE == kInit) {
+    st->rn2 = pr[0];
+    const double err = sqrt(pr[0]) / st->bn2;
+    if (!isfinite(pr[0])) {
+      st->status = AINV_ERR_NONFINITE;
+      st->done = 1;
+    } else if (err <= st->eps) {
+      st->status = AINV_SUCCESS;
+      st->done = 1;
+      st->verified = 1;  // computed from b - A x already
+    } else if (st->itmax <= 0) {
+      st->status = AINV_ERR_NOCONV;
+      st->done = 1;
+    }
+    st->rho = pr[1];
+  } else {  // kTrueRes
+    const double tn = sqrt(pr[0]), gap = sqrt(pr[1]);
+    bool replace;
+    if (verify) {
+      if (tn / st->bn2 <= st->eps || !isfinite(pr[0])) {
+        st->verified = 1;
+        st->rn2 = pr[0];
+        if (!isfinite(pr[0])) st->status = AINV_ERR_NONFINITE;
+        replace = false;
+      } else if (st->fails >= kMaxVerifyFails || st->iter >= st->itmax) {
+        st->verified = 1;
+        st->rn2 = pr[0];
+        st->status = AINV_ERR_NOCONV;
+        replace = false;
       } else {
-        st->alpha = st->rho / pr[0];
-      }
-    } else if (MODE == kBicgOmega) {
-      const double om = (pr[0] == 0.0) ? 0.0 : pr[1] / pr[0];
-      if (pr[0] == 0.0 || om == 0.0) {
-        st->status = AINV_ERR_BREAKDOWN;
-        st->done = 1;
-      } else {
-        st->omega = om;
-      }
-    } else {  // kReplace / kInit: convergence on the true residual
-      st->rn2 = pr[0];
-      const double err = sqrt(pr[0]) / st->bn2;
-      if (!isfinite(pr[0])) {
-        st->status = AINV_ERR_NONFINITE;
-        st->done = 1;
-      } else if (err <= st->eps) {
+        // the recurrence drifted: continue from the true residual
+        st->fails += 1;
+        st->done = 0;
         st->status = AINV_SUCCESS;
-        st->done = 1;
+        replace = true;
+        if (w2) st->rho_old = st->rho;  // k_bicg_xr skipped its rho step
       }
-      if (MODE == kInit) {
-        st->rho = pr[1];
-        if (!st->done && st->itmax <= 0) {
-          st->status = AINV_ERR_NOCONV;
-          st->done = 1;
-        }
-      } else if (w2 && !st->done) {
-        // rho for the coming iteration follows the replaced residual
-        st->rho = pr[1];
-        if (pr[1] == 0.0) {
+    } else {
+      replace = gap > kDrift * tn;
+    }
+    if (replace) {
+      st->replace = 1;
+      st->replacements += 1;
+      st->rn2 = pr[0];
+      if (w2) {  // BiCGSTAB: rho and beta follow the replaced residual
+        st->rho = pr[2];
+        if (pr[2] == 0.0) {
           st->status = AINV_ERR_BREAKDOWN;
           st->done = 1;
         } else {
@@ -170,25 +164,194 @@ __global__ void __launch_bounds__(kBlock)
   }
 }
 
-// CG: z = Z t (sweep 2 of the AINV apply) fused with rho = r.z, then beta.
-template <class V, class T>
+// y = A x with the reductions each caller needs (see MODE):
+//   kCgSigma:   sigma = x.y, alpha = rho/sigma               (q = A p)
+//   kBicgSigma: sigma = w1.y, alpha = rho/sigma              (v = A f, w1 = rt)
+//   kBicgOmega: omega = (y.w1)/(y.y)                         (t = A z, w1 = s)
+//   kInit:      y = w1 - A x, optional copy into w2 (rt), initial norm/rho
+//   kTrueRes:   y = w1 - A x (true residual, w1 = b) compared with the
+//               recurrence residual w3 = r; runs every check_every
+//               iterations and once when the recurrence claims convergence.
+//               Decides whether r is replaced (k_replace_r) and whether the
+//               convergence stands; w2 = rt for BiCGSTAB's rho.
+template <int MODE, int S, int P>
 __global__ void __launch_bounds__(kBlock)
-    k_cg_sweep2(int n, int nslices, const int *__restrict__ sptr, const int *__restrict__ col,
-                const V *__restrict__ val, const T *__restrict__ t,
-                const double *__restrict__ r, double *__restrict__ z, KState *st,
-                double *partials) {
-  if (st->done) return;
-  SliceCtx c;
-  double pr[1] = {0.0};
-  if (slice_ctx(nslices, sptr, c)) {
-    const auto acc = row_dot(col + c.beg + c.lane, val + c.beg + c.lane, t, c.w);
-    if (c.row < n) {
-      const double zi = (double)acc;
-      z[c.row] = zi;
-      pr[0] = r[c.row] * zi;
+    k_spmv_dots(SellView<double> m, const double *__restrict__ x, double *__restrict__ y,
+                const double *__restrict__ w1, double *__restrict__ w2,
+                const double *__restrict__ w3, KState *st, double *partials) {
+  bool verify = false;
+  if (MODE == kTrueRes) {
+    verify = st->done && st->status == AINV_SUCCESS && !st->verified;
+    const bool periodic = !st->done && st->check_every > 0 && st->iter > 0 &&
+                          st->iter % st->check_every == 0;
+    if (!verify && !periodic) return;
+  } else if (st->done) {
+    return;
+  }
+  double pr[3] = {0.0, 0.0, 0.0};
+  for_each_row<S, P>(m, x, [&](int i, double acc) {
+    if (MODE == kTrueRes || MODE == kInit) {
+      const double ri = w1[i] - acc;
+      y[i] = ri;
+      pr[0] += ri * ri;
+      if (MODE == kInit) {
+        if (w2) {
+          w2[i] = ri;
+          pr[1] += ri * ri;
+        }
+      } else {
+        const double g = ri - w3[i];
+        pr[1] += g * g;
+        if (w2) pr[2] += w2[i] * ri;
+      }
+    } else {
+      y[i] = acc;
+      if (MODE == kCgSigma) pr[0] += x[i] * acc;
+      if (MODE == kBicgSigma) pr[0] += w1[i] * acc;
+      if (MODE == kBicgOmega) {
+        pr[0] += acc * acc;
+        pr[1] += acc * w1[i];
+      }
+    }
+  });
+  if (grid_sum<3>(pr, partials, &st->ticket[1]) && threadIdx.x == 0)
+    finish_dots<MODE>(st, pr, verify, w2);
+}
+
+// r := b - A x when the last true-residual check asked for it.
+__global__ void __launch_bounds__(kBlock)
+    k_replace_r(int n, const double *__restrict__ rtrue, double *__restrict__ r,
+                const KState *st) {
+  if (!st->replace) return;
+  const int i = blockIdx.x * kBlock + threadIdx.x;
+  if (i < n) r[i] = rtrue[i];
+}
+
+// ---- streaming variants (stream.cuh) ----------------------------------------
+// Epilogue of the SpMV-with-dots kernels: the per-row operands are loaded
+// while the stage's copies land, the dots accumulate in pr.
+template <int MODE>
+struct EpiDots {
+  double *__restrict__ y;
+  const double *__restrict__ x;
+  const double *__restrict__ w1;
+  double *__restrict__ w2;
+  const double *__restrict__ w3;
+  double pr[3];
+  static constexpr int kRowVecs = (MODE == kTrueRes) ? 3 : 1;
+  // row operands: b (init / true residual, with r and rt), p (CG sigma),
+  // rt (BiCGSTAB sigma), s (BiCGSTAB omega)
+  __device__ __host__ __forceinline__ RowVecs row_vecs() const {
+    if (MODE == kTrueRes) return RowVecs{{w1, w3, w2}, {8, 8, w2 ? 8 : 0}};
+    if (MODE == kCgSigma) return RowVecs{{x, nullptr, nullptr}, {8, 0, 0}};
+    return RowVecs{{w1, nullptr, nullptr}, {8, 0, 0}};
+  }
+  __device__ __forceinline__ void post(int i, double acc, const StagedRows &r) {
+    if (MODE == kTrueRes || MODE == kInit) {
+      const double ri = r.get<double>(0, i) - acc;
+      y[i] = ri;
+      pr[0] += ri * ri;
+      if (MODE == kInit) {
+        if (w2) {
+          w2[i] = ri;
+          pr[1] += ri * ri;
+        }
+      } else {
+        const double g = ri - r.get<double>(1, i);
+        pr[1] += g * g;
+        if (w2) pr[2] += r.get<double>(2, i) * ri;
+      }
+    } else {
+      y[i] = acc;
+      const double a = r.get<double>(0, i);
+      if (MODE == kCgSigma || MODE == kBicgSigma) pr[0] += a * acc;
+      if (MODE == kBicgOmega) {
+        pr[0] += acc * acc;
+        pr[1] += acc * a;
+      }
     }
   }
+};
+
+template <int MODE, int P>
+__global__ void __launch_bounds__(kStreamThreads)
+    k_stream_dots(SellView<double> m, const StageDesc *__restrict__ stages, int nstages,
+                  StreamLayout L, const double *__restrict__ x, double *__restrict__ y,
+                  const double *__restrict__ w1, double *__restrict__ w2,
+                  const double *__restrict__ w3, KState *st, double *partials) {
+  bool verify = false;
+  if (MODE == kTrueRes) {
+    verify = st->done && st->status == AINV_SUCCESS && !st->verified;
+    const bool periodic = !st->done && st->check_every > 0 && st->iter > 0 &&
+                          st->iter % st->check_every == 0;
+    if (!verify && !periodic) return;
+  } else if (st->done) {
+    return;
+  }
+  EpiDots<MODE> epi{y, x, w1, w2, w3, {0.0, 0.0, 0.0}};
+  stream_rows<P, 1>(m, stages, nstages, x, L, epi, &st->timeout);
+  if (grid_sum<3>(epi.pr, partials, &st->ticket[1]) && threadIdx.x == 0)
+    finish_dots<MODE>(st, epi.pr, verify, w2);
+}
+
+// CG sweep 2 with rho = r.z, streaming.
+template <class T>
+struct EpiCgZ {
+  const double *__restrict__ r;
+  double *__restrict__ z;
+  double pr[1];
+  static constexpr int kRowVecs = 1;
+  __device__ __host__ __forceinline__ RowVecs row_vecs() const {
+    return RowVecs{{r, nullptr, nullptr}, {8, 0, 0}};
+  }
+  template <class A>
+  __device__ __forceinline__ void post(int i, A acc, const StagedRows &rows) {
+    const double zi = (double)acc;
+    z[i] = zi;
+    pr[0] += rows.get<double>(0, i) * zi;
+  }
+};
+
+__device__ __forceinline__ void finish_cg_rho(KState *st, double rz) {
+  st->replace = 0;
+  st->rho_old = st->rho;
+  st->rho = rz;
+  if (st->iter > 0) {
+    if (st->rho_old == 0.0) {
+      st->status = AINV_ERR_BREAKDOWN;
+      st->done = 1;
+    } else {
+      st->beta = st->rho / st->rho_old;
+    }
+  }
+}
+
+template <class V, class T, int P>
+__global__ void __launch_bounds__(kStreamThreads)
+    k_stream_cg_sweep2(SellView<V> m, const StageDesc *__restrict__ stages, int nstages,
+                       StreamLayout L, const T *__restrict__ t, const double *__restrict__ r,
+                       double *__restrict__ z, KState *st, double *partials) {
+  if (st->done) return;
+  EpiCgZ<T> epi{r, z, {0.0}};
+  stream_rows<P, stream_rmax<V>()>(m, stages, nstages, t, L, epi, &st->timeout);
+  if (grid_sum<1>(epi.pr, partials, &st->ticket[0]) && threadIdx.x == 0)
+    finish_cg_rho(st, epi.pr[0]);
+}
+
+// CG: z = Z t (sweep 2 of the AINV apply) fused with rho = r.z, then beta.
+template <class V, class T, int S, int P>
+__global__ void __launch_bounds__(kBlock)
+    k_cg_sweep2(SellView<V> m, const T *__restrict__ t, const double *__restrict__ r,
+                double *__restrict__ z, KState *st, double *partials) {
+  if (st->done) return;
+  double pr[1] = {0.0};
+  for_each_row<S, P>(m, t, [&](int i, auto acc) {
+    const double zi = (double)acc;
+    z[i] = zi;
+    pr[0] += r[i] * zi;
+  });
   if (grid_sum<1>(pr, partials, &st->ticket[0]) && threadIdx.x == 0) {
+    st->replace = 0;
     st->rho_old = st->rho;
     st->rho = pr[0];
     if (st->iter > 0) {
@@ -207,13 +370,13 @@ __global__ void __launch_bounds__(kBlock)
     k_cg_ident(int n, const double *__restrict__ r, double *__restrict__ z, KState *st,
                double *partials) {
   if (st->done) return;
-  const int i = blockIdx.x * kBlock + threadIdx.x;
   double pr[1] = {0.0};
-  if (i < n) {
+  for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
     z[i] = r[i];
-    pr[0] = r[i] * r[i];
+    pr[0] += r[i] * r[i];
   }
   if (grid_sum<1>(pr, partials, &st->ticket[0]) && threadIdx.x == 0) {
+    st->replace = 0;
     st->rho_old = st->rho;
     st->rho = pr[0];
     if (st->iter > 0) {
@@ -241,14 +404,13 @@ __global__ void __launch_bounds__(kBlock)
     k_cg_xr(int n, const double *__restrict__ p, const double *__restrict__ q,
             double *__restrict__ x, double *__restrict__ r, KState *st, double *partials) {
   if (st->done) return;
-  const int i = blockIdx.x * kBlock + threadIdx.x;
   const double alpha = st->alpha;
   double pr[1] = {0.0};
-  if (i < n) {
+  for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
     x[i] = x[i] + alpha * p[i];
     const double ri = r[i] - alpha * q[i];
     r[i] = ri;
-    pr[0] = ri * ri;
+    pr[0] += ri * ri;
   }
   if (grid_sum<1>(pr, partials, &st->ticket[2]) && threadIdx.x == 0)
     finish_iteration(st, pr[0]);
@@ -281,15 +443,14 @@ __global__ void __launch_bounds__(kBlock)
               const double *__restrict__ rt, double *__restrict__ x,
               double *__restrict__ r, KState *st, double *partials) {
   if (st->done) return;
-  const int i = blockIdx.x * kBlock + threadIdx.x;
   const double alpha = st->alpha, omega = st->omega;
   double pr[2] = {0.0, 0.0};
-  if (i < n) {
+  for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
     x[i] = (x[i] + alpha * f[i]) + omega * z[i];
     const double ri = s[i] - omega * t[i];
     r[i] = ri;
-    pr[0] = ri * ri;
-    pr[1] = rt[i] * ri;
+    pr[0] += ri * ri;
+    pr[1] += rt[i] * ri;
   }
   if (grid_sum<2>(pr, partials, &st->ticket[2]) && threadIdx.x == 0) {
     finish_iteration(st, pr[0]);
@@ -298,10 +459,125 @@ __global__ void __launch_bounds__(kBlock)
 }
 
 template <class V, class T>
+struct CgSweep2Launch {
+  const DevSell &m;
+  const void *t;
+  const double *r;
+  double *z;
+  KState *st;
+  double *partials;
+  int G;
+  cudaStream_t s;
+  template <int S, int P>
+  void run() const {
+    k_cg_sweep2<V, T, S, P><<<G, kBlock, 0, s>>>(view<V>(m), (const T *)t, r, z, st, partials);
+  }
+};
+
+inline bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+template <class V, class T>
+struct StreamCgSweep2Launch {
+  const DevSell &m;
+  StreamLayout L;
+  int grid;
+  size_t smem;
+  const void *t;
+  const double *r;
+  double *z;
+  KState *st;
+  double *partials;
+  cudaStream_t s;
+  bool *launched;
+  template <int S, int P>
+  void run() const {
+    auto kern = k_stream_cg_sweep2<V, T, P>;
+    if (!set_smem_attr((const void *)kern, smem)) return;
+    kern<<<grid, kStreamThreads, smem, s>>>(view<V>(m), m.stages, m.nstages, L, (const T *)t, r,
+                                            z, st, partials);
+    *launched = true;
+  }
+};
+
+template <class V, class T>
 void launch_cg_sweep2(const DevSell &m, const void *t, const double *r, double *z,
-                      KState *st, double *partials, cudaStream_t s) {
-  k_cg_sweep2<V, T><<<grid_for(m.nslices), kBlock, 0, s>>>(
-      m.n, m.nslices, m.sptr, m.col, (const V *)m.val, (const T *)t, r, z, st, partials);
+                      KState *st, double *partials, int G, cudaStream_t s) {
+  if (stream_enabled(m.prec)) {
+    StreamLayout L;
+    size_t smem = 0;
+    const int grid = stream_plan(m, (int)sizeof(T), EpiCgZ<T>::kRowVecs, L, smem);
+    bool launched = false;
+    if (grid > 0 && grid <= G && aligned16(t) && aligned16(r))
+      with_pack<V, 1>(m.pack, StreamCgSweep2Launch<V, T>{m, L, grid, smem, t, r, z, st, partials,
+                                                          s, &launched});
+    if (launched) return;
+  }
+  with_group_pack<V>(group_size(m.prec), m.pack,
+                     CgSweep2Launch<V, T>{m, t, r, z, st, partials, G, s});
+}
+
+template <int MODE>
+struct SpmvDotsLaunch {
+  const SellView<double> &A;
+  int G;
+  cudaStream_t s;
+  const double *x;
+  double *y;
+  const double *w1;
+  double *w2;
+  const double *w3;
+  KState *st;
+  double *pp;
+  template <int S, int P>
+  void run() const {
+    k_spmv_dots<MODE, S, P><<<G, kBlock, 0, s>>>(A, x, y, w1, w2, w3, st, pp);
+  }
+};
+
+template <int MODE>
+struct StreamDotsLaunch {
+  const DevSell &m;
+  StreamLayout L;
+  int grid;
+  size_t smem;
+  cudaStream_t s;
+  const double *x;
+  double *y;
+  const double *w1;
+  double *w2;
+  const double *w3;
+  KState *st;
+  double *pp;
+  bool *launched;
+  template <int S, int P>
+  void run() const {
+    auto kern = k_stream_dots<MODE, P>;
+    if (!set_smem_attr((const void *)kern, smem)) return;
+    kern<<<grid, kStreamThreads, smem, s>>>(view<double>(m), m.stages, m.nstages, L, x, y, w1,
+                                            w2, w3, st, pp);
+    *launched = true;
+  }
+};
+
+// y = A x with the dots of MODE (streaming when the layout allows).
+template <int MODE>
+void spmv_dots(const DevSell &Am, int G, cudaStream_t s, const double *x, double *y,
+               const double *w1, double *w2, const double *w3, KState *st, double *pp) {
+  if (stream_enabled(Am.prec)) {
+    StreamLayout L;
+    size_t smem = 0;
+    const int grid = stream_plan(Am, 8, EpiDots<MODE>::kRowVecs, L, smem);
+    const RowVecs rv = EpiDots<MODE>{y, x, w1, w2, w3, {0.0, 0.0, 0.0}}.row_vecs();
+    bool launched = false;
+    if (grid > 0 && grid <= G && aligned16(x) && aligned16(rv.p[0]) && aligned16(rv.p[1]) &&
+        aligned16(rv.p[2]))
+      with_pack<double, 1>(Am.pack, StreamDotsLaunch<MODE>{Am, L, grid, smem, s, x, y, w1, w2, w3,
+                                                           st, pp, &launched});
+    if (launched) return;
+  }
+  const SellView<double> A = view<double>(Am);
+  with_group_pack<double>(group_size(Am.prec), Am.pack,
+                          SpmvDotsLaunch<MODE>{A, G, s, x, y, w1, w2, w3, st, pp});
 }
 
 std::atomic<unsigned long long> g_serial{1};
@@ -313,7 +589,8 @@ unsigned long long next_serial() { return g_serial.fetch_add(1); }
 // ------------------------------------------------------------ workspace --
 struct KrylovWs {
   int n = 0, G = 0;
-  double *vec = nullptr;  // 10 vectors of n
+  size_t stride = 0;      // doubles between vectors (n rounded up to 32: 256 B aligned)
+  double *vec = nullptr;  // 11 vectors of n
   double *partials = nullptr;
   KState *st = nullptr;
   KState *hst = nullptr;  // pinned mirror
@@ -322,7 +599,8 @@ struct KrylovWs {
   cudaGraphExec_t exec = nullptr;
   unsigned long long key_serial = 0;
   int key_method = -1, key_replace = -1;
-  double *v(int i) const { return vec + (size_t)i * (size_t)n; }
+  KState last{};  // final state of the last solve (statistics)
+  double *v(int i) const { return vec + (size_t)i * stride; }
 };
 
 void destroy_ws(KrylovWs *w) {
@@ -339,7 +617,7 @@ void destroy_ws(KrylovWs *w) {
 
 namespace {
 
-enum { XW = 0, BW, R, RT, P, V, F, S, Z, T };
+enum { XW = 0, BW, R, RT, P, V, F, S, Z, T, RTRUE, kNumVec };
 
 int get_ws(ainv_csr *a, KrylovWs **out) {
   if (a->ws) {
@@ -352,14 +630,15 @@ int get_ws(ainv_csr *a, KrylovWs **out) {
     return AINV_ERR_ALLOC;
   }
   w->n = a->n;
-  w->G = (a->n + kBlock - 1) / kBlock;
-  cudaError_t e = cudaMalloc(&w->vec, sizeof(double) * 10 * (size_t)a->n);
+  w->stride = ((size_t)a->n + 31) / 32 * 32;
+  w->G = reduction_grid(a->n);
+  cudaError_t e = cudaMalloc(&w->vec, sizeof(double) * kNumVec * w->stride);
   if (e == cudaSuccess) e = cudaMalloc(&w->partials, sizeof(double) * 4 * (size_t)w->G);
   if (e == cudaSuccess) e = cudaMalloc(&w->st, sizeof(KState));
   if (e == cudaSuccess) e = cudaMallocHost(&w->hst, sizeof(KState));
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&w->s, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&w->ev, cudaEventDisableTiming);
-  if (e == cudaSuccess) e = cudaMemset(w->vec, 0, sizeof(double) * 10 * (size_t)a->n);
+  if (e == cudaSuccess) e = cudaMemset(w->vec, 0, sizeof(double) * kNumVec * w->stride);
   if (e != cudaSuccess) {
     destroy_ws(w);
     set_error("krylov workspace allocation failed: %s", cudaGetErrorString(e));
@@ -371,19 +650,21 @@ int get_ws(ainv_csr *a, KrylovWs **out) {
 }
 
 void precond_sweep2_cg(const ainv_handle *h, const double *r, double *z, KState *st,
-                       double *partials, cudaStream_t s) {
+                       double *partials, int G, cudaStream_t s) {
   switch (h->prec) {
-    case AINV_PREC_FP64: launch_cg_sweep2<double, double>(h->z, h->t, r, z, st, partials, s); break;
-    case AINV_PREC_FP32: launch_cg_sweep2<float, float>(h->z, h->t, r, z, st, partials, s); break;
-    default: launch_cg_sweep2<__nv_bfloat16, float>(h->z, h->t, r, z, st, partials, s); break;
+    case AINV_PREC_FP64: launch_cg_sweep2<double, double>(h->z, h->t, r, z, st, partials, G, s); break;
+    case AINV_PREC_FP32: launch_cg_sweep2<float, float>(h->z, h->t, r, z, st, partials, G, s); break;
+    default: launch_cg_sweep2<__nv_bfloat16, float>(h->z, h->t, r, z, st, partials, G, s); break;
   }
 }
 
-// One iteration, enqueued on ws->s.
+// One iteration, enqueued on ws->s.  Kernels ending in a reduction run on
+// the reduction grid G (one resident wave, grid-stride loops); the plain
+// vector updates use one thread per row.
 int enqueue_iteration(KrylovWs *w, const ainv_handle *h, const ainv_csr *a, int method) {
   const int n = w->n, G = w->G;
+  const int Gv = (n + kBlock - 1) / kBlock;
   const DevSell &A = a->a;
-  const int gA = grid_for(A.nslices);
   KState *st = w->st;
   double *pp = w->partials;
   cudaStream_t s = w->s;
@@ -391,44 +672,36 @@ int enqueue_iteration(KrylovWs *w, const ainv_handle *h, const ainv_csr *a, int 
   if (method == AINV_KRYLOV_CG) {
     double *r = w->v(R), *z = w->v(Z), *p = w->v(P), *q = w->v(V), *x = w->v(XW);
     if (h) {
-      AINV_TRY(launch_sweep_dscale(h->wt, h->d, r, h->t, s, stop));
-      precond_sweep2_cg(h, r, z, st, pp, s);
+      AINV_TRY(launch_sweep_dscale(h->wt, h->d, r, h->t, s, stop, &st->timeout));
+      precond_sweep2_cg(h, r, z, st, pp, G, s);
     } else {
       k_cg_ident<<<G, kBlock, 0, s>>>(n, r, z, st, pp);
     }
-    k_cg_p<<<G, kBlock, 0, s>>>(n, z, p, st);
-    k_spmv_dots<kCgSigma><<<gA, kBlock, 0, s>>>(n, A.nslices, A.sptr, A.col,
-                                                (const double *)A.val, p, q, nullptr,
-                                                nullptr, st, pp);
+    k_cg_p<<<Gv, kBlock, 0, s>>>(n, z, p, st);
+    spmv_dots<kCgSigma>(A, G, s, p, q, nullptr, nullptr, nullptr, st, pp);
     k_cg_xr<<<G, kBlock, 0, s>>>(n, p, q, x, r, st, pp);
-    k_spmv_dots<kReplace><<<gA, kBlock, 0, s>>>(n, A.nslices, A.sptr, A.col,
-                                                (const double *)A.val, x, r, w->v(BW),
-                                                nullptr, st, pp);
+    spmv_dots<kTrueRes>(A, G, s, x, w->v(RTRUE), w->v(BW), nullptr, r, st, pp);
+    k_replace_r<<<Gv, kBlock, 0, s>>>(n, w->v(RTRUE), r, st);
   } else {
     double *r = w->v(R), *rt = w->v(RT), *p = w->v(P), *v = w->v(V), *f = w->v(F),
            *sv = w->v(S), *z = w->v(Z), *t = w->v(T), *x = w->v(XW);
-    k_bicg_p<<<G, kBlock, 0, s>>>(n, r, v, p, st);
+    k_bicg_p<<<Gv, kBlock, 0, s>>>(n, r, v, p, st);
     if (h) {
-      AINV_TRY(ainv_apply_async(h, 'N', 1.0, p, 0.0, f, s, stop));
+      AINV_TRY(ainv_apply_async(h, 'N', 1.0, p, 0.0, f, s, stop, &st->timeout));
     } else {
       AINV_CUDA_TRY(cudaMemcpyAsync(f, p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     }
-    k_spmv_dots<kBicgSigma><<<gA, kBlock, 0, s>>>(n, A.nslices, A.sptr, A.col,
-                                                  (const double *)A.val, f, v, rt, nullptr,
-                                                  st, pp);
-    k_bicg_s<<<G, kBlock, 0, s>>>(n, r, v, sv, st);
+    spmv_dots<kBicgSigma>(A, G, s, f, v, rt, nullptr, nullptr, st, pp);
+    k_bicg_s<<<Gv, kBlock, 0, s>>>(n, r, v, sv, st);
     if (h) {
-      AINV_TRY(ainv_apply_async(h, 'N', 1.0, sv, 0.0, z, s, stop));
+      AINV_TRY(ainv_apply_async(h, 'N', 1.0, sv, 0.0, z, s, stop, &st->timeout));
     } else {
       AINV_CUDA_TRY(cudaMemcpyAsync(z, sv, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     }
-    k_spmv_dots<kBicgOmega><<<gA, kBlock, 0, s>>>(n, A.nslices, A.sptr, A.col,
-                                                  (const double *)A.val, z, t, sv, nullptr,
-                                                  st, pp);
+    spmv_dots<kBicgOmega>(A, G, s, z, t, sv, nullptr, nullptr, st, pp);
     k_bicg_xr<<<G, kBlock, 0, s>>>(n, f, z, sv, t, rt, x, r, st, pp);
-    k_spmv_dots<kReplace><<<gA, kBlock, 0, s>>>(n, A.nslices, A.sptr, A.col,
-                                                (const double *)A.val, x, r, w->v(BW), rt,
-                                                st, pp);
+    spmv_dots<kTrueRes>(A, G, s, x, w->v(RTRUE), w->v(BW), rt, r, st, pp);
+    k_replace_r<<<Gv, kBlock, 0, s>>>(n, w->v(RTRUE), r, st);
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
@@ -491,25 +764,26 @@ int krylov_solve(const ainv_handle *h, ainv_csr *a, const double *b, double *x, 
   KState init{};
   init.eps = eps;
   init.itmax = itmax;
-  init.replace_every = replace_every;
+  init.check_every = replace_every;
   init.method = method;
   *w->hst = init;
   AINV_CUDA_TRY(cudaMemcpyAsync(w->st, w->hst, sizeof(KState), cudaMemcpyHostToDevice, w->s));
   const DevSell &A = a->a;
   k_bnorm<<<w->G, kBlock, 0, w->s>>>(n, w->v(BW), w->st, w->partials);
-  k_spmv_dots<kInit><<<grid_for(A.nslices), kBlock, 0, w->s>>>(
-      n, A.nslices, A.sptr, A.col, (const double *)A.val, w->v(XW), w->v(R), w->v(BW),
-      method == AINV_KRYLOV_BICGSTAB ? w->v(RT) : nullptr, w->st, w->partials);
+  spmv_dots<kInit>(A, w->G, w->s, w->v(XW), w->v(R), w->v(BW),
+      method == AINV_KRYLOV_BICGSTAB ? w->v(RT) : nullptr, nullptr, w->st, w->partials);
   AINV_CUDA_TRY(cudaGetLastError());
 
+  // The first chunk always runs as plain launches (kernel attributes are
+  // settled outside any capture); later chunks replay one captured graph.
   const bool use_graph = getenv("AINV_NO_GRAPH") == nullptr;
-  if (use_graph) AINV_TRY(ensure_graph(w, h, a, method, replace_every));
   const long max_chunks = (long)itmax / kChunk + 2;
   for (long c = 0; c < max_chunks; c++) {
     AINV_CUDA_TRY(cudaMemcpyAsync(w->hst, w->st, sizeof(KState), cudaMemcpyDeviceToHost, w->s));
     AINV_CUDA_TRY(cudaStreamSynchronize(w->s));
     if (w->hst->done) break;
-    if (use_graph) {
+    if (use_graph && c > 0) {
+      AINV_TRY(ensure_graph(w, h, a, method, replace_every));
       AINV_CUDA_TRY(cudaGraphLaunch(w->exec, w->s));
     } else {
       for (int k = 0; k < kChunk; k++) AINV_TRY(enqueue_iteration(w, h, a, method));
@@ -521,8 +795,13 @@ int krylov_solve(const ainv_handle *h, ainv_csr *a, const double *b, double *x, 
   AINV_CUDA_TRY(cudaEventRecord(w->ev, w->s));
   AINV_CUDA_TRY(cudaStreamWaitEvent(user, w->ev, 0));
   const KState &f = *w->hst;
+  w->last = f;
   if (iter) *iter = f.iter;
   if (err) *err = sqrt(f.rn2) / f.bn2;
+  if (f.timeout) {
+    set_error("a device wait of the Krylov loop ran past its time limit");
+    return AINV_ERR_TIMEOUT;
+  }
   if (!f.done) {
     set_error("krylov loop did not terminate");
     return AINV_ERR_INTERNAL;
@@ -538,6 +817,17 @@ int krylov_solve(const ainv_handle *h, ainv_csr *a, const double *b, double *x, 
 }
 
 }  // namespace ainv
+
+extern "C" int ainv_csr_solve_info(const ainv_csr *a, int *verify_fails, int *replacements) {
+  if (!a) {
+    ainv::set_error("ainv_csr_solve_info: null operator");
+    return AINV_ERR_ARG;
+  }
+  const ainv::KState *s = a->ws ? &a->ws->last : nullptr;
+  if (verify_fails) *verify_fails = s ? s->fails : 0;
+  if (replacements) *replacements = s ? s->replacements : 0;
+  return AINV_SUCCESS;
+}
 
 extern "C" int ainv_gpu_solve(ainv_handle *h, const ainv_csr *a, const double *b_dev,
                               double *x_dev, int method, double eps, int itmax, int *iter,
@@ -558,7 +848,9 @@ extern "C" int ainv_gpu_solve(ainv_handle *h, const ainv_csr *a, const double *b
     ainv::set_error("ainv_gpu_solve: invalid eps/itmax");
     return AINV_ERR_ARG;
   }
-  // Mixed-precision factors: true-residual replacement every 50 iterations.
+  // Every solve confirms convergence on the true residual b - A x.  With
+  // FP32/BF16 factors the true residual is also checked every 50 iterations
+  // and replaces the recurrence residual if the two have drifted apart.
   const int replace = (h && h->prec != AINV_PREC_FP64) ? 50 : 0;
   return ainv::krylov_solve(h, const_cast<ainv_csr *>(a), b_dev, x_dev, method, eps, itmax,
                             replace, iter, err, (cudaStream_t)stream);

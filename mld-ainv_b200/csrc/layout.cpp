@@ -6,6 +6,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <cstdlib>
 
 #include "internal.h"
 
@@ -100,7 +101,8 @@ HostCsr transpose(const HostCsr &a) {
 }
 
 size_t DevSell::bytes() const {
-  return (size_t)(nslices + 1) * sizeof(int) + (size_t)slots * (sizeof(int) + prec_size(prec));
+  return (size_t)(nslices + 1) * 2 * sizeof(int) + (size_t)nidx * sizeof(int) +
+         (size_t)slots * prec_size(prec);
 }
 
 namespace {
@@ -129,54 +131,174 @@ template <class V>
 int upload_sell_t(const HostCsr &a, int prec, DevSell &out) {
   const int n = a.n;
   const int ns = (n + kSlice - 1) / kSlice;
-  std::vector<int> sptr((size_t)ns + 1, 0);
-  long long slots = 0;
+  // pass 1: per-slice encoding, width and offset list
+  std::vector<char> om((size_t)ns);
+  std::vector<int> width((size_t)ns);
+  std::vector<int> offs_ptr((size_t)ns + 1, 0);
+  std::vector<int> offs_all;
+  std::vector<int> offs;
+  long long base_slots = 0;
   for (int s = 0; s < ns; s++) {
+    const int r0 = s * kSlice, r1 = std::min(n, r0 + kSlice);
     int w = 0;
-    for (int r = s * kSlice; r < std::min(n, (s + 1) * kSlice); r++)
+    offs.clear();
+    for (int r = r0; r < r1; r++) {
       w = std::max(w, a.irp[r + 1] - a.irp[r]);
-    slots += (long long)w * kSlice;
-    if (slots > INT_MAX) {
+      for (int k = a.irp[r]; k < a.irp[r + 1]; k++) offs.push_back(a.ja[k] - r);
+    }
+    std::sort(offs.begin(), offs.end());
+    offs.erase(std::unique(offs.begin(), offs.end()), offs.end());
+    const long long u = (long long)offs.size();
+    const long long cost_off = u * kSlice * (long long)sizeof(V) + u * 4;
+    const long long cost_col = (long long)w * kSlice * (long long)(sizeof(V) + 4);
+    om[s] = u <= kMaxOffsets && cost_off <= cost_col;
+    width[s] = om[s] ? (int)u : w;
+    if (om[s]) offs_all.insert(offs_all.end(), offs.begin(), offs.end());
+    offs_ptr[s + 1] = (int)offs_all.size();
+    base_slots += (long long)width[s] * kSlice;
+  }
+  // pack P: largest power of two with P*sizeof(V) <= 16 and <= 6% padding
+  int P = 1;
+  for (int p = (int)(16 / sizeof(V)); p > 1; p /= 2) {
+    long long padded = 0;
+    for (int s = 0; s < ns; s++) padded += (long long)((width[s] + p - 1) / p * p) * kSlice;
+    if (padded * 100 <= base_slots * 106) {
+      P = p;
+      break;
+    }
+  }
+  // pass 2: fill
+  std::vector<int> sptr((size_t)ns + 1, 0), iptr((size_t)ns + 1, 0);
+  std::vector<int> idx;
+  std::vector<V> val;
+  idx.reserve((size_t)offs_all.size() + 64);
+  val.reserve((size_t)(base_slots + base_slots / 8 + 64));
+  int offset_slices = 0;
+  auto at = [P](int k, int lane) { return (size_t)(k / P) * kSlice * P + (size_t)lane * P + k % P; };
+  for (int s = 0; s < ns; s++) {
+    const int r0 = s * kSlice, r1 = std::min(n, r0 + kSlice);
+    const int wp = (width[s] + P - 1) / P * P;
+    const size_t vbase = val.size();
+    if (vbase + (size_t)wp * kSlice > (size_t)INT_MAX) {
       set_error("sliced layout exceeds 2^31 slots");
       return AINV_ERR_UNSUPPORTED;
     }
-    sptr[s + 1] = (int)slots;
-  }
-  std::vector<int> col((size_t)slots);
-  std::vector<V> val((size_t)slots);
-  for (int s = 0; s < ns; s++) {
-    const int w = (sptr[s + 1] - sptr[s]) / kSlice;
-    for (int lane = 0; lane < kSlice; lane++) {
-      const int r = s * kSlice + lane;
-      const int rr = std::min(r, n - 1);
-      const int beg = r < n ? a.irp[r] : 0, len = r < n ? a.irp[r + 1] - beg : 0;
-      for (int k = 0; k < w; k++) {
-        const size_t at = (size_t)sptr[s] + (size_t)k * kSlice + lane;
-        if (k < len) {
-          col[at] = a.ja[beg + k];
-          val[at] = cast_value<V>(a.val[beg + k]);
-        } else {
-          col[at] = rr;
-          val[at] = cast_value<V>(0.0);
+    val.resize(vbase + (size_t)wp * kSlice, cast_value<V>(0.0));
+    if (om[s]) {
+      offset_slices++;
+      const int *o = offs_all.data() + offs_ptr[s];
+      const int u = offs_ptr[s + 1] - offs_ptr[s];
+      idx.insert(idx.end(), o, o + u);
+      idx.resize(idx.size() + (size_t)(wp - u), 0);  // padding offsets hold value 0
+      for (int r = r0; r < r1; r++) {
+        const int lane = r - r0;
+        for (int k = a.irp[r]; k < a.irp[r + 1]; k++) {
+          const int pos = (int)(std::lower_bound(o, o + u, a.ja[k] - r) - o);
+          val[vbase + at(pos, lane)] = cast_value<V>(a.val[k]);
+        }
+      }
+    } else {
+      const size_t ibase = idx.size();
+      idx.resize(ibase + (size_t)wp * kSlice);
+      for (int lane = 0; lane < kSlice; lane++) {
+        const int r = r0 + lane;
+        const int rr = std::min(r, n - 1);
+        const int beg = r < n ? a.irp[r] : 0, len = r < n ? a.irp[r + 1] - beg : 0;
+        for (int k = 0; k < wp; k++) {
+          const size_t p = at(k, lane);
+          if (k < len) {
+            idx[ibase + p] = a.ja[beg + k];
+            val[vbase + p] = cast_value<V>(a.val[beg + k]);
+          } else {
+            idx[ibase + p] = rr;
+          }
         }
       }
     }
+    if (idx.size() > (size_t)INT_MAX) {
+      set_error("sliced layout exceeds 2^31 index words");
+      return AINV_ERR_UNSUPPORTED;
+    }
+    sptr[s + 1] = (int)val.size();
+    iptr[s + 1] = (int)idx.size();
   }
   DevSell m;
   m.n = n;
   m.nslices = ns;
   m.nnz = a.nnz();
-  m.slots = slots;
+  m.slots = (long long)val.size();
+  m.nidx = (long long)idx.size();
+  m.offset_slices = offset_slices;
+  m.pack = P;
   m.prec = prec;
-  cudaError_t e = cudaMalloc(&m.sptr, sizeof(int) * ((size_t)ns + 1));
-  if (e == cudaSuccess && slots > 0) e = cudaMalloc(&m.col, sizeof(int) * (size_t)slots);
-  if (e == cudaSuccess && slots > 0) e = cudaMalloc(&m.val, sizeof(V) * (size_t)slots);
+  // streaming stages: kConsumerSlices warps, each with 8/sizeof(V) slices,
+  // so a warp's share of a stage is about 1 KB of values at every precision
+  std::vector<StageDesc> stages;
+  const int stage_slices = kConsumerSlices * (int)std::max<size_t>(1, 8 / sizeof(V));
+  {
+    const int nst = (ns + stage_slices - 1) / stage_slices;
+    stages.resize((size_t)nst);
+    for (int st = 0; st < nst; st++) {
+      StageDesc &d = stages[(size_t)st];
+      std::memset(&d, 0, sizeof d);
+      d.s0 = st * stage_slices;
+      d.s1 = std::min(ns, d.s0 + stage_slices);
+      d.vstart = sptr[d.s0];
+      d.vbytes = (int)((sptr[d.s1] - sptr[d.s0]) * sizeof(V));
+      const long long ib0 = (long long)iptr[d.s0] * 4, ib1 = (long long)iptr[d.s1] * 4;
+      d.ibyte0 = ib0 / 16 * 16;
+      d.ibytes = (int)((ib1 + 15) / 16 * 16 - d.ibyte0);
+      // uniform: every slice in offset mode with the same offset list
+      // (AINV_STREAM_NO_WINDOWS=1 disables staging of the gathered windows)
+      static const bool no_windows = std::getenv("AINV_STREAM_NO_WINDOWS") != nullptr;
+      bool uni = !no_windows && om[d.s0] && width[d.s0] > 0 && width[d.s0] <= kStageMaxOffsets;
+      const int *o0 = offs_all.data() + offs_ptr[d.s0];
+      const int u0 = offs_ptr[d.s0 + 1] - offs_ptr[d.s0];
+      for (int s = d.s0 + 1; uni && s < d.s1; s++) {
+        const int u = offs_ptr[s + 1] - offs_ptr[s];
+        uni = om[s] && u == u0 && std::equal(o0, o0 + u0, offs_all.data() + offs_ptr[s]);
+      }
+      // a window must not need bytes past the end of the gathered vector
+      const long long r0 = (long long)d.s0 * kSlice, r1 = std::min<long long>(n, (long long)d.s1 * kSlice);
+      for (int k = 0; uni && k < u0; k++) {
+        const long long hi = std::min<long long>(n, r1 + o0[k]);
+        // each window copy rounds its end up to 16 bytes: it must not pass the
+        // end of a vector of n doubles or of n floats
+        for (long long xs : {4LL, 8LL})
+          if ((hi * xs + 15) / 16 * 16 > (long long)n * xs) uni = false;
+        if (r0 + o0[k] >= n || r1 + o0[k] <= 0) uni = false;
+      }
+      if (uni) {
+        d.noff = u0;
+        for (int k = 0; k < u0; k++) d.off[k] = o0[k];
+      }
+      m.stage_vmax = std::max(m.stage_vmax, d.vbytes);
+      m.stage_imax = std::max(m.stage_imax, d.ibytes);
+      m.stage_noff_max = std::max(m.stage_noff_max, d.noff);
+    }
+    m.nstages = nst;
+    m.stage_slices = stage_slices;
+  }
+  idx.resize(idx.size() + 4, 0);  // tail padding: index copies round up to 16 bytes
+  sptr.resize(sptr.size() + 4, sptr.back());  // and so do the slice-pointer copies
+  iptr.resize(iptr.size() + 4, iptr.back());
+  cudaError_t e = cudaMalloc(&m.sptr, sizeof(int) * sptr.size());
+  if (e == cudaSuccess) e = cudaMalloc(&m.iptr, sizeof(int) * iptr.size());
+  if (e == cudaSuccess && !idx.empty()) e = cudaMalloc(&m.idx, sizeof(int) * idx.size());
+  if (e == cudaSuccess && !stages.empty())
+    e = cudaMalloc(&m.stages, sizeof(StageDesc) * stages.size());
+  if (e == cudaSuccess && !stages.empty())
+    e = cudaMemcpy(m.stages, stages.data(), sizeof(StageDesc) * stages.size(),
+                   cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && !val.empty()) e = cudaMalloc(&m.val, sizeof(V) * val.size());
   if (e == cudaSuccess)
-    e = cudaMemcpy(m.sptr, sptr.data(), sizeof(int) * ((size_t)ns + 1), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess && slots > 0)
-    e = cudaMemcpy(m.col, col.data(), sizeof(int) * (size_t)slots, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess && slots > 0)
-    e = cudaMemcpy(m.val, val.data(), sizeof(V) * (size_t)slots, cudaMemcpyHostToDevice);
+    e = cudaMemcpy(m.sptr, sptr.data(), sizeof(int) * sptr.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(m.iptr, iptr.data(), sizeof(int) * iptr.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && !idx.empty())
+    e = cudaMemcpy(m.idx, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && !val.empty())
+    e = cudaMemcpy(m.val, val.data(), sizeof(V) * val.size(), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
     free_sell(m);
     set_error("device upload of sliced matrix failed: %s", cudaGetErrorString(e));
@@ -200,8 +322,10 @@ int upload_sell(const HostCsr &a, int prec, DevSell &out) {
 }
 
 void free_sell(DevSell &m) {
+  if (m.stages) cudaFree(m.stages);
   if (m.sptr) cudaFree(m.sptr);
-  if (m.col) cudaFree(m.col);
+  if (m.iptr) cudaFree(m.iptr);
+  if (m.idx) cudaFree(m.idx);
   if (m.val) cudaFree(m.val);
   m = DevSell{};
 }

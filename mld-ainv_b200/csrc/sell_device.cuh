@@ -1,5 +1,5 @@
-// Device helpers shared by the SELL-32 kernels (apply sweeps, A SpMV and
-// the fused Krylov kernels).
+// Device helpers shared by the sliced-layout kernels (apply sweeps, A SpMV
+// and the fused Krylov kernels).
 #pragma once
 
 #include <cuda_bf16.h>
@@ -34,61 +34,342 @@ __device__ __forceinline__ float ldd(const __nv_bfloat16 *p) {
   return __uint_as_float(((unsigned)u) << 16);
 }
 
-// Sequential (slot-ordered) dot of one SELL row with a gathered vector.
-// Indices and values for kUnroll slots are issued before the dependent
-// gathers so each lane keeps several independent requests in flight.
-template <class V, class X>
-__device__ __forceinline__ typename Acc<V>::type row_dot(const int *__restrict__ col,
-                                                         const V *__restrict__ val,
-                                                         const X *__restrict__ x, int w) {
-  using A = typename Acc<V>::type;
-  A acc = A(0);
-  int k = 0;
-  for (; k + kUnroll <= w; k += kUnroll) {
-    int c[kUnroll];
-    A v[kUnroll], xv[kUnroll];
-#pragma unroll
-    for (int u = 0; u < kUnroll; u++) {
-      c[u] = __ldcs(col + (k + u) * kSlice);
-      v[u] = (A)ldv(val + (k + u) * kSlice);
-    }
-#pragma unroll
-    for (int u = 0; u < kUnroll; u++) xv[u] = (A)__ldg(x + c[u]);
-#pragma unroll
-    for (int u = 0; u < kUnroll; u++) acc = fma(v[u], xv[u], acc);
-  }
-  for (; k < w; k++) {
-    const int c = __ldcs(col + k * kSlice);
-    acc = fma((A)ldv(val + k * kSlice), (A)__ldg(x + c), acc);
-  }
-  return acc;
+// Kernel-side view of a DevSell with typed values.
+template <class V>
+struct SellView {
+  int n, nslices;
+  const int *__restrict__ sptr;
+  const int *__restrict__ iptr;
+  const int *__restrict__ idx;
+  const V *__restrict__ val;
+};
+template <class V>
+inline SellView<V> view(const DevSell &m) {
+  return SellView<V>{m.n, m.nslices, m.sptr, m.iptr, m.idx, (const V *)m.val};
 }
 
-// Slice geometry for the calling thread: returns false when the warp has no
-// slice.  row may be >= n for the tail lanes of the last slice.
-struct SliceCtx {
-  int beg, w, row, lane;
+// ---- packed loads: P adjacent slots of one lane in one vector load --------
+__device__ __forceinline__ float bf16lo(unsigned w) { return __uint_as_float(w << 16); }
+__device__ __forceinline__ float bf16hi(unsigned w) { return __uint_as_float(w & 0xffff0000u); }
+
+template <class V, int P>
+struct Pack;
+template <>
+struct Pack<double, 1> {
+  static __device__ __forceinline__ void load(const double *p, double (&o)[1]) { o[0] = __ldcs(p); }
 };
-__device__ __forceinline__ bool slice_ctx(int nslices, const int *__restrict__ sptr,
-                                          SliceCtx &c) {
-  const int s = blockIdx.x * kSlicesPerBlock + (threadIdx.x >> 5);
-  if (s >= nslices) return false;
-  c.lane = threadIdx.x & (kSlice - 1);
-  c.beg = __ldg(sptr + s);
-  c.w = (__ldg(sptr + s + 1) - c.beg) / kSlice;
-  c.row = s * kSlice + c.lane;
-  return true;
+template <>
+struct Pack<double, 2> {
+  static __device__ __forceinline__ void load(const double *p, double (&o)[2]) {
+    const double2 v = __ldcs(reinterpret_cast<const double2 *>(p));
+    o[0] = v.x;
+    o[1] = v.y;
+  }
+};
+template <>
+struct Pack<float, 1> {
+  static __device__ __forceinline__ void load(const float *p, float (&o)[1]) { o[0] = __ldcs(p); }
+};
+template <>
+struct Pack<float, 2> {
+  static __device__ __forceinline__ void load(const float *p, float (&o)[2]) {
+    const float2 v = __ldcs(reinterpret_cast<const float2 *>(p));
+    o[0] = v.x;
+    o[1] = v.y;
+  }
+};
+template <>
+struct Pack<float, 4> {
+  static __device__ __forceinline__ void load(const float *p, float (&o)[4]) {
+    const float4 v = __ldcs(reinterpret_cast<const float4 *>(p));
+    o[0] = v.x;
+    o[1] = v.y;
+    o[2] = v.z;
+    o[3] = v.w;
+  }
+};
+template <>
+struct Pack<__nv_bfloat16, 1> {
+  static __device__ __forceinline__ void load(const __nv_bfloat16 *p, float (&o)[1]) {
+    o[0] = bf16lo(__ldcs(reinterpret_cast<const unsigned short *>(p)));
+  }
+};
+template <>
+struct Pack<__nv_bfloat16, 2> {
+  static __device__ __forceinline__ void load(const __nv_bfloat16 *p, float (&o)[2]) {
+    const unsigned v = __ldcs(reinterpret_cast<const unsigned *>(p));
+    o[0] = bf16lo(v);
+    o[1] = bf16hi(v);
+  }
+};
+template <>
+struct Pack<__nv_bfloat16, 4> {
+  static __device__ __forceinline__ void load(const __nv_bfloat16 *p, float (&o)[4]) {
+    const uint2 v = __ldcs(reinterpret_cast<const uint2 *>(p));
+    o[0] = bf16lo(v.x);
+    o[1] = bf16hi(v.x);
+    o[2] = bf16lo(v.y);
+    o[3] = bf16hi(v.y);
+  }
+};
+template <>
+struct Pack<__nv_bfloat16, 8> {
+  static __device__ __forceinline__ void load(const __nv_bfloat16 *p, float (&o)[8]) {
+    const uint4 v = __ldcs(reinterpret_cast<const uint4 *>(p));
+    o[0] = bf16lo(v.x);
+    o[1] = bf16hi(v.x);
+    o[2] = bf16lo(v.y);
+    o[3] = bf16hi(v.y);
+    o[4] = bf16lo(v.z);
+    o[5] = bf16hi(v.z);
+    o[6] = bf16lo(v.w);
+    o[7] = bf16hi(v.w);
+  }
+};
+
+// P adjacent int32 words: streaming (per-slot columns) or cached (offsets).
+template <int P, bool STREAM>
+__device__ __forceinline__ void load_ints(const int *p, int (&o)[P]) {
+  if constexpr (P == 1) {
+    o[0] = STREAM ? __ldcs(p) : __ldg(p);
+  } else if constexpr (P == 2) {
+    const int2 v = STREAM ? __ldcs(reinterpret_cast<const int2 *>(p))
+                          : __ldg(reinterpret_cast<const int2 *>(p));
+    o[0] = v.x;
+    o[1] = v.y;
+  } else {
+#pragma unroll
+    for (int h = 0; h < P / 4; h++) {
+      const int4 v = STREAM ? __ldcs(reinterpret_cast<const int4 *>(p) + h)
+                            : __ldg(reinterpret_cast<const int4 *>(p) + h);
+      o[4 * h] = v.x;
+      o[4 * h + 1] = v.y;
+      o[4 * h + 2] = v.z;
+      o[4 * h + 3] = v.w;
+    }
+  }
+}
+
+// Packs a value type can use (at most 16 bytes per load).
+template <class V, int P>
+constexpr bool pack_ok() {
+  return P == 1 || (P * (int)sizeof(V) <= 16 && (P == 2 || P == 4 || P == 8));
+}
+
+// Call f.template run<S, P>() for the runtime S (1, 2, 4) and P.
+template <class V, int S, class F>
+inline bool with_pack(int P, const F &f) {
+  switch (P) {
+    case 1: f.template run<S, 1>(); return true;
+    case 2: if constexpr (pack_ok<V, 2>()) { f.template run<S, 2>(); return true; } break;
+    case 4: if constexpr (pack_ok<V, 4>()) { f.template run<S, 4>(); return true; } break;
+    case 8: if constexpr (pack_ok<V, 8>()) { f.template run<S, 8>(); return true; } break;
+  }
+  return false;
+}
+template <class V, class F>
+inline bool with_group_pack(int S, int P, const F &f) {
+  switch (S) {
+    case 1: return with_pack<V, 1>(P, f);
+    case 4: return with_pack<V, 4>(P, f);
+    default: return with_pack<V, 2>(P, f);
+  }
+}
+
+// Warp-level slice loop: warp w of block b takes slices b*8+w, then every
+// gridDim.x*8-th slice after it.
+__device__ __forceinline__ int first_slice() {
+  return blockIdx.x * kSlicesPerBlock + (threadIdx.x >> 5);
+}
+__device__ __forceinline__ int slice_stride() { return gridDim.x * kSlicesPerBlock; }
+
+// ---- groups of S slices per warp ------------------------------------------
+// A warp walks its slices S at a time: the S+1 slice pointers come from one
+// lane-parallel load, and every value / offset load of the S slices (kUnroll
+// slots each) is issued before the first dependent gather, so a warp keeps
+// S*kUnroll independent 256 B requests in flight instead of waiting for
+// three dependent round trips per slice.
+template <int S>
+struct GroupCtx {
+  int vb[S], ib[S], w[S];
+  bool om[S];
+  int maxw;
+};
+
+template <class V, int S>
+__device__ __forceinline__ void group_ctx(const SellView<V> &m, int g, GroupCtx<S> &c) {
+  const int lane = threadIdx.x & 31;
+  int sp = 0, ip = 0;
+  if (lane <= S) {
+    const int s = min(g * S + lane, m.nslices);
+    sp = __ldg(m.sptr + s);
+    ip = __ldg(m.iptr + s);
+  }
+  c.maxw = 0;
+#pragma unroll
+  for (int q = 0; q < S; q++) {
+    const int vb = __shfl_sync(0xffffffffu, sp, q), ve = __shfl_sync(0xffffffffu, sp, q + 1);
+    const int ib = __shfl_sync(0xffffffffu, ip, q), ie = __shfl_sync(0xffffffffu, ip, q + 1);
+    c.vb[q] = vb;
+    c.ib[q] = ib;
+    c.w[q] = (ve - vb) / kSlice;
+    c.om[q] = (ie - ib) == c.w[q];
+    c.maxw = max(c.maxw, c.w[q]);
+  }
+}
+
+// Packs per loop step: 4 slots for P <= 4, one pack for P = 8.
+template <int P>
+struct Step { static constexpr int kPacks = P >= 4 ? 1 : 4 / P; };
+
+// Slots [k0, k0 + kPacks*P) of the S slices of a group, all in the same
+// index encoding (OM: shared offsets; else per-slot columns).  Loads are
+// predicated per pack (w is a multiple of P), so all value / index loads of
+// the step are in flight before the first dependent gather; the FMAs then
+// run in slot order, which is the row's column order.
+template <bool OM, int P, class V, class X, int S>
+__device__ __forceinline__ void group_slots(const SellView<V> &m, const GroupCtx<S> &c,
+                                            const int (&row)[S], int k0,
+                                            const X *__restrict__ x,
+                                            typename Acc<V>::type (&acc)[S]) {
+  using A = typename Acc<V>::type;
+  constexpr int J = Step<P>::kPacks;
+  const int lane = threadIdx.x & 31;
+  int col[S][J][P];
+  A vv[S][J][P];
+#pragma unroll
+  for (int q = 0; q < S; q++) {
+#pragma unroll
+    for (int j = 0; j < J; j++) {
+      const int k = k0 + j * P;
+      const bool ok = k < c.w[q];
+      const size_t pos = (size_t)(k / P) * (kSlice * P) + (size_t)lane * P;
+      if (ok) {
+        Pack<V, P>::load(m.val + c.vb[q] + pos, vv[q][j]);
+        if (OM) {
+          load_ints<P, false>(m.idx + c.ib[q] + k, col[q][j]);
+#pragma unroll
+          for (int e = 0; e < P; e++) col[q][j][e] += row[q];
+        } else {
+          load_ints<P, true>(m.idx + c.ib[q] + pos, col[q][j]);
+        }
+      } else {
+#pragma unroll
+        for (int e = 0; e < P; e++) {
+          vv[q][j][e] = A(0);
+          col[q][j][e] = 0;
+        }
+      }
+    }
+  }
+  A xv[S][J][P];
+#pragma unroll
+  for (int q = 0; q < S; q++)
+#pragma unroll
+    for (int j = 0; j < J; j++)
+#pragma unroll
+      for (int e = 0; e < P; e++)
+        xv[q][j][e] = (vv[q][j][e] != A(0) && (unsigned)col[q][j][e] < (unsigned)m.n)
+                          ? (A)__ldg(x + col[q][j][e])
+                          : A(0);
+#pragma unroll
+  for (int q = 0; q < S; q++)
+#pragma unroll
+    for (int j = 0; j < J; j++)
+#pragma unroll
+      for (int e = 0; e < P; e++) acc[q] = fma(vv[q][j][e], xv[q][j][e], acc[q]);
+}
+
+// acc[q] = row (g*S+q)*32+lane of M dotted with x.  The encoding test is
+// warp-uniform and sits outside the slot loop; a group mixing both
+// encodings is walked one slice at a time.
+template <int P, class V, class X, int S>
+__device__ __forceinline__ void group_dot(const SellView<V> &m, const GroupCtx<S> &c, int g,
+                                          const X *__restrict__ x,
+                                          typename Acc<V>::type (&acc)[S]) {
+  using A = typename Acc<V>::type;
+  constexpr int KS = Step<P>::kPacks * P;
+  const int lane = threadIdx.x & 31;
+  int row[S];
+  bool all_om = true, all_col = true;
+#pragma unroll
+  for (int q = 0; q < S; q++) {
+    acc[q] = A(0);
+    row[q] = (g * S + q) * kSlice + lane;
+    if (c.w[q] > 0) {
+      all_om = all_om && c.om[q];
+      all_col = all_col && !c.om[q];
+    }
+  }
+  if (all_om) {
+    for (int k0 = 0; k0 < c.maxw; k0 += KS) group_slots<true, P>(m, c, row, k0, x, acc);
+  } else if (all_col) {
+    for (int k0 = 0; k0 < c.maxw; k0 += KS) group_slots<false, P>(m, c, row, k0, x, acc);
+  } else {
+#pragma unroll
+    for (int q = 0; q < S; q++) {
+      GroupCtx<1> c1;
+      c1.vb[0] = c.vb[q];
+      c1.ib[0] = c.ib[q];
+      c1.w[0] = c.w[q];
+      c1.om[0] = c.om[q];
+      c1.maxw = c.w[q];
+      const int r1[1] = {row[q]};
+      A a1[1] = {A(0)};
+      if (c.om[q]) {
+        for (int k0 = 0; k0 < c1.maxw; k0 += KS) group_slots<true, P>(m, c1, r1, k0, x, a1);
+      } else {
+        for (int k0 = 0; k0 < c1.maxw; k0 += KS) group_slots<false, P>(m, c1, r1, k0, x, a1);
+      }
+      acc[q] = a1[0];
+    }
+  }
+}
+
+// Visit every row of M: epi(row, acc) for rows < n, S slices per warp step,
+// warps striding over the grid.
+template <int S, int P, class V, class X, class Epi>
+__device__ __forceinline__ void for_each_row(const SellView<V> &m, const X *__restrict__ x,
+                                             Epi &&epi) {
+  const int ngroups = (m.nslices + S - 1) / S;
+  const int lane = threadIdx.x & 31;
+  for (int g = first_slice(); g < ngroups; g += slice_stride()) {
+    GroupCtx<S> c;
+    group_ctx(m, g, c);
+    typename Acc<V>::type acc[S];
+    group_dot<P>(m, c, g, x, acc);
+#pragma unroll
+    for (int q = 0; q < S; q++) {
+      const int row = (g * S + q) * kSlice + lane;
+      if (row < m.n) epi(row, acc[q]);
+    }
+  }
 }
 
 inline int grid_for(int nslices) { return (nslices + kSlicesPerBlock - 1) / kSlicesPerBlock; }
 
+// Slices per warp step (S of group_dot) for a value type; the default can
+// be overridden with AINV_SLICES_PER_WARP=1|2|4 for tuning.
+int group_size(int prec);
+inline int grid_for_groups(int nslices, int S) {
+  return grid_for((nslices + S - 1) / S);
+}
+
+// Blocks for kernels that end in a grid-wide reduction: at most one resident
+// wave (8 blocks of 256 threads per SM) so the last block folds few
+// partials; never more blocks than units of 256 rows.
+int reduction_grid(long long rows);
+
 // ---- deterministic block reduction --------------------------------------
-// Fixed shuffle tree inside each warp, then warp 0 folds the kWarps
-// partials in index order.  The result is valid in thread 0.
+// Fixed shuffle tree inside each warp, then thread 0 folds the per-warp
+// partials of every warp of the block in index order.  Works for any block
+// size up to 1024 threads; the result is valid in thread 0.
+constexpr int kMaxWarps = 32;
 template <int NV>
 __device__ __forceinline__ void block_sum(double (&v)[NV]) {
-  __shared__ double sh[NV][kWarps];
+  __shared__ double sh[NV][kMaxWarps];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nwarps = (blockDim.x + 31) >> 5;
 #pragma unroll
   for (int i = 0; i < NV; i++) {
 #pragma unroll
@@ -103,7 +384,7 @@ __device__ __forceinline__ void block_sum(double (&v)[NV]) {
 #pragma unroll
     for (int i = 0; i < NV; i++) {
       double s = 0.0;
-      for (int w = 0; w < kWarps; w++) s += sh[i][w];
+      for (int w = 0; w < nwarps; w++) s += sh[i][w];
       v[i] = s;
     }
   }
@@ -111,9 +392,10 @@ __device__ __forceinline__ void block_sum(double (&v)[NV]) {
 }
 
 // Grid-wide deterministic sum: every block stores its partials, the last
-// block to arrive (ticket) folds all partials in block order.  Returns true
-// in the last block, where thread 0 holds the totals in v.  The ticket is
-// reset by the last block so the slot can be reused by the next launch.
+// block to arrive (atomic ticket, no waiting) folds all partials in block
+// order.  Returns true in the last block, where thread 0 holds the totals in
+// v.  The ticket is reset by the last block so the slot can be reused by the
+// next launch.
 template <int NV>
 __device__ __forceinline__ bool grid_sum(double (&v)[NV], double *__restrict__ partials,
                                          unsigned *__restrict__ ticket) {
@@ -133,7 +415,7 @@ __device__ __forceinline__ bool grid_sum(double (&v)[NV], double *__restrict__ p
 #pragma unroll
   for (int i = 0; i < NV; i++) {
     double s = 0.0;
-    for (int b = threadIdx.x; b < G; b += kBlock) s += __ldcg(partials + i * G + b);
+    for (int b = threadIdx.x; b < G; b += blockDim.x) s += __ldcg(partials + i * G + b);
     v[i] = s;
   }
   block_sum<NV>(v);

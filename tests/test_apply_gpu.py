@@ -204,3 +204,48 @@ def test_cnv_changes_precision():
     for p in ["BF16", "FP32", "FP64"]:
         assert sv.cnv(p) == 0
         assert sv.device.prec == p
+
+
+def _random_unit_triangular(n, per_row, lower, seed):
+    """Random unit-triangular CSR with scattered columns (no shared offsets)."""
+    rng = np.random.default_rng(seed)
+    irp, ja, val = [0], [], []
+    for i in range(n):
+        pool = np.arange(0, i) if lower else np.arange(i + 1, n)
+        k = min(len(pool), int(rng.integers(0, per_row + 1)))
+        cols = sorted(rng.choice(pool, size=k, replace=False).tolist()) if k else []
+        row = (cols + [i]) if lower else ([i] + cols)
+        vals = [1.0 if c == i else float(rng.uniform(-0.5, 0.5)) for c in row]
+        ja += row
+        val += vals
+        irp.append(len(ja))
+    return np.array(irp, np.int32), np.array(ja, np.int32), np.array(val)
+
+
+@pytest.mark.parametrize("trans", ["N", "T"])
+def test_apply_column_mode_random_factors(trans):
+    """Scattered patterns force the per-entry column encoding."""
+    n = 3000
+    wt = _random_unit_triangular(n, 9, True, 1)
+    z = _random_unit_triangular(n, 9, False, 2)
+    d = ainv.pde.rand_uniform(3, n, 0.5, 2.0)
+    f = dict(wt_irp=wt[0], wt_ja=wt[1], wt_val=wt[2], z_irp=z[0], z_ja=z[1], z_val=z[2], d=d)
+    df = device_factors(f)
+    for which in ("wt", "z", "zt", "w"):
+        lay = df.layout_info(which)
+        assert lay["offset_slices"] < lay["nslices"] // 4, lay   # mostly column mode
+    x, y0 = ainv.pde.rand_uniform(4, n), ainv.pde.rand_uniform(5, n)
+    y = _gpu_apply(df, x, 0.75, -1.5, y0, trans)
+    ref = O.ainv_apply(oracle_factors(f), x, 0.75, -1.5, y0, trans)
+    assert relerr(y, ref) <= 1e-12
+
+
+def test_stencil_factors_use_offset_mode():
+    irp, ja, val = ainv.pde.gen_pde3d(40, "convdiff", (10 / np.sqrt(3),) * 3)
+    f = build_factors(irp, ja, val)
+    df = device_factors(f)
+    for which in ("wt", "z", "zt", "w"):
+        lay = df.layout_info(which)
+        assert lay["offset_slices"] == lay["nslices"]
+        assert lay["nidx"] <= 8 * lay["nslices"]          # a few offsets per slice
+        assert lay["slots"] <= 1.02 * 4 * 64000 + 32 * 4   # ~4 slots per row

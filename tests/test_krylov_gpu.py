@@ -27,6 +27,25 @@ def _within5(gpu_it, ref_it):
     return abs(gpu_it - ref_it) <= max(1, int(np.ceil(0.05 * ref_it)))
 
 
+def _oracle_spread(method, a, of, b, eps, itmax, k=6):
+    """Iteration counts of the oracle solve on b and on k copies of b perturbed
+    at rounding level (1e-15 relative).  BiCGSTAB's count moves by up to ~10%
+    under such perturbations at these sizes, so parity is judged against this
+    spread: GPU count within 5% of [min, max]."""
+    rng = np.random.default_rng(7)
+    its = []
+    for j in range(k + 1):
+        bj = b if j == 0 else b * (1.0 + 1e-15 * rng.standard_normal(len(b)))
+        _, it, _, rc = O.solve(method, a, of, bj, eps=eps, itmax=itmax)
+        assert rc == 0
+        its.append(it)
+    return min(its), max(its)
+
+
+def _within_spread(gpu_it, lo, hi):
+    return lo - max(1, np.ceil(0.05 * lo)) <= gpu_it <= hi + max(1, np.ceil(0.05 * hi))
+
+
 def test_cg_poisson_40():
     """40^3 Poisson, b = A*1, x0 = 0, AINV LLK drop 0.1 cap 20, CG to 1e-9."""
     irp, ja, val = ainv.pde.gen_pde3d(40, "poisson")
@@ -36,11 +55,12 @@ def test_cg_poisson_40():
     b = O.spmv(a, np.ones(n))
     xr, it_ref, err_ref, rc = O.solve("CG", a, oracle_factors(f), b, eps=1e-9, itmax=1000)
     assert rc == 0
+    lo, hi = _oracle_spread("CG", a, oracle_factors(f), b, 1e-9, 1000)
     A = ainv.DeviceOperator(irp, ja, val)
     x = torch.zeros(n, dtype=torch.float64, device=DEV)
     res = A.solve(_t(b), x, device_factors(f), "CG", 1e-9, 1000)
     assert res.converged, res
-    assert _within5(res.iter, it_ref), (res.iter, it_ref)
+    assert _within_spread(res.iter, lo, hi), (res.iter, it_ref, lo, hi)
     xs = x.cpu().numpy()
     assert res.err <= 1e-9
     assert _true_relres(irp, ja, val, xs, b) <= 1.05e-9
@@ -56,13 +76,12 @@ def test_bicgstab_convdiff(idim):
     a = O.CSR(n, irp, ja, val)
     xstar = ainv.pde.rand_uniform(0, n)
     b = O.spmv(a, xstar)
-    _, it_ref, _, rc = O.solve("BICGSTAB", a, oracle_factors(f), b, eps=1e-9, itmax=2000)
-    assert rc == 0
+    lo, hi = _oracle_spread("BICGSTAB", a, oracle_factors(f), b, 1e-9, 2000)
     A = ainv.DeviceOperator(irp, ja, val)
     x = torch.zeros(n, dtype=torch.float64, device=DEV)
     res = A.solve(_t(b), x, device_factors(f), "BICGSTAB", 1e-9, 2000)
     assert res.converged, res
-    assert _within5(res.iter, it_ref), (res.iter, it_ref)
+    assert _within_spread(res.iter, lo, hi), (res.iter, lo, hi)
     assert _true_relres(irp, ja, val, x.cpu().numpy(), b) <= 1.05e-9
 
 
@@ -80,6 +99,20 @@ def test_mixed_factors_reach_fp64_tolerance(prec):
     res = A.solve(_t(b), x, device_factors(f, prec), "BICGSTAB", 1e-9, 2000)
     assert res.converged, res
     assert _true_relres(irp, ja, val, x.cpu().numpy(), b) <= 2e-9
+
+
+def test_unpreconditioned_bicgstab_count():
+    """No preconditioner: the device loop alone against the oracle's spread."""
+    irp, ja, val = ainv.pde.gen_pde3d(64, "convdiff", (10 / np.sqrt(3),) * 3)
+    n = len(irp) - 1
+    a = O.CSR(n, irp, ja, val)
+    b = O.spmv(a, ainv.pde.rand_uniform(0, n))
+    ident = O.CSR(n, np.arange(n + 1, dtype=np.int32), np.arange(n, dtype=np.int32), np.ones(n))
+    lo, hi = _oracle_spread("BICGSTAB", a, O.Factors(ident, ident, np.ones(n)), b, 1e-9, 3000)
+    A = ainv.DeviceOperator(irp, ja, val)
+    x = torch.zeros(n, dtype=torch.float64, device=DEV)
+    res = A.solve(_t(b), x, None, "BICGSTAB", 1e-9, 3000)
+    assert res.converged and _within_spread(res.iter, lo, hi), (res, lo, hi)
 
 
 def test_unpreconditioned_cg_matches_oracle_count():
@@ -137,6 +170,27 @@ def test_solve_is_deterministic_and_reuses_graph():
         xs.append(x.cpu().numpy())
     np.testing.assert_array_equal(xs[0], xs[1])
     np.testing.assert_array_equal(xs[0], xs[2])
+
+
+def test_reported_error_is_the_true_residual():
+    """Convergence is confirmed on b - A x: the returned err is the true one."""
+    irp, ja, val = ainv.pde.gen_pde3d(28, "convdiff", (10 / np.sqrt(3),) * 3)
+    n = len(irp) - 1
+    f = build_factors(irp, ja, val)
+    b = O.spmv(O.CSR(n, irp, ja, val), ainv.pde.rand_uniform(0, n))
+    A = ainv.DeviceOperator(irp, ja, val)
+    for method in ("BICGSTAB", "CG"):
+        if method == "CG":   # CG on the SPD Poisson operator
+            irp, ja, val = ainv.pde.gen_pde3d(28, "poisson")
+            f = build_factors(irp, ja, val)
+            A = ainv.DeviceOperator(irp, ja, val)
+            b = O.spmv(O.CSR(n, irp, ja, val), ainv.pde.rand_uniform(0, n))
+        x = torch.zeros(n, dtype=torch.float64, device=DEV)
+        res = A.solve(_t(b), x, device_factors(f, "FP32"), method, 1e-10, 2000)
+        assert res.converged
+        true = _true_relres(irp, ja, val, x.cpu().numpy(), b)
+        assert true <= 1e-10
+        assert abs(res.err - true) <= 1e-3 * true
 
 
 def test_spmv_matches_oracle():
