@@ -19,4 +19,13 @@ constexpr int kAlgMLK = 4;      // 'MLK'
 int ainv_biconjg_build(const HostCsr &a, int alg, int fill_in, double thresh, HostCsr &wt,
                        HostCsr &z, std::vector<double> &d);
 
+// INVK: ILU(fill1) then level-fill2 sparse inverses of U and L.
+int invk_build(const HostCsr &a, int fill1, int fill2, HostCsr &wt, HostCsr &z,
+               std::vector<double> &d);
+
+// INVT: ILUT(fill, thresh) with maxval scaling, then sparse inverses of U
+// and L with (invfill, invthresh).
+int invt_build(const HostCsr &a, int fill, double thresh, int invfill, double invthresh,
+               HostCsr &wt, HostCsr &z, std::vector<double> &d);
+
 }  // namespace ainv

@@ -226,10 +226,13 @@ int mld_d_solver_build(mld_d_solver *sv, int n, const int *irp, const int *ja,
       return AINV_ERR_UNSUPPORTED;
     }
     rc = ainv::ainv_biconjg_build(a, sv->alg, sv->fill_in, sv->thresh, sv->wt, sv->z, sv->d);
+  } else if (sv->kind == kInvk) {
+    // src/impl/mld_d_invk_solver_bld.f90:68-69: (fill_in, inv_fill) -> (w, d, z)
+    rc = ainv::invk_build(a, sv->fill_in, sv->inv_fill, sv->wt, sv->z, sv->d);
   } else {
-    ainv::set_error("%s build is not built into this library",
-                    sv->kind == kInvk ? "INVK" : "INVT");
-    return AINV_ERR_UNSUPPORTED;
+    // src/impl/mld_d_invt_solver_bld.f90:68-70
+    rc = ainv::invt_build(a, sv->fill_in, sv->thresh, sv->inv_fill, sv->inv_thresh, sv->wt,
+                          sv->z, sv->d);
   }
   if (rc != AINV_SUCCESS) return rc;
   sv->built = true;

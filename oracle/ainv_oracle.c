@@ -558,3 +558,494 @@ int orc_get_threads(void) {
   return 1;
 #endif
 }
+
+/* ====================================================================
+ * INVK / INVT factor construction.
+ *
+ * The incomplete factorisations are MLD2P4's mld_iluk_fact and
+ * mld_ilut_fact (MLD2P4 >= 2.1.1, not vendored in the reference), restated
+ * from their published IKJ row algorithm: the row of A is loaded into a
+ * dense work row, an ascending index heap drives the elimination, L keeps
+ * the multipliers row(k)*d(k), U is stored divided by the pivot, neither
+ * stores its unit diagonal, and d holds the inverted pivots.  ILUT scales A
+ * by 1/max|a_ij| (iscale = maxval, src/impl/mld_d_invt_bld.f90:108-109),
+ * drops against thresh * ||scaled row||_2 and keeps nlw+fill / nup+fill
+ * entries per triangle (always including the largest original upper
+ * entry); its pivots are mapped back to A by the same weight.
+ * The sparse inverses follow the plugin:
+ *   mld_dsparse_invk  src/impl/mld_dsparse_invk.f90:88-146
+ *   invk_copyin/inv/copyout  src/impl/mld_d_invk_{copyin,inv,copyout}.f90
+ *   mld_dsparse_invt  src/impl/mld_dsparse_invt.f90:96-144
+ *   invt_copyin/inv/copyout  src/impl/mld_d_invt_{copyin,inv,copyout}.f90
+ * ==================================================================== */
+
+typedef struct {
+  int n;
+  int *irp, *ja, *lev;
+  double *val;
+  long nnz, cap;
+} gcsr; /* growable CSR, rows appended in order */
+
+static void g_init(gcsr *m, int n, int with_lev) {
+  m->n = n;
+  m->irp = (int *)calloc((size_t)n + 1, sizeof(int));
+  m->cap = 1024;
+  m->nnz = 0;
+  m->ja = (int *)malloc(sizeof(int) * (size_t)m->cap);
+  m->val = (double *)malloc(sizeof(double) * (size_t)m->cap);
+  m->lev = with_lev ? (int *)malloc(sizeof(int) * (size_t)m->cap) : NULL;
+}
+static void g_push(gcsr *m, int j, double v, int lev) {
+  if (m->nnz == m->cap) {
+    m->cap *= 2;
+    m->ja = (int *)realloc(m->ja, sizeof(int) * (size_t)m->cap);
+    m->val = (double *)realloc(m->val, sizeof(double) * (size_t)m->cap);
+    if (m->lev) m->lev = (int *)realloc(m->lev, sizeof(int) * (size_t)m->cap);
+  }
+  m->ja[m->nnz] = j;
+  m->val[m->nnz] = v;
+  if (m->lev) m->lev[m->nnz] = lev;
+  m->nnz++;
+}
+static void g_free(gcsr *m) {
+  free(m->irp); free(m->ja); free(m->val); free(m->lev);
+  memset(m, 0, sizeof(*m));
+}
+static void g_transpose(const gcsr *a, gcsr *t) {
+  g_init(t, a->n, 0);
+  long nnz = a->nnz > 0 ? a->nnz : 1;
+  free(t->ja); free(t->val);
+  t->ja = (int *)malloc(sizeof(int) * (size_t)nnz);
+  t->val = (double *)malloc(sizeof(double) * (size_t)nnz);
+  t->cap = nnz;
+  t->nnz = a->nnz;
+  csr_transpose(a->n, a->irp, a->ja, a->val, t->irp, t->ja, t->val);
+}
+
+/* reference BLAS dnrm2: one-pass scaled sum of squares */
+static double o_dnrm2(int n, const double *x) {
+  double scale = 0.0, ssq = 1.0;
+  for (int i = 0; i < n; i++) {
+    if (x[i] != 0.0) {
+      double absxi = fabs(x[i]);
+      if (scale < absxi) {
+        ssq = 1.0 + ssq * ((scale / absxi) * (scale / absxi));
+        scale = absxi;
+      } else {
+        ssq = ssq + (absxi / scale) * (absxi / scale);
+      }
+    }
+  }
+  return scale * sqrt(ssq);
+}
+
+/* insertion sort of (xwid, xw) pairs by xwid: psb_msort on distinct keys */
+static void sort_pairs(int nz, int *xwid, double *xw) {
+  for (int a = 1; a < nz; a++) {
+    int kid = xwid[a];
+    double kv = xw[a];
+    int b = a - 1;
+    while (b >= 0 && xwid[b] > kid) {
+      xwid[b + 1] = xwid[b];
+      xw[b + 1] = xw[b];
+      b--;
+    }
+    xwid[b + 1] = kid;
+    xw[b + 1] = kv;
+  }
+}
+
+/* ILU(k), ialg = ILU(n): returns 0, or -(i+1) for a too-small pivot */
+static int o_iluk(int n, const int *irp, const int *ja, const double *val,
+                  int fill, gcsr *L, gcsr *U, double *d) {
+  double *row = (double *)calloc((size_t)n, sizeof(double));
+  int *rowlevs = (int *)malloc(sizeof(int) * (size_t)n);
+  int *idxs = (int *)malloc(sizeof(int) * (size_t)n);
+  iheap heap = {0};
+  int rc = 0;
+  for (int j = 0; j < n; j++) rowlevs[j] = -(n + 1);
+  g_init(L, n, 0);
+  g_init(U, n, 1);
+  for (int i = 0; i < n && rc == 0; i++) {
+    heap.n = 0;
+    for (int p = irp[i]; p < irp[i + 1]; p++) {
+      row[ja[p]] = val[p];
+      rowlevs[ja[p]] = 0;
+      ih_push(&heap, ja[p]);
+    }
+    int nidx = 0, lastk = -1, k;
+    while (ih_pop(&heap, &k) == 0) {
+      if (k == lastk) continue;
+      lastk = k;
+      idxs[nidx++] = k;
+      if (row[k] != 0.0 && rowlevs[k] <= fill && k < i) {
+        double rwk = row[k];
+        int lrwk = rowlevs[k];
+        row[k] = row[k] * d[k];
+        for (long jj = U->irp[k]; jj < U->irp[k + 1]; jj++) {
+          int j = U->ja[jj];
+          if (rowlevs[j] < 0) {
+            ih_push(&heap, j);
+            rowlevs[j] = abs(rowlevs[j]);
+          }
+          row[j] = row[j] - rwk * U->val[jj];
+          int nl = lrwk + U->lev[jj] + 1;
+          if (nl < rowlevs[j]) rowlevs[j] = nl;
+        }
+      }
+    }
+    d[i] = 0.0;
+    for (int p = 0; p < nidx; p++) {
+      int j = idxs[p];
+      if (j < i) {
+        if (rowlevs[j] <= fill) g_push(L, j, row[j], 0);
+      } else if (j == i) {
+        d[i] = d[i] + row[i];
+      } else {
+        if (rowlevs[j] <= fill) g_push(U, j, row[j], rowlevs[j]);
+      }
+      row[j] = 0.0;
+      rowlevs[j] = -(n + 1);
+    }
+    L->irp[i + 1] = (int)L->nnz;
+    U->irp[i + 1] = (int)U->nnz;
+    if (fabs(d[i]) < ORC_EPSTOL) {
+      rc = -(i + 1);
+    } else {
+      d[i] = 1.0 / d[i];
+      for (long p = U->irp[i]; p < U->irp[i + 1]; p++) U->val[p] = d[i] * U->val[p];
+    }
+  }
+  free(row); free(rowlevs); free(idxs); free(heap.v);
+  return rc;
+}
+
+/* ILUT(fill, thresh) with maxval scaling */
+static int o_ilut(int n, const int *irp, const int *ja, const double *val,
+                  int fill, double thresh, gcsr *L, gcsr *U, double *d) {
+  double maxv = 0.0;
+  g_init(L, n, 0);
+  g_init(U, n, 0);
+  for (long p = 0; p < irp[n]; p++)
+    if (fabs(val[p]) > maxv) maxv = fabs(val[p]);
+  if (!(maxv > 0.0)) return -(n + 1);
+  double scale = 1.0 / maxv;
+  double *row = (double *)calloc((size_t)n, sizeof(double));
+  double *sv = (double *)malloc(sizeof(double) * (size_t)(n + 1));
+  int *idxs = NULL, idxcap = 0;
+  double *xw = NULL;
+  int *xwid = NULL, xcap = 0;
+  iheap heap = {0};
+  dheap dh = {0};
+  int rc = 0;
+  for (int i = 0; i < n && rc == 0; i++) {
+    /* copyin */
+    heap.n = 0;
+    int nlw = 0, nup = 0, jmaxup = -1, nzr = 0;
+    double dmaxup = 0.0;
+    for (int p = irp[i]; p < irp[i + 1]; p++) {
+      int k = ja[p];
+      row[k] = scale * val[p];
+      sv[nzr++] = row[k];
+      ih_push(&heap, k);
+      if (k < i) nlw++;
+      if (k > i) {
+        nup++;
+        if (fabs(row[k]) > dmaxup) { jmaxup = k; dmaxup = fabs(row[k]); }
+      }
+    }
+    double nrmi = o_dnrm2(nzr, sv);
+    /* fact */
+    int nidx = 0, lastk = -1, k;
+    while (ih_pop(&heap, &k) == 0) {
+      if (k == lastk) continue;
+      lastk = k;
+      if (nidx == idxcap) {
+        idxcap = idxcap ? 2 * idxcap : 256;
+        idxs = (int *)realloc(idxs, sizeof(int) * (size_t)idxcap);
+      }
+      idxs[nidx++] = k;
+      if (k < i) {
+        double rwk = row[k];
+        row[k] = row[k] * d[k];
+        if (fabs(row[k]) < thresh * nrmi) {
+          row[k] = 0.0;
+          continue;
+        }
+        for (long jj = U->irp[k]; jj < U->irp[k + 1]; jj++) {
+          int j = U->ja[jj];
+          if (row[j] == 0.0) ih_push(&heap, j);
+          row[j] = row[j] - rwk * U->val[jj];
+        }
+      }
+    }
+    if (nidx > xcap) {
+      xcap = nidx;
+      xw = (double *)realloc(xw, sizeof(double) * (size_t)xcap);
+      xwid = (int *)realloc(xwid, sizeof(int) * (size_t)xcap);
+    }
+    /* copyout: lower part */
+    dh.last = 0;
+    int nz = 0, idxp = 0;
+    while (idxp < nidx && idxs[idxp] < i) {
+      int widx = idxs[idxp++];
+      double witem = row[widx];
+      if (fabs(witem) < thresh * nrmi) continue;
+      xw[nz] = witem; xwid[nz] = widx; nz++;
+      dh_insert(&dh, witem, widx);
+    }
+    if (nz > nlw + fill) {
+      nz = nlw + fill;
+      for (int q = 0; q < nz; q++) dh_get_first(&dh, &xw[q], &xwid[q]);
+    }
+    sort_pairs(nz, xwid, xw);
+    for (int q = 0; q < nz; q++) g_push(L, xwid[q], xw[q], 0);
+    L->irp[i + 1] = (int)L->nnz;
+    /* the diagonal */
+    if (idxp >= nidx || idxs[idxp] != i || fabs(row[i]) < ORC_EPSTOL) {
+      rc = -(i + 1);
+      break;
+    }
+    d[i] = 1.0 / row[i];
+    idxp++;
+    /* upper part */
+    dh.last = 0;
+    nz = 0;
+    for (; idxp < nidx; idxp++) {
+      int widx = idxs[idxp];
+      double witem = row[widx];
+      if (widx != jmaxup && fabs(witem) < thresh * nrmi) continue;
+      xw[nz] = witem; xwid[nz] = widx; nz++;
+      dh_insert(&dh, witem, widx);
+    }
+    if (nz > nup + fill) {
+      int fnd = 0;
+      nz = nup + fill;
+      for (int q = 0; q < nz; q++) {
+        dh_get_first(&dh, &xw[q], &xwid[q]);
+        if (xwid[q] == jmaxup) fnd = 1;
+      }
+      if (i < jmaxup && !fnd) {
+        xw[nz - 1] = row[jmaxup];
+        xwid[nz - 1] = jmaxup;
+      }
+    }
+    sort_pairs(nz, xwid, xw);
+    for (int q = 0; q < nz; q++) g_push(U, xwid[q], d[i] * xw[q], 0);
+    U->irp[i + 1] = (int)U->nnz;
+    for (int q = 0; q < nidx; q++) row[idxs[q]] = 0.0;
+  }
+  for (int i = 0; i < n; i++) d[i] = d[i] * scale;
+  free(row); free(sv); free(idxs); free(xw); free(xwid);
+  free(heap.v); free(dh.key); free(dh.idx);
+  return rc;
+}
+
+/* mld_dsparse_invk on a unit upper triangle without stored diagonal */
+static int o_sparse_invk(const gcsr *a, int fill, gcsr *z) {
+  int n = a->n;
+  double *row = (double *)calloc((size_t)n, sizeof(double));
+  int *rowlevs = (int *)malloc(sizeof(int) * (size_t)n);
+  int *idxs = (int *)malloc(sizeof(int) * (size_t)(n + 1));
+  iheap heap = {0};
+  int rc = 0;
+  for (int j = 0; j < n; j++) rowlevs[j] = -(n + 1);
+  g_init(z, n, 0);
+  for (int i = 0; i < n - 1 && rc == 0; i++) {
+    heap.n = 0;
+    for (long p = a->irp[i]; p < a->irp[i + 1]; p++) {
+      int k = a->ja[p];
+      row[k] = -1.0 * a->val[p];
+      rowlevs[k] = 0;
+      ih_push(&heap, k);
+    }
+    row[i] = 1.0;
+    rowlevs[i] = 0;
+    int nidx = 1, lastk = i, k;
+    idxs[0] = i;
+    while (ih_pop(&heap, &k) == 0) {
+      if (k == lastk) continue;
+      lastk = k;
+      idxs[nidx++] = k;
+      if (row[k] != 0.0 && rowlevs[k] <= fill) {
+        double rwk = row[k];
+        int lrwk = rowlevs[k];
+        for (long jj = a->irp[k]; jj < a->irp[k + 1]; jj++) {
+          int j = a->ja[jj];
+          if (j <= k) { rc = -(i + 1); break; }
+          if (rowlevs[j] < 0) {
+            ih_push(&heap, j);
+            rowlevs[j] = abs(rowlevs[j]);
+          }
+          row[j] = row[j] - rwk * a->val[jj];
+          if (lrwk + 1 < rowlevs[j]) rowlevs[j] = lrwk + 1;
+        }
+      }
+    }
+    for (int p = 0; p < nidx; p++) {
+      int j = idxs[p];
+      if (j >= i) {
+        if (rowlevs[j] <= fill) g_push(z, j, row[j], 0);
+        row[j] = 0.0;
+        rowlevs[j] = -(n + 1);
+      }
+    }
+    z->irp[i + 1] = (int)z->nnz;
+  }
+  if (n > 0) {
+    g_push(z, n - 1, 1.0, 0);
+    z->irp[n] = (int)z->nnz;
+  }
+  free(row); free(rowlevs); free(idxs); free(heap.v);
+  return rc;
+}
+
+/* mld_dsparse_invt on a unit upper triangle without stored diagonal */
+static int o_sparse_invt(const gcsr *a, int nzrmax, double sp_thresh, gcsr *z) {
+  int n = a->n;
+  double *row = (double *)calloc((size_t)n, sizeof(double));
+  int *irwt = (int *)calloc((size_t)n, sizeof(int));
+  int *idxs = (int *)malloc(sizeof(int) * (size_t)(n + 1));
+  double *xw = (double *)malloc(sizeof(double) * (size_t)(n + 1));
+  int *xwid = (int *)malloc(sizeof(int) * (size_t)(n + 1));
+  iheap heap = {0};
+  dheap dh = {0};
+  int rc = 0;
+  g_init(z, n, 0);
+  for (int i = 0; i < n - 1 && rc == 0; i++) {
+    /* copyin, sign -1 */
+    heap.n = 0;
+    int nup = 0;
+    for (long p = a->irp[i]; p < a->irp[i + 1]; p++) {
+      int k = a->ja[p];
+      row[k] = -1.0 * a->val[p];
+      ih_push(&heap, k);
+      irwt[k] = 1;
+      if (k > i) nup++;
+    }
+    double nrmi = o_dnrm2(a->irp[i + 1] - a->irp[i], a->val + a->irp[i]);
+    row[i] = 1.0;
+    if (nrmi < 1.0)
+      nrmi = sqrt(1.0 + nrmi * nrmi);
+    else
+      nrmi = nrmi * sqrt(1.0 + 1.0 / (nrmi * nrmi));
+    /* inv */
+    int nidx = 1, lastk = i, k;
+    idxs[0] = i;
+    irwt[i] = 1;
+    while (ih_pop(&heap, &k) == 0 && rc == 0) {
+      if (k == lastk) continue;
+      lastk = k;
+      double rwk = row[k];
+      if (fabs(rwk) < sp_thresh * nrmi) {
+        row[k] = 0.0;
+        irwt[k] = 0;
+        continue;
+      }
+      for (long jj = a->irp[k]; jj < a->irp[k + 1]; jj++) {
+        int j = a->ja[jj];
+        if (j <= k) { rc = -(i + 1); break; }
+        row[j] = row[j] - rwk * a->val[jj];
+        if (irwt[j] == 0) {
+          if (fabs(row[j]) < sp_thresh * nrmi) {
+            row[j] = 0.0;
+          } else {
+            ih_push(&heap, j);
+            irwt[j] = 1;
+          }
+        }
+      }
+      idxs[nidx++] = k;
+      irwt[k] = 0;
+    }
+    irwt[i] = 0;
+    /* copyout (the enabled branch) */
+    dh.last = 0;
+    int nz = 0;
+    double wmin = 1.7976931348623157e308; /* HUGE(wmin) */
+    for (int p = 0; p < nidx; p++) {
+      int widx = idxs[p];
+      double witem = row[widx];
+      if (widx != i && fabs(witem) < sp_thresh * nrmi) continue;
+      if (nz > nup + nzrmax && fabs(witem) < wmin) continue;
+      if (fabs(witem) < wmin) wmin = fabs(witem);
+      xw[nz] = witem; xwid[nz] = widx; nz++;
+      dh_insert(&dh, witem, widx);
+    }
+    if (nz > nup + nzrmax) {
+      nz = nup + nzrmax;
+      for (int q = 0; q < nz; q++) dh_get_first(&dh, &xw[q], &xwid[q]);
+    }
+    sort_pairs(nz, xwid, xw);
+    for (int q = 0; q < nz; q++) g_push(z, xwid[q], xw[q], 0);
+    for (int p = 0; p < nidx; p++) row[idxs[p]] = 0.0;
+    z->irp[i + 1] = (int)z->nnz;
+  }
+  if (n > 0) {
+    g_push(z, n - 1, 1.0, 0);
+    z->irp[n] = (int)z->nnz;
+  }
+  free(row); free(irwt); free(idxs); free(xw); free(xwid);
+  free(heap.v); free(dh.key); free(dh.idx);
+  return rc;
+}
+
+static void g_export(gcsr *m, int **irp, int **ja, double **val, long *nnz) {
+  *irp = m->irp;
+  *ja = m->ja;
+  *val = m->val;
+  *nnz = m->nnz;
+  free(m->lev);
+  memset(m, 0, sizeof(*m));
+}
+
+/* (L, U) -> (W^T = (inv(L^T))^T, Z = inv(U)) */
+static int o_invert_pair(int kind, gcsr *L, gcsr *U, int fill, double thresh,
+                         int **wt_irp, int **wt_ja, double **wt_val, long *nnz_wt,
+                         int **z_irp, int **z_ja, double **z_val, long *nnz_z) {
+  gcsr z, lt, zl, wt;
+  int rc = kind == 0 ? o_sparse_invk(U, fill, &z) : o_sparse_invt(U, fill, thresh, &z);
+  if (rc != 0) { g_free(&z); return rc; }
+  g_transpose(L, &lt);
+  rc = kind == 0 ? o_sparse_invk(&lt, fill, &zl) : o_sparse_invt(&lt, fill, thresh, &zl);
+  g_free(&lt);
+  if (rc != 0) { g_free(&z); g_free(&zl); return rc; }
+  g_transpose(&zl, &wt);
+  g_free(&zl);
+  g_export(&wt, wt_irp, wt_ja, wt_val, nnz_wt);
+  g_export(&z, z_irp, z_ja, z_val, nnz_z);
+  return 0;
+}
+
+int orc_invk_build(int n, const int *irp, const int *ja, const double *val,
+                   int fill1, int fill2,
+                   int **wt_irp, int **wt_ja, double **wt_val, long *nnz_wt,
+                   int **z_irp, int **z_ja, double **z_val, long *nnz_z, double *d) {
+  gcsr L, U;
+  if (n <= 0 || fill1 < 0 || fill2 < 0) return -1;
+  int rc = o_iluk(n, irp, ja, val, fill1, &L, &U, d);
+  if (rc == 0)
+    rc = o_invert_pair(0, &L, &U, fill2, 0.0, wt_irp, wt_ja, wt_val, nnz_wt,
+                       z_irp, z_ja, z_val, nnz_z);
+  g_free(&L);
+  g_free(&U);
+  return rc;
+}
+
+int orc_invt_build(int n, const int *irp, const int *ja, const double *val,
+                   int fillin, double thresh, int invfill, double invthresh,
+                   int **wt_irp, int **wt_ja, double **wt_val, long *nnz_wt,
+                   int **z_irp, int **z_ja, double **z_val, long *nnz_z, double *d) {
+  gcsr L, U;
+  if (n <= 0 || fillin < 0 || invfill < 0 || !(thresh >= 0.0) || !(invthresh >= 0.0))
+    return -1;
+  int rc = o_ilut(n, irp, ja, val, fillin, thresh, &L, &U, d);
+  if (rc == 0)
+    rc = o_invert_pair(1, &L, &U, invfill, invthresh, wt_irp, wt_ja, wt_val, nnz_wt,
+                       z_irp, z_ja, z_val, nnz_z);
+  g_free(&L);
+  g_free(&U);
+  return rc;
+}
+
+void orc_free(void *p) { free(p); }

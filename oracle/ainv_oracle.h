@@ -55,6 +55,23 @@ int orc_ainv_build(int alg, int n, const int *irp, const int *ja,
                    int *z_irp, int *z_ja, double *z_val, long *nnz_z,
                    double *d);
 
+/* mld_d_invk_bld (src/impl/mld_d_invk_bld.f90:104-125): ILU(fill1), then
+ * the level-fill2 sparse inverses of U and L (via L^T).  mld_d_invt_bld
+ * (src/impl/mld_d_invt_bld.f90:108-136): ILUT(fillin, thresh) with maxval
+ * scaling, then the (invfill, invthresh) sparse inverses.  Both produce
+ * W^T ~ L^-1 (CSR), Z ~ U^-1 (CSR) and d = D^-1 (n entries, caller-owned).
+ * The factor arrays are allocated here; release each with orc_free.
+ * Returns 0, or a negative value (-(row+1) for a too-small pivot). */
+int orc_invk_build(int n, const int *irp, const int *ja, const double *val,
+                   int fill1, int fill2,
+                   int **wt_irp, int **wt_ja, double **wt_val, long *nnz_wt,
+                   int **z_irp, int **z_ja, double **z_val, long *nnz_z, double *d);
+int orc_invt_build(int n, const int *irp, const int *ja, const double *val,
+                   int fillin, double thresh, int invfill, double invthresh,
+                   int **wt_irp, int **wt_ja, double **wt_val, long *nnz_wt,
+                   int **z_irp, int **z_ja, double **z_val, long *nnz_z, double *d);
+void orc_free(void *p);
+
 /* ---- application phase --------------------------------------------------*/
 /* y = alpha*A*x + beta*y (PSBLAS CSR csmv, trans='N'); OpenMP over rows. */
 void orc_csr_spmv(int n, const int *irp, const int *ja, const double *val,

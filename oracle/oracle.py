@@ -62,6 +62,17 @@ def lib():
         L.orc_cg.argtypes = kry
         L.orc_bicgstab.restype = C.c_int
         L.orc_bicgstab.argtypes = kry
+        pp_i = C.POINTER(C.POINTER(C.c_int))
+        pp_d = C.POINTER(C.POINTER(C.c_double))
+        outs = [pp_i, pp_i, pp_d, C.POINTER(C.c_long),
+                pp_i, pp_i, pp_d, C.POINTER(C.c_long), _f64p]
+        L.orc_invk_build.restype = C.c_int
+        L.orc_invk_build.argtypes = [C.c_int, _i32p, _i32p, _f64p, C.c_int,
+                                     C.c_int] + outs
+        L.orc_invt_build.restype = C.c_int
+        L.orc_invt_build.argtypes = [C.c_int, _i32p, _i32p, _f64p, C.c_int,
+                                     C.c_double, C.c_int, C.c_double] + outs
+        L.orc_free.argtypes = [C.c_void_p]
         L.orc_set_threads.argtypes = [C.c_int]
         L.orc_get_threads.restype = C.c_int
         _lib = L
@@ -128,6 +139,42 @@ def ainv_build(a: CSR, alg: str = "LLK", fill_in: int = 20,
         raise RuntimeError(f"orc_ainv_build failed: {rc}")
     return Factors(CSR(n, wi, wj[:nw.value].copy(), wv[:nw.value].copy()),
                    CSR(n, zi, zj[:nz.value].copy(), zv[:nz.value].copy()), d)
+
+
+def _owned_factors(n, call) -> Factors:
+    """Run an oracle builder that allocates its factor arrays; copy and free."""
+    ptrs = [C.POINTER(C.c_int)(), C.POINTER(C.c_int)(), C.POINTER(C.c_double)(),
+            C.POINTER(C.c_int)(), C.POINTER(C.c_int)(), C.POINTER(C.c_double)()]
+    nw, nz = C.c_long(), C.c_long()
+    d = np.zeros(n, np.float64)
+    rc = call(C.byref(ptrs[0]), C.byref(ptrs[1]), C.byref(ptrs[2]), C.byref(nw),
+              C.byref(ptrs[3]), C.byref(ptrs[4]), C.byref(ptrs[5]), C.byref(nz), d)
+    try:
+        if rc != 0:
+            raise RuntimeError(f"oracle factor build failed: {rc}")
+        sizes = [n + 1, nw.value, nw.value, n + 1, nz.value, nz.value]
+        arrs = [np.ctypeslib.as_array(p, shape=(k,)).copy() if k else
+                np.zeros(0, np.int32 if i % 3 < 2 else np.float64)
+                for i, (p, k) in enumerate(zip(ptrs, sizes))]
+    finally:
+        for p in ptrs:
+            if p:
+                lib().orc_free(C.cast(p, C.c_void_p))
+    return Factors(CSR(n, *arrs[:3]), CSR(n, *arrs[3:]), d)
+
+
+def invk_build(a: CSR, fill1: int = 1, fill2: int = 1) -> Factors:
+    """INVK factors: ILU(fill1), then level-fill2 sparse inverses."""
+    return _owned_factors(a.n, lambda *o: lib().orc_invk_build(
+        a.n, a.irp, a.ja, a.val, fill1, fill2, *o))
+
+
+def invt_build(a: CSR, fillin: int = 20, thresh: float = 0.05,
+               invfill: int = 20, invthresh: float = 0.05) -> Factors:
+    """INVT factors: ILUT(fillin, thresh), then (invfill, invthresh) inverses."""
+    return _owned_factors(a.n, lambda *o: lib().orc_invt_build(
+        a.n, a.irp, a.ja, a.val, fillin, float(thresh), invfill,
+        float(invthresh), *o))
 
 
 def spmv(a: CSR, x, alpha=1.0, beta=0.0, y=None, trans="N") -> np.ndarray:

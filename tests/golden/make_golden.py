@@ -21,6 +21,7 @@ from __future__ import annotations
 import heapq
 import math
 import os
+import sys
 
 import numpy as np
 
@@ -273,6 +274,241 @@ def splitmix_uniform(seed, n, lo=-1.0, hi=1.0):
     return out
 
 
+# ------------------------------------------------------ INVK / INVT ----
+# MLD2P4's ILU(k) / ILUT (external to the reference; restated from their
+# published IKJ row algorithm) and the plugin's sparse inverses
+# (src/impl/mld_dsparse_invk.f90, mld_d_invk_{copyin,inv,copyout}.f90,
+# src/impl/mld_dsparse_invt.f90, mld_d_invt_{copyin,inv,copyout}.f90).
+# Rows are lists of (column, value); L and U carry no diagonal.
+
+def dnrm2(xs):
+    """Reference BLAS dnrm2 (one-pass scaled sum of squares)."""
+    scale, ssq = 0.0, 1.0
+    for x in xs:
+        if x != 0.0:
+            ax = abs(x)
+            if scale < ax:
+                ssq = 1.0 + ssq * ((scale / ax) * (scale / ax))
+                scale = ax
+            else:
+                ssq = ssq + (ax / scale) * (ax / scale)
+    return scale * math.sqrt(ssq)
+
+
+def drain(h):
+    """Pop an ascending index heap, skipping repeats (the lastk test)."""
+    last = None
+    while h:
+        k = heapq.heappop(h)
+        if k != last:
+            last = k
+            yield k
+
+
+def iluk(rows, fill):
+    n = len(rows)
+    unset = -(n + 1)
+    row, lev = [0.0] * n, [unset] * n
+    L, U, Ulev, d = [], [], [], [0.0] * n
+    for i in range(n):
+        h = []
+        for c, v in rows[i]:
+            row[c], lev[c] = v, 0
+            heapq.heappush(h, c)
+        idxs = []
+        for k in drain(h):
+            idxs.append(k)
+            if row[k] != 0.0 and lev[k] <= fill and k < i:
+                rwk, lk = row[k], lev[k]
+                row[k] = row[k] * d[k]
+                for (j, uv), ul in zip(U[k], Ulev[k]):
+                    if lev[j] < 0:
+                        heapq.heappush(h, j)
+                        lev[j] = -lev[j]
+                    row[j] = row[j] - rwk * uv
+                    lev[j] = min(lev[j], lk + ul + 1)
+        lr, ur, ulv, piv = [], [], [], 0.0
+        for j in idxs:
+            if j < i and lev[j] <= fill:
+                lr.append((j, row[j]))
+            elif j == i:
+                piv = row[j]
+            elif j > i and lev[j] <= fill:
+                ur.append((j, row[j]))
+                ulv.append(lev[j])
+            row[j], lev[j] = 0.0, unset
+        if abs(piv) < EPSTOL:
+            raise ZeroDivisionError(f"ILU(k) pivot at row {i}")
+        d[i] = 1.0 / piv
+        L.append(lr)
+        U.append([(j, d[i] * v) for j, v in ur])
+        Ulev.append(ulv)
+    return L, U, d
+
+
+def top_magnitude(items, cap):
+    """Offer (index, value) pairs to the magnitude heap, pop `cap` of them."""
+    h = MagHeapDown()
+    for j, v in items:
+        h.insert(v, j)
+    out = []
+    for _ in range(cap):
+        v, j = h.get_first()
+        out.append((j, v))
+    return out
+
+
+def ilut(rows, fill, thresh):
+    n = len(rows)
+    w = 1.0 / max(abs(v) for e in rows for _, v in e)
+    row = [0.0] * n
+    L, U, d = [], [], [0.0] * n
+    for i in range(n):
+        h, vals = [], []
+        nlw = nup = 0
+        jmaxup, dmaxup = None, 0.0
+        for c, v in rows[i]:
+            row[c] = w * v
+            vals.append(row[c])
+            heapq.heappush(h, c)
+            if c < i:
+                nlw += 1
+            if c > i:
+                nup += 1
+                if abs(row[c]) > dmaxup:
+                    jmaxup, dmaxup = c, abs(row[c])
+        tol = thresh * dnrm2(vals)
+        idxs = []
+        for k in drain(h):
+            idxs.append(k)
+            if k < i:
+                rwk = row[k]
+                row[k] = row[k] * d[k]
+                if abs(row[k]) < tol:
+                    row[k] = 0.0
+                    continue
+                for j, uv in U[k]:
+                    if row[j] == 0.0:
+                        heapq.heappush(h, j)
+                    row[j] = row[j] - rwk * uv
+        low = [(j, row[j]) for j in idxs if j < i and not abs(row[j]) < tol]
+        if len(low) > nlw + fill:
+            low = top_magnitude(low, nlw + fill)
+        L.append(sorted(low))
+        if i not in idxs or abs(row[i]) < EPSTOL:
+            raise ZeroDivisionError(f"ILUT pivot at row {i}")
+        d[i] = 1.0 / row[i]
+        up = [(j, row[j]) for j in idxs
+              if j > i and (j == jmaxup or not abs(row[j]) < tol)]
+        if len(up) > nup + fill:
+            top = top_magnitude(up, nup + fill)
+            if jmaxup is not None and jmaxup not in [j for j, _ in top]:
+                top[-1] = (jmaxup, row[jmaxup])
+            up = top
+        U.append([(j, d[i] * v) for j, v in sorted(up)])
+        for j in idxs:
+            row[j] = 0.0
+    return L, U, [v * w for v in d]
+
+
+def sparse_invk(U, fill):
+    n = len(U)
+    Z = []
+    for i in range(n - 1):
+        row, lev = {i: 1.0}, {i: 0}
+        h = []
+        for c, v in U[i]:
+            row[c], lev[c] = -1.0 * v, 0
+            heapq.heappush(h, c)
+        idxs = [i]
+        for k in drain(h):
+            if k == i:
+                continue
+            idxs.append(k)
+            if row[k] != 0.0 and lev[k] <= fill:
+                for j, uv in U[k]:
+                    if j not in lev:
+                        heapq.heappush(h, j)
+                        lev[j], row[j] = n + 1, 0.0
+                    row[j] = row[j] - row[k] * uv
+                    lev[j] = min(lev[j], lev[k] + 1)
+        Z.append([(j, row[j]) for j in idxs if lev[j] <= fill])
+    Z.append([(n - 1, 1.0)])
+    return Z
+
+
+def sparse_invt(U, fill, thresh):
+    n = len(U)
+    Z = []
+    for i in range(n - 1):
+        row = {i: 1.0}
+        queued = set()
+        h = []
+        for c, v in U[i]:
+            row[c] = -1.0 * v
+            heapq.heappush(h, c)
+            queued.add(c)
+        nup = sum(1 for c, _ in U[i] if c > i)
+        nrmi = dnrm2([v for _, v in U[i]])
+        if nrmi < 1.0:
+            nrmi = math.sqrt(1.0 + nrmi * nrmi)
+        else:
+            nrmi = nrmi * math.sqrt(1.0 + 1.0 / (nrmi * nrmi))
+        tol = thresh * nrmi
+        idxs = [i]
+        for k in drain(h):
+            rwk = row[k]
+            queued.discard(k)
+            if abs(rwk) < tol:
+                row[k] = 0.0
+                continue
+            for j, uv in U[k]:
+                row[j] = row.get(j, 0.0) - rwk * uv
+                if j not in queued:
+                    if abs(row[j]) < tol:
+                        row[j] = 0.0
+                    else:
+                        heapq.heappush(h, j)
+                        queued.add(j)
+            idxs.append(k)
+        cap = nup + fill
+        acc, wmin = [], sys.float_info.max
+        for j in idxs:
+            v = row[j]
+            if j != i and abs(v) < tol:
+                continue
+            if len(acc) > cap and abs(v) < wmin:
+                continue
+            wmin = min(abs(v), wmin)
+            acc.append((j, v))
+        if len(acc) > cap:
+            acc = top_magnitude(acc, cap)
+        Z.append(sorted(acc))
+    Z.append([(n - 1, 1.0)])
+    return Z
+
+
+def transpose_rows(R):
+    T = [[] for _ in R]
+    for r, e in enumerate(R):
+        for c, v in e:
+            T[c].append((r, v))
+    return T
+
+
+def inverse_build(rows, solver, p):
+    """INVK p = (fill1, fill2); INVT p = (fill, thresh, invfill, invthresh)."""
+    if solver == "INVK":
+        L, U, d = iluk(rows, p[0])
+        inv = lambda T: sparse_invk(T, p[1])  # noqa: E731
+    else:
+        L, U, d = ilut(rows, p[0], p[1])
+        inv = lambda T: sparse_invt(T, p[2], p[3])  # noqa: E731
+    z = rows_to_csr(inv(U))
+    wt = rows_to_csr(transpose_rows(inv(transpose_rows(L))))
+    return wt, z, np.array(d)
+
+
 # ---------------------------------------------------------------- cases --
 CASES = [
     # name, grid, kind, beta, alg, fill_in, thresh
@@ -293,7 +529,79 @@ HAND_4x4 = [  # small nonsymmetric case worked by hand in the test
 ]
 
 
+INV_CASES = [
+    # name, grid, kind, beta, solver, params
+    ("invk_poisson5_k1", 5, "poisson", (0, 0, 0), "INVK", (1, 1)),
+    ("invk_convdiff5_k2", 5, "convdiff", (40.0, -25.0, 10.0), "INVK", (2, 1)),
+    ("invk_convdiff4_k0", 4, "convdiff", (-15.0, 5.0, 30.0), "INVK", (0, 0)),
+    ("invt_convdiff6", 6, "convdiff", (20.0, 20.0, 20.0), "INVT", (20, 0.05, 20, 0.05)),
+    ("invt_poisson5_tight", 5, "poisson", (0, 0, 0), "INVT", (3, 0.01, 2, 0.02)),
+    ("invt_convdiff5_cap", 5, "convdiff", (35.0, -12.0, 8.0), "INVT", (0, 0.002, 1, 0.005)),
+]
+
+
+def rand_rows(seed, n, density):
+    """Unstructured nonsymmetric test matrix: diagonal 4 + U(-1,1), each
+    off-diagonal present with probability `density`, values U(-1,1).  The
+    ILUT rule that keeps the largest original upper entry only fires on
+    matrices like this one, where fill can outgrow the original entries."""
+    u = splitmix_uniform(seed, n * n, 0.0, 1.0)
+    v = splitmix_uniform(seed + 1000, n * n, -1.0, 1.0)
+    rows = []
+    for i in range(n):
+        e = []
+        for j in range(n):
+            if i == j:
+                e.append((j, 4.0 + v[i * n + j]))
+            elif u[i * n + j] < density:
+                e.append((j, v[i * n + j]))
+        rows.append(e)
+    return rows
+
+
+RAND_CASES = [
+    # name, seed, n, density, solver, params
+    ("invt_rand10_jmaxup", 5, 10, 0.35, "INVT", (0, 0.0, 2, 0.01)),
+    ("invk_rand10", 5, 10, 0.35, "INVK", (1, 1)),
+]
+
+
+def save(name, rows, a, wt, z, d, extra):
+    n = len(rows)
+    x = splitmix_uniform(7, n)
+    y0 = splitmix_uniform(8, n)
+    yN = apply(wt, z, d, x, "N", 1.5, 0.5, y0)
+    yT = apply(wt, z, d, x, "T", -0.75, 2.0, y0)
+    np.savez_compressed(
+        os.path.join(HERE, f"{name}.npz"),
+        a_irp=a[0], a_ja=a[1], a_val=a[2],
+        wt_irp=wt[0], wt_ja=wt[1], wt_val=wt[2],
+        z_irp=z[0], z_ja=z[1], z_val=z[2], d=d,
+        x=x, y0=y0, yN=yN, yT=yT, **extra)
+    print(f"{name}: n={n} nnzA={len(a[1])} nnzWt={len(wt[1])} nnzZ={len(z[1])}")
+
+
+def main_inverse():
+    for name, idim, kind, beta, solver, p in INV_CASES:
+        rows = pde3d(idim, kind, beta)
+        a = rows_to_csr(rows)
+        wt, z, d = inverse_build(rows, solver, p)
+        save(name, rows, a, wt, z, d, dict(
+            meta=np.array([idim, {"poisson": 0, "convdiff": 1}[kind], 0], np.int64),
+            beta=np.array(beta, np.float64), kind=np.array(kind),
+            solver=np.array(solver), params=np.array(p, np.float64)))
+    for name, seed, n, dens, solver, p in RAND_CASES:
+        rows = rand_rows(seed, n, dens)
+        a = rows_to_csr(rows)
+        wt, z, d = inverse_build(rows, solver, p)
+        save(name, rows, a, wt, z, d, dict(
+            meta=np.array([seed, 3, n], np.int64), beta=np.zeros(3),
+            kind=np.array("rand"), density=np.array(dens),
+            solver=np.array(solver), params=np.array(p, np.float64)))
+
+
 def main():
+    main_inverse()
     cases = [(c[0], pde3d(c[1], c[2], c[3]), c) for c in CASES]
     cases.append(("hand4", HAND_4x4, ("hand4", 0, "hand", (0, 0, 0), "LLK", 4, 0.0)))
     for name, rows, c in cases:

@@ -3,7 +3,9 @@
 Fixtures come from tests/golden/make_golden.py, an independent pure-Python
 restatement of the reference (src/impl/mld_dsparse_biconjg_llk.F90,
 src/impl/mld_d_sparsify.f90, src/impl/mld_d_ainv_bld.F90,
-src/impl/mld_d_base_ainv_solver_apply_vect.f90).  Integer patterns and
+src/impl/mld_d_base_ainv_solver_apply_vect.f90, and for INVK / INVT
+src/impl/mld_dsparse_invk.f90, src/impl/mld_dsparse_invt.f90 with their
+copyin / inv / copyout routines over a restated MLD2P4 ILU(k) / ILUT).  Integer patterns and
 factor values must match bit for bit; applies to 1e-13 relative.
 """
 import glob
@@ -23,19 +25,32 @@ def _csr(irp, ja, val, n):
     return sp.csr_matrix((val, ja, irp), shape=(n, n))
 
 
+def _oracle_factors(g, a):
+    """The oracle's factors for a fixture: AINV, or INVK / INVT when the
+    fixture names its solver and parameters."""
+    solver = str(g["solver"]) if "solver" in g.files else "AINV"
+    if solver == "INVK":
+        p = g["params"]
+        return O.invk_build(a, int(p[0]), int(p[1]))
+    if solver == "INVT":
+        p = g["params"]
+        return O.invt_build(a, int(p[0]), float(p[1]), int(p[2]), float(p[3]))
+    return O.ainv_build(a, str(g["alg"]), int(g["meta"][2]), float(g["thresh"]))
+
+
 @pytest.mark.parametrize("path", FIXTURES, ids=[os.path.basename(p)[:-4] for p in FIXTURES])
 def test_oracle_matches_golden(path):
     g = np.load(path)
     a = O.CSR(len(g["a_irp"]) - 1, g["a_irp"], g["a_ja"], g["a_val"])
     kind = str(g["kind"])
-    if kind != "hand":
+    if kind in ("poisson", "convdiff"):
         idim = int(g["meta"][0])
         b = tuple(float(v) for v in g["beta"])
         gen = O.gen_pde3d(idim, kind, b)
         np.testing.assert_array_equal(gen.irp, a.irp)
         np.testing.assert_array_equal(gen.ja, a.ja)
         np.testing.assert_array_equal(gen.val, a.val)
-    f = O.ainv_build(a, str(g["alg"]), int(g["meta"][2]), float(g["thresh"]))
+    f = _oracle_factors(g, a)
     np.testing.assert_array_equal(f.wt.irp, g["wt_irp"])
     np.testing.assert_array_equal(f.wt.ja, g["wt_ja"])
     np.testing.assert_array_equal(f.wt.val, g["wt_val"])
