@@ -372,7 +372,8 @@ def main():
 
 
 def run_extras(ainv, torch, dev, irp, ja, val, f, sv, flush, stream, fp64_ms):
-    """Mixed-precision apply GB/s and BiCGSTAB solves/s (FP64 vs FP32 factors)."""
+    """Mixed-precision apply GB/s, BiCGSTAB solves/s (FP64 vs FP32 factors),
+    and the INVK / INVT variants."""
     n = len(irp) - 1
     nnz = (len(f["wt_ja"]), len(f["z_ja"]))
     out = {"mixed": {}, "solve": {}}
@@ -425,7 +426,74 @@ def run_extras(ainv, torch, dev, irp, ja, val, f, sv, flush, stream, fp64_ms):
                               "s_per_solve": round(min(times), 5),
                               "solves_per_s": round(1.0 / min(times), 3)}
     sv.cnv("FP64")
+    out["variants"] = run_variants(ainv, torch, dev, irp, ja, val, A, b, bn, xs, x, y,
+                                   flush, stream)
     A.close()
+    return out
+
+
+def run_variants(ainv, torch, dev, irp, ja, val, A, b, bn, xs, x, y, flush, stream):
+    """The INVK (fill level 1) and INVT (threshold 0.05, fill cap 20) solvers
+    on the same matrix and right-hand side: host build time, FP64 apply GB/s
+    (layout bytes, L2 flushed), and BiCGSTAB to 1e-9 with FP64 and FP32
+    factors."""
+    n = len(irp) - 1
+    out = {}
+    settings = {"INVK": {"SUB_FILLIN": 1, "INV_FILLIN": 1},
+                "INVT": {"SUB_FILLIN": 20, "SUB_ILUTHRS": 0.05,
+                         "INV_FILLIN": 20, "INV_THRESH": 0.05}}
+    for name, kv in settings.items():
+        sv = (ainv.mld_d_invk_solver_type() if name == "INVK"
+              else ainv.mld_d_invt_solver_type())
+        for k, v in kv.items():
+            (sv.csetr if isinstance(v, float) else sv.cseti)(k, v)
+        t0 = time.perf_counter()
+        info = sv.build(irp, ja, val)
+        t_build = time.perf_counter() - t0
+        if info != 0:
+            out[name] = {"info": info, "error": ainv.last_error()}
+            continue
+        f = sv.factors()
+        rec = {"settings": kv, "build_s": round(t_build, 2),
+               "nnz_wt": int(len(f["wt_ja"])), "nnz_z": int(len(f["z_ja"]))}
+        assert sv.cnv("FP64") == 0, ainv.last_error()
+        df = sv.device
+        for _ in range(5):
+            df.apply(x, y, 1.0, 0.0, "N", stream)
+        evs = []
+        for _ in range(30):
+            flush.zero_()
+            a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            df.apply(x, y, 1.0, 0.0, "N", stream)
+            e.record(stream)
+            evs.append((a, e))
+        torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(e) for a, e in evs) / len(evs)
+        Bv = sum(layout_bytes(n, {k: df.layout_info(k) for k in ("wt", "z")}, 8, 8))
+        rec["apply"] = {"ms": round(ms, 5), "GB/s": round(Bv / (ms * 1e-3) / 1e9, 2),
+                        "bytes": Bv,
+                        "csr_bytes": csr_apply_bytes(n, rec["nnz_wt"], rec["nnz_z"])}
+        rec["solve"] = {}
+        for prec in ("FP64", "FP32"):
+            if prec != "FP64":
+                sv.cnv(prec)
+            times, res = [], None
+            for _ in range(2):
+                xx = torch.zeros(n, dtype=torch.float64, device=dev)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                res = A.solve(b, xx, sv.device, "BICGSTAB", 1e-9, 2000, stream)
+                times.append(time.perf_counter() - t0)
+            r = torch.empty_like(b)
+            A.spmv(xx, r, 1.0, 0.0, stream)
+            rec["solve"][prec] = {
+                "iters": res.iter, "info": res.info, "relres": res.err,
+                "true_relres": float(torch.linalg.vector_norm(b - r)) / bn,
+                "max_err_vs_xstar": float((xx - xs).abs().max()),
+                "s_per_solve": round(min(times), 5), "solves_per_s": round(1.0 / min(times), 3)}
+        sv.free()
+        out[name] = rec
     return out
 
 

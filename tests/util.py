@@ -30,3 +30,20 @@ def relerr(y, ref):
     """Norm-wise relative error ||y - ref||_inf / ||ref||_inf."""
     y = np.asarray(y)
     return float(np.abs(y - ref).max() / max(np.abs(ref).max(), 1e-300))
+
+
+# The 200^3 convection-diffusion variants: INVK (fill level 1) and INVT
+# (threshold 0.05, fill cap 20), the sub / inverse settings taken alike.
+INVK_SETTINGS = {"SUB_FILLIN": 1, "INV_FILLIN": 1}
+INVT_SETTINGS = {"SUB_FILLIN": 20, "SUB_ILUTHRS": 0.05, "INV_FILLIN": 20, "INV_THRESH": 0.05}
+
+
+def build_inverse_factors(solver, irp, ja, val, settings=None):
+    """Product host build of INVK / INVT (mld_d_inv[kt]_solver_type)."""
+    sv = ainv.mld_d_invk_solver_type() if solver == "INVK" else ainv.mld_d_invt_solver_type()
+    if settings is None:
+        settings = INVK_SETTINGS if solver == "INVK" else INVT_SETTINGS
+    for k, v in settings.items():
+        (sv.csetr if isinstance(v, float) else sv.cseti)(k, v)
+    assert sv.build(irp, ja, val) == 0, ainv.last_error()
+    return sv.factors()
