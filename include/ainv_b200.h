@@ -210,6 +210,67 @@ int mld_d_solver_descr(const mld_d_solver *sv, char *buf, size_t len);
  * <prefix>_diag.mtx, <prefix>_zmat.mtx. */
 int mld_d_solver_dump(const mld_d_solver *sv, const char *prefix);
 
+/* ---- solve server: continuous batching of many solves ----------------- */
+/* The reference solves one system at a time (psb_krylov at
+ * tests/pdegen/ppde3d.f90:280-281).  The server keeps preconditioned
+ * BiCGSTAB solves (istop=2, the loop of ainv_gpu_solve) against resident
+ * operators in flight together: every graph launch advances all admitted
+ * requests, whatever their operator and size, by a fixed number of
+ * iterations, and requests are admitted first-come first-served as slots
+ * and device memory free up.  A request's result does not depend on what
+ * else runs beside it (bit-identical iterates alone or in a mix).
+ * x0 = 0 for every request. */
+typedef struct ainv_server ainv_server;
+
+typedef struct {
+  long long id;
+  int op;          /* operator index from ainv_server_add_operator */
+  int status;      /* AINV_SUCCESS, AINV_ERR_NOCONV, ... as ainv_gpu_solve */
+  int iter;        /* BiCGSTAB iterations */
+  double err;      /* final relative residual (confirmed on b - A x) */
+  double t_submit; /* server clock (seconds since creation) */
+  double t_admit;
+  double t_done;   /* x written back to the caller's buffer */
+} ainv_result;
+
+typedef struct {
+  long long submitted, completed, graph_launches, kernel_launches;
+  int active, queued, peak_active, max_slots, grid, iters_per_launch;
+  size_t arena_bytes, arena_used, arena_peak;
+  double clock;
+} ainv_server_info;
+
+/* max_slots (1..64): requests in flight together.  hbm_bytes: device bytes
+ * for the requests' vectors (0: half of the free HBM); a request is admitted
+ * only while its vectors fit (ainv_server_request_bytes).  iters_per_launch
+ * (1..64): iterations per graph launch, i.e. how often completion is
+ * checked.  Starts the server's engine thread on the current device. */
+int ainv_server_create(ainv_server **srv, int max_slots, size_t hbm_bytes,
+                       int iters_per_launch);
+/* Register a resident operator A with its factors h (AINV, INVK or INVT,
+ * any precision; FP32/BF16 factors get true-residual replacement every 50
+ * iterations).  Both must outlive the server. */
+int ainv_server_add_operator(ainv_server *srv, const ainv_csr *a, const ainv_handle *h,
+                             int *op);
+/* Queue a solve of A_op x = b.  b (host, n doubles) is read at admission and
+ * x (host, n doubles) written at completion: both must stay valid until
+ * ainv_server_wait returns for *id.  Thread-safe. */
+int ainv_server_submit(ainv_server *srv, int op, const double *b, double *x, double eps,
+                       int itmax, long long *id);
+/* Wait for request id (timeout_s < 0: no limit); fills *res (may be NULL)
+ * and returns the request's status, or AINV_ERR_TIMEOUT if it is still
+ * running.  Each id is waited for once. */
+int ainv_server_wait(ainv_server *srv, long long id, double timeout_s, ainv_result *res);
+int ainv_server_stats(ainv_server *srv, ainv_server_info *out);
+/* Finishes every queued request, stops the engine, frees the server. */
+int ainv_server_destroy(ainv_server *srv);
+/* Device bytes one request of n rows holds while admitted. */
+size_t ainv_server_request_bytes(int n);
+/* The block plan of a launch: grid blocks shared among nslots requests of
+ * rows[k] rows in proportion to their 512-row chunks (at least one each,
+ * never more than their chunks).  Host-only; b0/nb receive nslots entries. */
+int ainv_server_plan(int nslots, const int *rows, int grid, int *b0, int *nb);
+
 #ifdef __cplusplus
 }
 #endif

@@ -8,7 +8,8 @@ from .device import DeviceFactors, DeviceOperator, SolveResult
 from .solver import (mld_d_ainv_solver_type, mld_d_invk_solver_type,
                      mld_d_invt_solver_type)
 from . import pde
+from .serve import SolveServer
 
 __all__ = ["AINV_ALG", "KRYLOV", "PREC", "AinvError", "LIB_PATH", "check", "last_error", "lib",
            "DeviceFactors", "DeviceOperator", "SolveResult", "mld_d_ainv_solver_type",
-           "mld_d_invk_solver_type", "mld_d_invt_solver_type", "pde"]
+           "mld_d_invk_solver_type", "mld_d_invt_solver_type", "pde", "SolveServer"]

@@ -76,7 +76,32 @@ SIGNATURES = [
     ("mld_d_solver_get_wrksz", _i, []),
     ("mld_d_solver_descr", _i, [_vp, C.c_char_p, C.c_size_t]),
     ("mld_d_solver_dump", _i, [_vp, C.c_char_p]),
+    ("ainv_server_create", _i, [C.POINTER(_vp), _i, C.c_size_t, _i]),
+    ("ainv_server_add_operator", _i, [_vp, _vp, _vp, _ip]),
+    ("ainv_server_submit", _i, [_vp, _i, _vp, _vp, _d, _i, _llp]),
+    ("ainv_server_wait", _i, [_vp, _ll, _d, _vp]),
+    ("ainv_server_stats", _i, [_vp, _vp]),
+    ("ainv_server_destroy", _i, [_vp]),
+    ("ainv_server_request_bytes", C.c_size_t, [_i]),
+    ("ainv_server_plan", _i, [_i, _vp, _i, _vp, _vp]),
 ]
+
+
+class Result(C.Structure):
+    """ainv_result"""
+    _fields_ = [("id", C.c_longlong), ("op", C.c_int), ("status", C.c_int),
+                ("iter", C.c_int), ("err", C.c_double), ("t_submit", C.c_double),
+                ("t_admit", C.c_double), ("t_done", C.c_double)]
+
+
+class ServerInfo(C.Structure):
+    """ainv_server_info"""
+    _fields_ = [("submitted", C.c_longlong), ("completed", C.c_longlong),
+                ("graph_launches", C.c_longlong), ("kernel_launches", C.c_longlong),
+                ("active", C.c_int), ("queued", C.c_int), ("peak_active", C.c_int),
+                ("max_slots", C.c_int), ("grid", C.c_int), ("iters_per_launch", C.c_int),
+                ("arena_bytes", C.c_size_t), ("arena_used", C.c_size_t),
+                ("arena_peak", C.c_size_t), ("clock", C.c_double)]
 
 
 class AinvError(RuntimeError):
