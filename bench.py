@@ -213,6 +213,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip solves/s and mixed legs")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
+    ap.add_argument("--serve-requests", type=int, default=2000)
+    ap.add_argument("--serve-rates", default="50,200,2000",
+                    help="mean arrival rates (requests/s) of the serving sweep")
+    ap.add_argument("--serve-slots", type=int, default=32)
+    ap.add_argument("--serve-iters", type=int, default=4)
     ap.add_argument("--idim", type=int, default=IDIM,
                     help="grid side (default 200; smaller sizes for profiler captures)")
     args = ap.parse_args()
@@ -332,6 +338,11 @@ def main():
     extras = {}
     if not args.no_extras:
         extras = run_extras(ainv, torch, dev, irp, ja, val, f, sv, flush, stream, ms)
+
+    if not args.no_extras:
+        extras["block_cg"] = run_block_cg(ainv, torch, dev)
+    if not args.no_serve:
+        extras["serving"] = run_serving(ainv, torch, args)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -495,6 +506,136 @@ def run_variants(ainv, torch, dev, irp, ja, val, A, b, bn, xs, x, y, flush, stre
         sv.free()
         out[name] = rec
     return out
+
+
+def run_block_cg(ainv, torch, dev, idim=128, m=32):
+    """Multi-right-hand-side CG: 3-D Poisson on a 128^3 grid, 32 right-hand
+    sides N(0,1) (seed k for column k), AINV drop 0.1 fill 20 with FP32
+    factors, FP64 A, CG to 1e-9 per column.  One block solve (SpMM products)
+    against the same 32 systems solved one after another."""
+    irp, ja, val = ainv.pde.gen_pde3d(idim, "poisson")
+    n = len(irp) - 1
+    sv = ainv.mld_d_ainv_solver_type()
+    sv.cseti("SUB_FILLIN", FILL)
+    sv.csetr("SUB_ILUTHRS", THRESH)
+    assert sv.build(irp, ja, val) == 0, ainv.last_error()
+    assert sv.cnv("FP32") == 0, ainv.last_error()
+    A = ainv.DeviceOperator(irp, ja, val)
+    Bh = np.stack([ainv.pde.rand_normal(k, n) for k in range(m)], axis=1)
+    B = torch.from_numpy(Bh).to(dev)
+    X = torch.zeros_like(B)
+    A.block_solve(B, X, sv.device, 1e-9, 2000)  # warm-up (workspace, graph)
+    times = []
+    for _ in range(3):
+        X.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = A.block_solve(B, X, sv.device, 1e-9, 2000)
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+    R = B.clone()
+    for l in range(m):
+        r = torch.empty(n, dtype=torch.float64, device=dev)
+        A.spmv(X[:, l].contiguous(), r, 1.0, 0.0)
+        R[:, l] -= r
+    rel = (torch.linalg.vector_norm(R, dim=0) / torch.linalg.vector_norm(B, dim=0)).max()
+    # the same systems one at a time through the single-vector loop
+    t_single, it_single = 0.0, []
+    for l in range(m):
+        b = B[:, l].contiguous()
+        x = torch.zeros(n, dtype=torch.float64, device=dev)
+        if l == 0:
+            A.solve(b, x, sv.device, "CG", 1e-9, 2000)
+            x.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r1 = A.solve(b, x, sv.device, "CG", 1e-9, 2000)
+        torch.cuda.synchronize()
+        t_single += time.perf_counter() - t0
+        it_single.append(r1.iter)
+    tb = min(times)
+    out = {"workload": f"poisson3d_{idim}_ainv_drop0.1_fill20_fp32_cg_{m}rhs", "n": n,
+           "rhs": m, "converged": bool(res.converged), "max_true_relres": float(rel),
+           "iters_mean": round(float(np.mean(res.iters)), 2), "iters_max": int(max(res.iters)),
+           "s_per_block_solve": round(tb, 4), "rhs_solves_per_s": round(m / tb, 2),
+           "single_rhs_s_total": round(t_single, 4),
+           "single_rhs_solves_per_s": round(m / t_single, 2),
+           "single_iters_mean": round(float(np.mean(it_single)), 2),
+           "speedup_vs_single": round(t_single / tb, 3)}
+    A.close()
+    sv.free()
+    return out
+
+
+def run_serving(ainv, torch, args):
+    """Serving: a stream of BiCGSTAB requests (tol 1e-8, FP32 factors, x0 = 0)
+    with Poisson arrivals against 16 resident operators (3-D Poisson and
+    convection-diffusion, n^3 grids with n log-uniform in [24, 128], AINV
+    drop 0.1 fill 20), N(0,1) right-hand sides seeded by the request id.
+    Latency = submit (host b) -> solution in the host x buffer."""
+    from ainv import serve, workload
+    specs = workload.serving_operators()
+    t0 = time.perf_counter()
+    ops = []
+    for sp in specs:
+        irp, ja, val = ainv.pde.gen_pde3d(sp.idim, sp.kind, sp.beta)
+        sv = ainv.mld_d_ainv_solver_type()
+        sv.cseti("SUB_FILLIN", FILL)
+        sv.csetr("SUB_ILUTHRS", THRESH)
+        assert sv.build(irp, ja, val) == 0, ainv.last_error()
+        f = sv.factors()
+        ops.append((ainv.DeviceOperator(irp, ja, val),
+                    ainv.DeviceFactors((f["wt_irp"], f["wt_ja"], f["wt_val"]),
+                                       (f["z_irp"], f["z_ja"], f["z_val"]), f["d"],
+                                       prec="FP32"), sp.n))
+    t_build = time.perf_counter() - t0
+    nreq = args.serve_requests
+    opsel = workload.request_ops(nreq, len(ops))
+    rhs = [torch.from_numpy(workload.request_rhs(r, ops[opsel[r]][2])).pin_memory()
+           for r in range(nreq)]
+    xs = [torch.zeros(ops[opsel[r]][2], dtype=torch.float64).pin_memory() for r in range(nreq)]
+
+    def stream(rate, count, slots):
+        arr = workload.poisson_arrivals(rate, count)
+        with serve.SolveServer(max_slots=slots, iters_per_launch=args.serve_iters) as srv:
+            ids = [srv.add_operator(a, f) for a, f, _ in ops]
+            srv.wait(srv.submit(ids[0], rhs[0], xs[0]))  # warm-up
+            start = time.perf_counter()
+            rids = []
+            for r in range(count):
+                dt = arr[r] - (time.perf_counter() - start)
+                if dt > 0:
+                    time.sleep(dt)
+                rids.append(srv.submit(ids[opsel[r]], rhs[r], xs[r], 1e-8, 2000))
+            res = [srv.wait(q) for q in rids]
+            st = srv.stats()
+        t_first = min(q.t_submit for q in res)
+        t_last = max(q.t_done for q in res)
+        lat = np.array([q.latency for q in res]) * 1e3
+        wait = np.array([q.t_admit - q.t_submit for q in res]) * 1e3
+        return {"rate": rate, "requests": count, "converged": int(sum(q.converged for q in res)),
+                "max_relres": float(max(q.err for q in res)),
+                "solves_per_s": round(count / (t_last - t_first), 2),
+                "p50_ms": round(float(np.percentile(lat, 50)), 3),
+                "p90_ms": round(float(np.percentile(lat, 90)), 3),
+                "p99_ms": round(float(np.percentile(lat, 99)), 3),
+                "mean_queue_ms": round(float(wait.mean()), 3),
+                "iters_mean": round(float(np.mean([q.iter for q in res])), 2),
+                "peak_active": st["peak_active"], "graph_launches": st["graph_launches"],
+                "kernel_launches": st["kernel_launches"],
+                "arena_peak_bytes": st["arena_peak"], "arena_bytes": st["arena_bytes"]}
+
+    sweep = [stream(float(r), nreq, args.serve_slots) for r in args.serve_rates.split(",")]
+    # the same kernels with one slot: requests served one after another
+    unbatched = stream(float(args.serve_rates.split(",")[-1]), min(nreq, 300), 1)
+    for a, f, _ in ops:
+        f.close()
+        a.close()
+    return {"operators": [{"idim": sp.idim, "kind": sp.kind,
+                           "beta": [round(b, 3) for b in sp.beta]} for sp in specs],
+            "factors": "AINV LLK drop 0.1 fill 20, FP32", "tol": 1e-8,
+            "slots": args.serve_slots, "iters_per_launch": args.serve_iters,
+            "build_s": round(t_build, 1), "sweep": sweep, "unbatched_one_slot": unbatched}
 
 
 if __name__ == "__main__":

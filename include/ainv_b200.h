@@ -163,6 +163,19 @@ int ainv_gpu_solve(ainv_handle *h, const ainv_csr *a, const double *b_dev,
  * recurrence residual was replaced by b - A x. */
 int ainv_csr_solve_info(const ainv_csr *a, int *verify_fails, int *replacements);
 
+/* Preconditioned CG on m (1..32) right-hand sides at once: column l solves
+ * A x_l = b_l with its own CG recurrence (psb_dcg, istop=2, as
+ * ainv_gpu_solve) while every product with A and with the factors is one
+ * SpMM over all columns.  B and X are device arrays of n rows by m columns,
+ * row-interleaved (entry (i, l) at B[i*ldb + l]); X holds x0 on entry and
+ * the solutions on exit.  iters / errs / status (each m entries, may be
+ * NULL) receive per column the iterations, the relative residual and the
+ * status; the return value is AINV_SUCCESS when every column converged, else
+ * the first failing column's status.  h may be NULL (no preconditioner). */
+int ainv_gpu_block_solve(ainv_handle *h, const ainv_csr *a, int m, const double *B, int ldb,
+                         double *X, int ldx, double eps, int itmax, int *iters, double *errs,
+                         int *status, void *stream);
+
 /* ---- host solver types (mirror of the Fortran plugin types) ----------- */
 /* type: "AINV", "INVK" or "INVT".  default() is applied on creation. */
 int mld_d_solver_create(mld_d_solver **sv, const char *type);

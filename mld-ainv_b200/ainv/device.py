@@ -124,6 +124,19 @@ class SolveResult:
                 f"verify_fails={self.verify_fails}, replacements={self.replacements})")
 
 
+class BlockSolveResult:
+    def __init__(self, info, iters, errs, status):
+        self.info, self.iters, self.errs, self.status = info, iters, errs, status
+
+    @property
+    def converged(self) -> bool:
+        return self.info == SUCCESS and all(s == SUCCESS for s in self.status)
+
+    def __repr__(self):
+        return (f"BlockSolveResult(info={self.info}, iters={self.iters}, "
+                f"max_err={max(self.errs):.3e})")
+
+
 class DeviceOperator:
     """Sparse operator A (FP64) on the device, with the Krylov driver."""
 
@@ -160,6 +173,25 @@ class DeviceOperator:
         vf, rp = C.c_int(0), C.c_int(0)
         lib().ainv_csr_solve_info(self._h, C.byref(vf), C.byref(rp))
         return SolveResult(info, it.value, err.value, vf.value, rp.value)
+
+    def block_solve(self, B, X, factors: DeviceFactors | None = None, eps=1e-9, itmax=1000,
+                    stream=None) -> "BlockSolveResult":
+        """CG on the m columns of B (a CUDA float64 tensor of shape (n, m),
+        m <= 32, row-major): one SpMM per product for all columns, each column
+        with its own recurrence.  X (same shape) holds x0 and receives the
+        solutions.  Statuses are returned per column instead of raised."""
+        if B.dim() != 2 or B.shape != X.shape or B.shape[0] != self.n:
+            raise ValueError("B and X must both have shape (n, m)")
+        m = B.shape[1]
+        it = (C.c_int * m)()
+        err = (C.c_double * m)()
+        st = (C.c_int * m)()
+        info = lib().ainv_gpu_block_solve(factors.handle if factors is not None else None,
+                                          self._h, m, dptr(B), m, dptr(X), m, eps, itmax, it,
+                                          err, st, _stream(stream))
+        if info not in (SUCCESS, 4102, 4103, 4104):
+            check(info)
+        return BlockSolveResult(info, list(it), list(err), list(st))
 
     def close(self) -> None:
         if self._h:

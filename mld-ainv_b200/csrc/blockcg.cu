@@ -1,0 +1,588 @@
+// Multi-right-hand-side preconditioned CG: up to 32 systems A x_l = b_l
+// solved together, every matrix pass shared by all of them.
+//
+// Multivectors are row-interleaved with a stride of 32 columns: entry
+// (row, l) at v[row * 32 + l], so the 32 values of one row are one 256-byte
+// line.  Every product is an SpMM over the sliced layout in which one warp
+// takes one 32-row slice and lane l is column l: a slot's 32 values are
+// loaded once (coalesced, one per row), broadcast row by row with shuffles,
+// and each broadcast value multiplies a whole gathered row of the input
+// multivector (one 256 B line).  The matrix streams once per iteration for
+// all columns instead of once per column.
+//
+// Each column follows the PSBLAS CG recurrence (psb_dcg, istop=2, as driven
+// at tests/pdegen/ppde3d.f90:280-281) with its own scalars: the column-wise
+// form of block CG, so every column iterates exactly as a single-vector solve
+// would (the per-row products accumulate in the same order as the
+// single-vector kernels) and stops on its own criterion; converged columns
+// stay frozen while the others continue.  The preconditioner runs in the
+// factors' precision (FP32 multivector intermediate for FP32/BF16 factors),
+// A, the recurrence, dots and norms in FP64, with the true-residual checks of
+// the single-vector loop.
+#include <algorithm>
+#include <cstdint>
+#include <cstdlib>
+#include <new>
+
+#include "kstate.cuh"
+#include "sell_device.cuh"
+
+namespace ainv {
+namespace mrhs {
+
+using namespace dev;
+using namespace kstate;
+
+constexpr int kCols = 32;    // multivector stride (columns per row)
+constexpr int kChunk = 8;    // iterations per captured graph launch
+constexpr int kRecheck = 50; // true-residual period for FP32/BF16 factors
+
+struct MState {
+  KState col[kCols];
+  int m;
+  int alldone;  // every column finished (converged and confirmed, or failed)
+  unsigned ticket;
+  int pad;
+};
+
+// ---------------------------------------------------------------- device --
+// acc[r] = row (32 s + r) of M times column `lane` of x (stride 32).  Slot
+// order and fma sequence per row are those of the single-vector kernels.
+template <class V, class X, class A>
+__device__ __forceinline__ void slice_mm(const SellView<V> &m, int pack, int s,
+                                         const X *__restrict__ x, A (&acc)[kCols]) {
+  const int lane = threadIdx.x & 31;
+  const int vb = __ldg(m.sptr + s), ve = __ldg(m.sptr + s + 1);
+  const int ib = __ldg(m.iptr + s), ie = __ldg(m.iptr + s + 1);
+  const int w = (ve - vb) / kSlice;
+  const bool om = (ie - ib) == w;
+  const int row0 = s * kSlice;
+#pragma unroll
+  for (int r = 0; r < kCols; r++) acc[r] = A(0);
+  for (int k = 0; k < w; k++) {
+    const int pos = (k / pack) * (kSlice * pack) + lane * pack + (k % pack);
+    const A v = (A)ldv(m.val + vb + pos);
+    if (om) {
+      const int off = __ldg(m.idx + ib + k);
+#pragma unroll
+      for (int r = 0; r < kCols; r++) {
+        const A vr = __shfl_sync(0xffffffffu, v, r);
+        const int cr = row0 + r + off;
+        const A xv = (vr != A(0) && (unsigned)cr < (unsigned)m.n)
+                         ? (A)__ldg(x + (size_t)cr * kCols + lane) : A(0);
+        acc[r] = fma(vr, xv, acc[r]);
+      }
+    } else {
+      const int c = __ldcs(m.idx + ib + pos);
+#pragma unroll
+      for (int r = 0; r < kCols; r++) {
+        const A vr = __shfl_sync(0xffffffffu, v, r);
+        const int cr = __shfl_sync(0xffffffffu, c, r);
+        const A xv = (vr != A(0) && (unsigned)cr < (unsigned)m.n)
+                         ? (A)__ldg(x + (size_t)cr * kCols + lane) : A(0);
+        acc[r] = fma(vr, xv, acc[r]);
+      }
+    }
+  }
+}
+
+// Visit every slice of M (warps striding over the grid): epi(row, acc) for
+// each of the slice's rows < n, lane = column.
+template <class V, class X, class Epi>
+__device__ __forceinline__ void for_each_slice(const SellView<V> &m, int pack,
+                                               const X *__restrict__ x, Epi &&epi) {
+  using A = typename Acc<V>::type;
+  for (int s = first_slice(); s < m.nslices; s += slice_stride()) {
+    A acc[kCols];
+    slice_mm(m, pack, s, x, acc);
+#pragma unroll
+    for (int r = 0; r < kCols; r++) {
+      const int row = s * kSlice + r;
+      if (row < m.n) epi(row, acc[r]);
+    }
+  }
+}
+
+// Per-column grid sums.  Each thread holds partials for column
+// (threadIdx.x & 31); blocks fold their warps in order, store one partial
+// per column, and the last block (atomic ticket) folds the block partials in
+// block order, warp w taking blocks w, w+8, ... and the warps then combined
+// in order.  Returns true in the last block; totals in warp 0, lane = column.
+template <int NV>
+__device__ __forceinline__ bool col_sum(double (&v)[NV], double *__restrict__ partials,
+                                        unsigned *ticket) {
+  __shared__ double sh[NV][kWarps][kCols];
+  __shared__ bool is_last;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int G = gridDim.x;
+#pragma unroll
+  for (int i = 0; i < NV; i++) sh[i][warp][lane] = v[i];
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int i = 0; i < NV; i++) {
+      double s = 0.0;
+      for (int w = 0; w < kWarps; w++) s += sh[i][w][lane];
+      partials[((size_t)i * kCols + lane) * G + blockIdx.x] = s;
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) is_last = atomicAdd(ticket, 1u) == (unsigned)G - 1;
+  __syncthreads();
+  if (!is_last) return false;
+  __threadfence();
+#pragma unroll
+  for (int i = 0; i < NV; i++) {
+    double s = 0.0;
+    for (int b = warp; b < G; b += kWarps) s += __ldcg(partials + ((size_t)i * kCols + lane) * G + b);
+    sh[i][warp][lane] = s;
+  }
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int i = 0; i < NV; i++) {
+      double s = 0.0;
+      for (int w = 0; w < kWarps; w++) s += sh[i][w][lane];
+      v[i] = s;
+    }
+    if (lane == 0) *ticket = 0u;
+  }
+  return true;
+}
+
+__device__ __forceinline__ bool finished(const KState &c) {
+  return c.done && (c.verified || c.status != AINV_SUCCESS);
+}
+
+// Called by warp 0 of a last block after its per-column updates.
+__device__ __forceinline__ void update_alldone(MState *ms) {
+  const int lane = threadIdx.x & 31;
+  const bool f = lane >= ms->m || finished(ms->col[lane]);
+  const bool all = __all_sync(0xffffffffu, f);
+  if (lane == 0) ms->alldone = all ? 1 : 0;
+}
+
+// R = B - A X, ||b_l||, ||r_l|| (initial state of every column).
+__global__ void __launch_bounds__(kBlock)
+    k_mv_init(SellView<double> a, int apack, const double *__restrict__ X,
+              const double *__restrict__ B, double *__restrict__ R, MState *ms,
+              double *partials) {
+  const int lane = threadIdx.x & 31;
+  double pr[2] = {0.0, 0.0};
+  for_each_slice(a, apack, X, [&](int row, double acc) {
+    const size_t e = (size_t)row * kCols + lane;
+    const double bi = B[e];
+    const double ri = bi - acc;
+    R[e] = ri;
+    pr[0] += ri * ri;
+    pr[1] += bi * bi;
+  });
+  if (col_sum<2>(pr, partials, &ms->ticket) && threadIdx.x < 32) {
+    if (lane < ms->m) {
+      KState *st = &ms->col[lane];
+      const double bn = sqrt(pr[1]);
+      st->bn2 = (bn == 0.0) ? 1.0 : bn;
+      const double p3[3] = {pr[0], 0.0, 0.0};
+      finish_dots<kInit>(st, p3, false, nullptr);
+    }
+    update_alldone(ms);
+  }
+}
+
+// Sweep 1 of the apply on all columns: T = D^-1 .* (W^T R).
+template <class V, class T>
+__global__ void __launch_bounds__(kBlock)
+    k_mv_sweep1(SellView<V> m, int pack, const double *__restrict__ R, const V *__restrict__ d,
+                T *__restrict__ Tm, const MState *ms) {
+  if (ms->alldone) return;
+  const int lane = threadIdx.x & 31;
+  for_each_slice(m, pack, R, [&](int row, auto acc) {
+    Tm[(size_t)row * kCols + lane] = (T)(ldd(d + row) * acc);
+  });
+}
+
+// Sweep 2 on all columns: Zv = Z T, with rho_l = r_l . z_l and beta_l.
+template <class V, class T>
+__global__ void __launch_bounds__(kBlock)
+    k_mv_sweep2(SellView<V> m, int pack, const T *__restrict__ Tm, const double *__restrict__ R,
+                double *__restrict__ Zv, MState *ms, double *partials) {
+  if (ms->alldone) return;
+  const int lane = threadIdx.x & 31;
+  double pr[1] = {0.0};
+  for_each_slice(m, pack, Tm, [&](int row, auto acc) {
+    const size_t e = (size_t)row * kCols + lane;
+    const double zi = (double)acc;
+    Zv[e] = zi;
+    pr[0] += R[e] * zi;
+  });
+  if (col_sum<1>(pr, partials, &ms->ticket) && threadIdx.x < 32) {
+    if (lane < ms->m && !ms->col[lane].done) cg_take_rho(&ms->col[lane], pr[0]);
+    update_alldone(ms);
+  }
+}
+
+// Unpreconditioned: Zv = R, rho = r.r.
+__global__ void __launch_bounds__(kBlock)
+    k_mv_ident(long long ne, const double *__restrict__ R, double *__restrict__ Zv, MState *ms,
+               double *partials) {
+  if (ms->alldone) return;
+  double pr[1] = {0.0};
+  for (long long e = (long long)blockIdx.x * kBlock + threadIdx.x; e < ne;
+       e += (long long)gridDim.x * kBlock) {
+    Zv[e] = R[e];
+    pr[0] += R[e] * R[e];
+  }
+  const int lane = threadIdx.x & 31;
+  if (col_sum<1>(pr, partials, &ms->ticket) && threadIdx.x < 32) {
+    if (lane < ms->m && !ms->col[lane].done) cg_take_rho(&ms->col[lane], pr[0]);
+    update_alldone(ms);
+  }
+}
+
+// P = Zv (first iteration of the column) or Zv + beta_l P.
+__global__ void __launch_bounds__(kBlock)
+    k_mv_p(long long ne, const double *__restrict__ Zv, double *__restrict__ P,
+           const MState *ms) {
+  if (ms->alldone) return;
+  const int lane = threadIdx.x & 31;  // element e has column e % 32 = lane
+  const KState &c = ms->col[lane];
+  if (lane >= ms->m || c.done) return;
+  const bool first = c.iter == 0;
+  const double beta = c.beta;
+  for (long long e = (long long)blockIdx.x * kBlock + threadIdx.x; e < ne;
+       e += (long long)gridDim.x * kBlock)
+    P[e] = first ? Zv[e] : Zv[e] + beta * P[e];
+}
+
+// Q = A P with sigma_l = p_l . q_l, alpha_l = rho_l / sigma_l.
+__global__ void __launch_bounds__(kBlock)
+    k_mv_spmm_sigma(SellView<double> a, int apack, const double *__restrict__ P,
+                    double *__restrict__ Q, MState *ms, double *partials) {
+  if (ms->alldone) return;
+  const int lane = threadIdx.x & 31;
+  double pr[1] = {0.0};
+  for_each_slice(a, apack, P, [&](int row, double acc) {
+    const size_t e = (size_t)row * kCols + lane;
+    Q[e] = acc;
+    pr[0] += P[e] * acc;
+  });
+  if (col_sum<1>(pr, partials, &ms->ticket) && threadIdx.x < 32) {
+    if (lane < ms->m && !ms->col[lane].done) {
+      const double p3[3] = {pr[0], 0.0, 0.0};
+      finish_dots<kCgSigma>(&ms->col[lane], p3, false, nullptr);
+    }
+    update_alldone(ms);
+  }
+}
+
+// X += alpha_l P, R -= alpha_l Q, ||r_l||^2 and the convergence test.
+__global__ void __launch_bounds__(kBlock)
+    k_mv_xr(long long ne, const double *__restrict__ P, const double *__restrict__ Q,
+            double *__restrict__ X, double *__restrict__ R, MState *ms, double *partials) {
+  if (ms->alldone) return;
+  const int lane = threadIdx.x & 31;
+  const bool live = lane < ms->m && !ms->col[lane].done;
+  const double alpha = ms->col[lane].alpha;
+  double pr[1] = {0.0};
+  if (live) {
+    for (long long e = (long long)blockIdx.x * kBlock + threadIdx.x; e < ne;
+         e += (long long)gridDim.x * kBlock) {
+      X[e] = X[e] + alpha * P[e];
+      const double ri = R[e] - alpha * Q[e];
+      R[e] = ri;
+      pr[0] += ri * ri;
+    }
+  }
+  if (col_sum<1>(pr, partials, &ms->ticket) && threadIdx.x < 32) {
+    if (live) finish_iteration(&ms->col[lane], pr[0]);
+    update_alldone(ms);
+  }
+}
+
+// Which columns take a true-residual pass this iteration (as the
+// single-vector kTrueRes kernel decides per solve).
+__device__ __forceinline__ bool col_verify(const KState &c) {
+  return c.done && c.status == AINV_SUCCESS && !c.verified;
+}
+__device__ __forceinline__ bool col_periodic(const KState &c) {
+  return !c.done && c.check_every > 0 && c.iter > 0 && c.iter % c.check_every == 0;
+}
+
+// Rt = B - A X against R for the columns that need a check; decides
+// confirmation / replacement per column (finish_dots<kTrueRes>).
+__global__ void __launch_bounds__(kBlock)
+    k_mv_trueres(SellView<double> a, int apack, const double *__restrict__ X,
+                 const double *__restrict__ B, const double *__restrict__ R,
+                 double *__restrict__ Rt, MState *ms, double *partials) {
+  if (ms->alldone) return;
+  const int lane = threadIdx.x & 31;
+  const KState &c = ms->col[lane];
+  const bool mine = lane < ms->m && (col_verify(c) || col_periodic(c));
+  const bool verify = lane < ms->m && col_verify(c);
+  if (!__syncthreads_or(mine)) return;  // no column needs a check
+  double pr[3] = {0.0, 0.0, 0.0};
+  for_each_slice(a, apack, X, [&](int row, double acc) {
+    const size_t e = (size_t)row * kCols + lane;
+    const double ri = B[e] - acc;
+    Rt[e] = ri;
+    pr[0] += ri * ri;
+    const double g = ri - R[e];
+    pr[1] += g * g;
+  });
+  if (col_sum<3>(pr, partials, &ms->ticket) && threadIdx.x < 32) {
+    if (mine) finish_dots<kTrueRes>(&ms->col[lane], pr, verify, nullptr);
+    update_alldone(ms);
+  }
+}
+
+// R := Rt for the columns whose check asked for a replacement.
+__global__ void __launch_bounds__(kBlock)
+    k_mv_replace(long long ne, const double *__restrict__ Rt, double *__restrict__ R,
+                 const MState *ms) {
+  const int lane = threadIdx.x & 31;
+  if (lane >= ms->m || !ms->col[lane].replace) return;
+  for (long long e = (long long)blockIdx.x * kBlock + threadIdx.x; e < ne;
+       e += (long long)gridDim.x * kBlock)
+    R[e] = Rt[e];
+}
+
+// Caller layout (n x m, leading dimension ld) <-> stride-32 multivector.
+__global__ void __launch_bounds__(kBlock)
+    k_mv_gather(int n, int m, int ld, const double *__restrict__ src, double *__restrict__ dst) {
+  const long long ne = (long long)n * kCols;
+  for (long long e = (long long)blockIdx.x * kBlock + threadIdx.x; e < ne;
+       e += (long long)gridDim.x * kBlock) {
+    const int l = (int)(e & (kCols - 1));
+    const long long row = e >> 5;
+    dst[e] = l < m ? src[row * ld + l] : 0.0;
+  }
+}
+__global__ void __launch_bounds__(kBlock)
+    k_mv_scatter(int n, int m, int ld, const double *__restrict__ src, double *__restrict__ dst) {
+  const long long ne = (long long)n * kCols;
+  for (long long e = (long long)blockIdx.x * kBlock + threadIdx.x; e < ne;
+       e += (long long)gridDim.x * kBlock) {
+    const int l = (int)(e & (kCols - 1));
+    if (l < m) dst[(e >> 5) * ld + l] = src[e];
+  }
+}
+
+// ------------------------------------------------------------------ host --
+enum { MX = 0, MB, MR, MZ, MP, MQ, MRT, kNumMv };
+
+}  // namespace mrhs
+
+struct MrhsWs {
+  int n = 0, G = 0;
+  size_t stride = 0;       // doubles per multivector (n * 32)
+  double *mv = nullptr;    // 7 FP64 multivectors
+  void *t = nullptr;       // apply intermediate (n * 32 of double or float)
+  double *partials = nullptr;
+  mrhs::MState *st = nullptr, *hst = nullptr;
+  cudaStream_t s = nullptr;
+  cudaEvent_t ev = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  unsigned long long key_serial = ~0ull;
+  double *v(int i) const { return mv + (size_t)i * stride; }
+};
+
+void destroy_mws(MrhsWs *w) {
+  if (!w) return;
+  if (w->exec) cudaGraphExecDestroy(w->exec);
+  if (w->mv) cudaFree(w->mv);
+  if (w->t) cudaFree(w->t);
+  if (w->partials) cudaFree(w->partials);
+  if (w->st) cudaFree(w->st);
+  if (w->hst) cudaFreeHost(w->hst);
+  if (w->ev) cudaEventDestroy(w->ev);
+  if (w->s) cudaStreamDestroy(w->s);
+  delete w;
+}
+
+namespace mrhs {
+namespace {
+
+int get_ws(ainv_csr *a, MrhsWs **out) {
+  if (a->mws) {
+    *out = a->mws;
+    return AINV_SUCCESS;
+  }
+  MrhsWs *w = new (std::nothrow) MrhsWs;
+  if (!w) {
+    set_error("block solve workspace: host allocation failed");
+    return AINV_ERR_ALLOC;
+  }
+  int sms = 148, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  w->n = a->n;
+  w->stride = (size_t)a->n * kCols;
+  w->G = std::max(1, std::min(grid_for(a->a.nslices), 4 * sms));
+  cudaError_t e = cudaMalloc(&w->mv, sizeof(double) * kNumMv * w->stride);
+  if (e == cudaSuccess) e = cudaMalloc(&w->t, sizeof(double) * w->stride);
+  if (e == cudaSuccess) e = cudaMalloc(&w->partials, sizeof(double) * 3 * kCols * (size_t)w->G);
+  if (e == cudaSuccess) e = cudaMalloc(&w->st, sizeof(MState));
+  if (e == cudaSuccess) e = cudaMallocHost(&w->hst, sizeof(MState));
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&w->s, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&w->ev, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaMemset(w->mv, 0, sizeof(double) * kNumMv * w->stride);
+  if (e != cudaSuccess) {
+    destroy_mws(w);
+    set_error("block solve workspace allocation failed: %s", cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? AINV_ERR_ALLOC : AINV_ERR_CUDA;
+  }
+  a->mws = w;
+  *out = w;
+  return AINV_SUCCESS;
+}
+
+template <class V, class T>
+void launch_precond(const MrhsWs *w, const ainv_handle *h, cudaStream_t s) {
+  const SellView<V> wt = view<V>(h->wt), z = view<V>(h->z);
+  k_mv_sweep1<V, T><<<w->G, kBlock, 0, s>>>(wt, h->wt.pack, w->v(MR), (const V *)h->d, (T *)w->t,
+                                           w->st);
+  k_mv_sweep2<V, T><<<w->G, kBlock, 0, s>>>(z, h->z.pack, (const T *)w->t, w->v(MR), w->v(MZ),
+                                           w->st, w->partials);
+}
+
+int enqueue_iteration(const MrhsWs *w, const ainv_handle *h, const ainv_csr *a) {
+  const cudaStream_t s = w->s;
+  const long long ne = (long long)w->stride;
+  const int Gv = (int)std::min<long long>((ne + kBlock - 1) / kBlock, (long long)w->G);
+  const SellView<double> A = view<double>(a->a);
+  if (h) {
+    switch (h->prec) {
+      case AINV_PREC_FP64: launch_precond<double, double>(w, h, s); break;
+      case AINV_PREC_FP32: launch_precond<float, float>(w, h, s); break;
+      default: launch_precond<__nv_bfloat16, float>(w, h, s); break;
+    }
+  } else {
+    k_mv_ident<<<Gv, kBlock, 0, s>>>(ne, w->v(MR), w->v(MZ), w->st, w->partials);
+  }
+  k_mv_p<<<Gv, kBlock, 0, s>>>(ne, w->v(MZ), w->v(MP), w->st);
+  k_mv_spmm_sigma<<<w->G, kBlock, 0, s>>>(A, a->a.pack, w->v(MP), w->v(MQ), w->st, w->partials);
+  k_mv_xr<<<Gv, kBlock, 0, s>>>(ne, w->v(MP), w->v(MQ), w->v(MX), w->v(MR), w->st, w->partials);
+  k_mv_trueres<<<w->G, kBlock, 0, s>>>(A, a->a.pack, w->v(MX), w->v(MB), w->v(MR), w->v(MRT),
+                                       w->st, w->partials);
+  k_mv_replace<<<Gv, kBlock, 0, s>>>(ne, w->v(MRT), w->v(MR), w->st);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_error("block solve launch failed: %s", cudaGetErrorString(e));
+    return AINV_ERR_CUDA;
+  }
+  return AINV_SUCCESS;
+}
+
+int ensure_graph(MrhsWs *w, const ainv_handle *h, const ainv_csr *a) {
+  const unsigned long long key = h ? h->serial : 0ull;
+  if (w->exec && w->key_serial == key) return AINV_SUCCESS;
+  if (w->exec) {
+    cudaGraphExecDestroy(w->exec);
+    w->exec = nullptr;
+  }
+  AINV_CUDA_TRY(cudaStreamBeginCapture(w->s, cudaStreamCaptureModeThreadLocal));
+  int rc = AINV_SUCCESS;
+  for (int k = 0; k < kChunk && rc == AINV_SUCCESS; k++) rc = enqueue_iteration(w, h, a);
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(w->s, &g);
+  if (rc != AINV_SUCCESS || e != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    if (rc == AINV_SUCCESS) set_error("block solve capture failed: %s", cudaGetErrorString(e));
+    return rc != AINV_SUCCESS ? rc : AINV_ERR_CUDA;
+  }
+  const cudaError_t ei = cudaGraphInstantiate(&w->exec, g, 0);
+  cudaGraphDestroy(g);
+  if (ei != cudaSuccess) {
+    w->exec = nullptr;
+    set_error("block solve graph instantiate failed: %s", cudaGetErrorString(ei));
+    return AINV_ERR_CUDA;
+  }
+  w->key_serial = key;
+  return AINV_SUCCESS;
+}
+
+}  // namespace
+}  // namespace mrhs
+}  // namespace ainv
+
+extern "C" int ainv_gpu_block_solve(ainv_handle *h, const ainv_csr *ac, int m, const double *B,
+                                    int ldb, double *X, int ldx, double eps, int itmax,
+                                    int *iters, double *errs, int *status, void *stream) {
+  using namespace ainv;
+  using namespace ainv::mrhs;
+  ainv_csr *a = const_cast<ainv_csr *>(ac);
+  if (!a || !B || !X || m < 1 || m > kCols || ldb < m || ldx < m) {
+    set_error("ainv_gpu_block_solve: invalid arguments (m must be 1..%d, ld >= m)", kCols);
+    return AINV_ERR_ARG;
+  }
+  if (h && h->n != a->n) {
+    set_error("ainv_gpu_block_solve: preconditioner size %d != operator size %d", h->n, a->n);
+    return AINV_ERR_ARG;
+  }
+  if (!(eps > 0.0) || itmax < 0) {
+    set_error("ainv_gpu_block_solve: invalid eps/itmax");
+    return AINV_ERR_ARG;
+  }
+  MrhsWs *w = nullptr;
+  AINV_TRY(get_ws(a, &w));
+  const cudaStream_t user = (cudaStream_t)stream;
+  const int n = a->n;
+  const int Gc = std::max(1, std::min(w->G, (int)(((long long)n * kCols + kBlock - 1) / kBlock)));
+  AINV_CUDA_TRY(cudaEventRecord(w->ev, user));
+  AINV_CUDA_TRY(cudaStreamWaitEvent(w->s, w->ev, 0));
+  k_mv_gather<<<Gc, kBlock, 0, w->s>>>(n, m, ldb, B, w->v(MB));
+  k_mv_gather<<<Gc, kBlock, 0, w->s>>>(n, m, ldx, X, w->v(MX));
+  MState init{};
+  init.m = m;
+  for (int l = 0; l < kCols; l++) {
+    KState &c = init.col[l];
+    c.eps = eps;
+    c.itmax = itmax;
+    c.method = AINV_KRYLOV_CG;
+    c.check_every = (h && h->prec != AINV_PREC_FP64) ? kRecheck : 0;
+    if (l >= m) {  // unused lanes: finished from the start
+      c.done = 1;
+      c.verified = 1;
+    }
+  }
+  *w->hst = init;
+  AINV_CUDA_TRY(cudaMemcpyAsync(w->st, w->hst, sizeof(MState), cudaMemcpyHostToDevice, w->s));
+  k_mv_init<<<w->G, kBlock, 0, w->s>>>(view<double>(a->a), a->a.pack, w->v(MX), w->v(MB),
+                                       w->v(MR), w->st, w->partials);
+  AINV_CUDA_TRY(cudaGetLastError());
+  const bool use_graph = getenv("AINV_NO_GRAPH") == nullptr;
+  const long max_chunks = (long)itmax / kChunk + 2 + 4 * kMaxVerifyFails;
+  for (long c = 0; c < max_chunks; c++) {
+    AINV_CUDA_TRY(cudaMemcpyAsync(w->hst, w->st, sizeof(MState), cudaMemcpyDeviceToHost, w->s));
+    AINV_CUDA_TRY(cudaStreamSynchronize(w->s));
+    if (w->hst->alldone) break;
+    if (use_graph && c > 0) {
+      AINV_TRY(ensure_graph(w, h, a));
+      AINV_CUDA_TRY(cudaGraphLaunch(w->exec, w->s));
+    } else {
+      for (int k = 0; k < kChunk; k++) AINV_TRY(enqueue_iteration(w, h, a));
+    }
+  }
+  k_mv_scatter<<<Gc, kBlock, 0, w->s>>>(n, m, ldx, w->v(MX), X);
+  AINV_CUDA_TRY(cudaMemcpyAsync(w->hst, w->st, sizeof(MState), cudaMemcpyDeviceToHost, w->s));
+  AINV_CUDA_TRY(cudaStreamSynchronize(w->s));
+  AINV_CUDA_TRY(cudaEventRecord(w->ev, w->s));
+  AINV_CUDA_TRY(cudaStreamWaitEvent(user, w->ev, 0));
+  const MState &f = *w->hst;
+  int rc = AINV_SUCCESS;
+  for (int l = 0; l < m; l++) {
+    const KState &c = f.col[l];
+    if (iters) iters[l] = c.iter;
+    if (errs) errs[l] = sqrt(c.rn2) / c.bn2;
+    const int sl = c.done ? c.status : AINV_ERR_INTERNAL;
+    if (status) status[l] = sl;
+    if (sl != AINV_SUCCESS && rc == AINV_SUCCESS) rc = sl;
+  }
+  if (!f.alldone) {
+    set_error("block solve did not terminate");
+    return AINV_ERR_INTERNAL;
+  }
+  if (rc != AINV_SUCCESS) set_error("block solve: a column ended with status %d", rc);
+  return rc;
+}

@@ -256,6 +256,7 @@ int ainv_csr_spmv(const ainv_csr *a, double alpha, const double *x_dev, double b
 int ainv_csr_destroy(ainv_csr *a) {
   if (a) {
     ainv::destroy_ws(a->ws);
+    ainv::destroy_mws(a->mws);
     ainv::free_sell(a->a);
     if (a->status) cudaFree(a->status);
     delete a;

@@ -121,6 +121,8 @@ int upload_values(const double *h, size_t n, int prec, void **dptr);
 namespace ainv {
 struct KrylovWs;
 void destroy_ws(KrylovWs *w);
+struct MrhsWs;
+void destroy_mws(MrhsWs *w);
 // Process-unique id for handles (keys cached CUDA graphs; never reused).
 unsigned long long next_serial();
 }  // namespace ainv
@@ -146,6 +148,7 @@ struct ainv_csr {
   int *status = nullptr;  // device word: nonzero after a streaming wait timed out
   ainv::DevSell a;
   ainv::KrylovWs *ws = nullptr;  // Krylov vectors, state and captured graph
+  ainv::MrhsWs *mws = nullptr;   // the same for multi-right-hand-side solves
 };
 
 // ------------------------------------------------------------- kernels --

@@ -231,19 +231,7 @@ __global__ void __launch_bounds__(kBlock)
     z[i] = zi;
     pr[0] += r[i] * zi;
   });
-  if (grid_sum<1>(pr, partials, &st->ticket[0]) && threadIdx.x == 0) {
-    st->replace = 0;
-    st->rho_old = st->rho;
-    st->rho = pr[0];
-    if (st->iter > 0) {
-      if (st->rho_old == 0.0) {
-        st->status = AINV_ERR_BREAKDOWN;
-        st->done = 1;
-      } else {
-        st->beta = st->rho / st->rho_old;
-      }
-    }
-  }
+  if (grid_sum<1>(pr, partials, &st->ticket[0]) && threadIdx.x == 0) cg_take_rho(st, pr[0]);
 }
 
 // CG without preconditioner: z = r, rho = r.r.
@@ -256,19 +244,7 @@ __global__ void __launch_bounds__(kBlock)
     z[i] = r[i];
     pr[0] += r[i] * r[i];
   }
-  if (grid_sum<1>(pr, partials, &st->ticket[0]) && threadIdx.x == 0) {
-    st->replace = 0;
-    st->rho_old = st->rho;
-    st->rho = pr[0];
-    if (st->iter > 0) {
-      if (st->rho_old == 0.0) {
-        st->status = AINV_ERR_BREAKDOWN;
-        st->done = 1;
-      } else {
-        st->beta = st->rho / st->rho_old;
-      }
-    }
-  }
+  if (grid_sum<1>(pr, partials, &st->ticket[0]) && threadIdx.x == 0) cg_take_rho(st, pr[0]);
 }
 
 // CG: p = z (first iteration) or p = z + beta p.

@@ -44,6 +44,21 @@ __device__ __forceinline__ void finish_iteration(KState *st, double rn2) {
   }
 }
 
+// CG: rho = r.z from the preconditioner sweep, then beta = rho / rho_old.
+__device__ __forceinline__ void cg_take_rho(KState *st, double rho) {
+  st->replace = 0;
+  st->rho_old = st->rho;
+  st->rho = rho;
+  if (st->iter > 0) {
+    if (st->rho_old == 0.0) {
+      st->status = AINV_ERR_BREAKDOWN;
+      st->done = 1;
+    } else {
+      st->beta = st->rho / st->rho_old;
+    }
+  }
+}
+
 // BiCGSTAB: start the next iteration's scalars from rho = rt.r.
 __device__ __forceinline__ void bicg_next_rho(KState *st, double rr) {
   if (st->done) return;
