@@ -3,12 +3,12 @@
 //
 // Multivectors are row-interleaved with a stride of 32 columns: entry
 // (row, l) at v[row * 32 + l], so the 32 values of one row are one 256-byte
-// line.  Every product is an SpMM over the sliced layout in which one warp
-// takes one 32-row slice and lane l is column l: a slot's 32 values are
-// loaded once (coalesced, one per row), broadcast row by row with shuffles,
-// and each broadcast value multiplies a whole gathered row of the input
-// multivector (one 256 B line).  The matrix streams once per iteration for
-// all columns instead of once per column.
+// line.  Every product is an SpMM over the sliced layout: a warp walks one
+// 32-row slice four rows at a time, 8 lanes per row, each lane owning 4
+// columns, so every matrix entry is loaded once and multiplies a whole
+// gathered row of the input multivector (8 lanes x 32 bytes = one 256-byte
+// line).  The matrix streams once per iteration for all columns instead of
+// once per column.
 //
 // Each column follows the PSBLAS CG recurrence (psb_dcg, istop=2, as driven
 // at tests/pdegen/ppde3d.f90:280-281) with its own scalars: the column-wise
@@ -46,87 +46,123 @@ struct MState {
 };
 
 // ---------------------------------------------------------------- device --
-// acc[r] = row (32 s + r) of M times column `lane` of x (stride 32).  Slot
-// order and fma sequence per row are those of the single-vector kernels.
+// Lane map of the SpMM kernels: a warp works on 4 rows of a slice at a time,
+// lane = 8 q + g takes row q of the four and columns 4g .. 4g+3, so the 8
+// lanes of a row read its 32 columns as one 256-byte line (32 bytes each).
+constexpr int kColsPerLane = 4;
+constexpr int kRowsPerStep = kSlice / 8;  // 4
+constexpr int kSlotBatch = 4;
+
+__device__ __forceinline__ void ldg4(const double *p, double (&o)[4]) {
+  const double2 a = __ldg(reinterpret_cast<const double2 *>(p));
+  const double2 b = __ldg(reinterpret_cast<const double2 *>(p) + 1);
+  o[0] = a.x;
+  o[1] = a.y;
+  o[2] = b.x;
+  o[3] = b.y;
+}
+__device__ __forceinline__ void ldg4(const float *p, float (&o)[4]) {
+  const float4 a = __ldg(reinterpret_cast<const float4 *>(p));
+  o[0] = a.x;
+  o[1] = a.y;
+  o[2] = a.z;
+  o[3] = a.w;
+}
+__device__ __forceinline__ void ld4(const double *p, double (&o)[4]) {
+  const double2 a = reinterpret_cast<const double2 *>(p)[0];
+  const double2 b = reinterpret_cast<const double2 *>(p)[1];
+  o[0] = a.x;
+  o[1] = a.y;
+  o[2] = b.x;
+  o[3] = b.y;
+}
+__device__ __forceinline__ void st4(double *p, const double (&v)[4]) {
+  reinterpret_cast<double2 *>(p)[0] = make_double2(v[0], v[1]);
+  reinterpret_cast<double2 *>(p)[1] = make_double2(v[2], v[3]);
+}
+__device__ __forceinline__ void st4(float *p, const float (&v)[4]) {
+  *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+
+// acc[e] = row `row` (slice-local rs) of M times column c0 + e of x.  Slots
+// are taken kSlotBatch at a time: their values and index words load
+// together, then the batch's gathers (skipped where the value is 0) are all
+// in flight before the first fma.  Slot order and fma sequence per (row,
+// column) are those of the single-vector kernels.
 template <class V, class X, class A>
-__device__ __forceinline__ void slice_mm(const SellView<V> &m, int pack, int s,
-                                         const X *__restrict__ x, A (&acc)[kCols]) {
-  const int lane = threadIdx.x & 31;
-  const int vb = __ldg(m.sptr + s), ve = __ldg(m.sptr + s + 1);
-  const int ib = __ldg(m.iptr + s), ie = __ldg(m.iptr + s + 1);
-  const int w = (ve - vb) / kSlice;
-  const bool om = (ie - ib) == w;
-  const int row0 = s * kSlice;
+__device__ __forceinline__ void row_mm(const SellView<V> &m, int pack, int vb, int ib, int w,
+                                       bool om, int row, int rs, const X *__restrict__ x, int c0,
+                                       A (&acc)[kColsPerLane]) {
 #pragma unroll
-  for (int r = 0; r < kCols; r++) acc[r] = A(0);
-  for (int k = 0; k < w; k++) {
-    const int pos = (k / pack) * (kSlice * pack) + lane * pack + (k % pack);
-    const A v = (A)ldv(m.val + vb + pos);
-    if (om) {
-      const int off = __ldg(m.idx + ib + k);
+  for (int e = 0; e < kColsPerLane; e++) acc[e] = A(0);
+  for (int k0 = 0; k0 < w; k0 += kSlotBatch) {
+    A v[kSlotBatch];
+    int c[kSlotBatch];
 #pragma unroll
-      for (int r = 0; r < kCols; r++) {
-        const A vr = __shfl_sync(0xffffffffu, v, r);
-        const int cr = row0 + r + off;
-        const A xv = (vr != A(0) && (unsigned)cr < (unsigned)m.n)
-                         ? (A)__ldg(x + (size_t)cr * kCols + lane) : A(0);
-        acc[r] = fma(vr, xv, acc[r]);
-      }
-    } else {
-      const int c = __ldcs(m.idx + ib + pos);
-#pragma unroll
-      for (int r = 0; r < kCols; r++) {
-        const A vr = __shfl_sync(0xffffffffu, v, r);
-        const int cr = __shfl_sync(0xffffffffu, c, r);
-        const A xv = (vr != A(0) && (unsigned)cr < (unsigned)m.n)
-                         ? (A)__ldg(x + (size_t)cr * kCols + lane) : A(0);
-        acc[r] = fma(vr, xv, acc[r]);
+    for (int j = 0; j < kSlotBatch; j++) {
+      const int k = k0 + j;
+      if (k < w) {
+        const int pos = (k / pack) * (kSlice * pack) + rs * pack + (k % pack);
+        v[j] = (A)ldv(m.val + vb + pos);
+        c[j] = om ? row + __ldg(m.idx + ib + k) : __ldcs(m.idx + ib + pos);
+      } else {
+        v[j] = A(0);
+        c[j] = 0;
       }
     }
+    A xv[kSlotBatch][kColsPerLane];
+#pragma unroll
+    for (int j = 0; j < kSlotBatch; j++) {
+      if (v[j] != A(0) && (unsigned)c[j] < (unsigned)m.n) {
+        X t[kColsPerLane];
+        ldg4(x + (size_t)c[j] * kCols + c0, t);
+#pragma unroll
+        for (int e = 0; e < kColsPerLane; e++) xv[j][e] = (A)t[e];
+      } else {
+#pragma unroll
+        for (int e = 0; e < kColsPerLane; e++) xv[j][e] = A(0);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < kSlotBatch; j++)
+#pragma unroll
+      for (int e = 0; e < kColsPerLane; e++) acc[e] = fma(v[j], xv[j][e], acc[e]);
   }
 }
 
-// Visit every slice of M (warps striding over the grid): epi(row, acc) for
-// each of the slice's rows < n, lane = column.
+// Visit every row of M (warps striding over slices): epi(row, c0, acc) with
+// the thread's 4 columns; each thread's rows come in ascending order.
 template <class V, class X, class Epi>
 __device__ __forceinline__ void for_each_slice(const SellView<V> &m, int pack,
                                                const X *__restrict__ x, Epi &&epi) {
   using A = typename Acc<V>::type;
+  const int lane = threadIdx.x & 31;
+  const int q = lane >> 3, c0 = (lane & 7) * kColsPerLane;
   for (int s = first_slice(); s < m.nslices; s += slice_stride()) {
-    A acc[kCols];
-    slice_mm(m, pack, s, x, acc);
-#pragma unroll
-    for (int r = 0; r < kCols; r++) {
-      const int row = s * kSlice + r;
-      if (row < m.n) epi(row, acc[r]);
+    const int vb = __ldg(m.sptr + s), ve = __ldg(m.sptr + s + 1);
+    const int ib = __ldg(m.iptr + s), ie = __ldg(m.iptr + s + 1);
+    const int w = (ve - vb) / kSlice;
+    const bool om = (ie - ib) == w;
+#pragma unroll 2
+    for (int t = 0; t < kSlice / kRowsPerStep; t++) {
+      const int rs = t * kRowsPerStep + q;
+      const int row = s * kSlice + rs;
+      A acc[kColsPerLane];
+      row_mm(m, pack, vb, ib, w, om, row, rs, x, c0, acc);
+      if (row < m.n) epi(row, c0, acc);
     }
   }
 }
 
-// Per-column grid sums.  Each thread holds partials for column
-// (threadIdx.x & 31); blocks fold their warps in order, store one partial
-// per column, and the last block (atomic ticket) folds the block partials in
-// block order, warp w taking blocks w, w+8, ... and the warps then combined
-// in order.  Returns true in the last block; totals in warp 0, lane = column.
+// Last-block fold shared by the per-column sums: block partials
+// partials[(i*32 + c)*G + b], warp w taking blocks w, w+8, ... then the
+// warps combined in order; totals in warp 0, lane = column.
 template <int NV>
-__device__ __forceinline__ bool col_sum(double (&v)[NV], double *__restrict__ partials,
-                                        unsigned *ticket) {
-  __shared__ double sh[NV][kWarps][kCols];
+__device__ __forceinline__ bool fold_last(double (&tot)[NV], double *__restrict__ partials,
+                                          unsigned *ticket, double (&sh)[NV][kWarps][kCols]) {
   __shared__ bool is_last;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int G = gridDim.x;
-#pragma unroll
-  for (int i = 0; i < NV; i++) sh[i][warp][lane] = v[i];
-  __syncthreads();
-  if (warp == 0) {
-#pragma unroll
-    for (int i = 0; i < NV; i++) {
-      double s = 0.0;
-      for (int w = 0; w < kWarps; w++) s += sh[i][w][lane];
-      partials[((size_t)i * kCols + lane) * G + blockIdx.x] = s;
-    }
-    __threadfence();
-  }
   __syncthreads();
   if (threadIdx.x == 0) is_last = atomicAdd(ticket, 1u) == (unsigned)G - 1;
   __syncthreads();
@@ -144,11 +180,63 @@ __device__ __forceinline__ bool col_sum(double (&v)[NV], double *__restrict__ pa
     for (int i = 0; i < NV; i++) {
       double s = 0.0;
       for (int w = 0; w < kWarps; w++) s += sh[i][w][lane];
-      v[i] = s;
+      tot[i] = s;
     }
     if (lane == 0) *ticket = 0u;
   }
   return true;
+}
+
+// Per-column grid sums for the vector kernels: each thread holds partials
+// for column (threadIdx.x & 31).  Blocks fold their warps in order and store
+// one partial per column; the last block folds the blocks in order.
+template <int NV>
+__device__ __forceinline__ bool col_sum(double (&v)[NV], double *__restrict__ partials,
+                                        unsigned *ticket) {
+  __shared__ double sh[NV][kWarps][kCols];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int G = gridDim.x;
+#pragma unroll
+  for (int i = 0; i < NV; i++) sh[i][warp][lane] = v[i];
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int i = 0; i < NV; i++) {
+      double s = 0.0;
+      for (int w = 0; w < kWarps; w++) s += sh[i][w][lane];
+      partials[((size_t)i * kCols + lane) * G + blockIdx.x] = s;
+    }
+    __threadfence();
+  }
+  return fold_last<NV>(v, partials, ticket, sh);
+}
+
+// The same for the SpMM kernels, whose threads hold partials for their 4
+// columns: the block's 32 row-lanes per column are folded in (warp, row)
+// order.
+template <int NV>
+__device__ __forceinline__ bool col_sum4(const double (&v)[NV][kColsPerLane], double (&tot)[NV],
+                                         double *__restrict__ partials, unsigned *ticket) {
+  __shared__ double part[NV][kCols][kWarps * kRowsPerStep + 1];
+  __shared__ double sh[NV][kWarps][kCols];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int slot = warp * kRowsPerStep + (lane >> 3), c0 = (lane & 7) * kColsPerLane;
+  const int G = gridDim.x;
+#pragma unroll
+  for (int i = 0; i < NV; i++)
+#pragma unroll
+    for (int e = 0; e < kColsPerLane; e++) part[i][c0 + e][slot] = v[i][e];
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int i = 0; i < NV; i++) {
+      double s = 0.0;
+      for (int k = 0; k < kWarps * kRowsPerStep; k++) s += part[i][lane][k];
+      partials[((size_t)i * kCols + lane) * G + blockIdx.x] = s;
+    }
+    __threadfence();
+  }
+  return fold_last<NV>(tot, partials, ticket, sh);
 }
 
 __device__ __forceinline__ bool finished(const KState &c) {
@@ -169,21 +257,26 @@ __global__ void __launch_bounds__(kBlock)
               const double *__restrict__ B, double *__restrict__ R, MState *ms,
               double *partials) {
   const int lane = threadIdx.x & 31;
-  double pr[2] = {0.0, 0.0};
-  for_each_slice(a, apack, X, [&](int row, double acc) {
-    const size_t e = (size_t)row * kCols + lane;
-    const double bi = B[e];
-    const double ri = bi - acc;
-    R[e] = ri;
-    pr[0] += ri * ri;
-    pr[1] += bi * bi;
+  double pr[2][kColsPerLane] = {};
+  for_each_slice(a, apack, X, [&](int row, int c0, const double (&acc)[kColsPerLane]) {
+    const size_t e0 = (size_t)row * kCols + c0;
+    double b[kColsPerLane], r[kColsPerLane];
+    ldg4(B + e0, b);
+#pragma unroll
+    for (int e = 0; e < kColsPerLane; e++) {
+      r[e] = b[e] - acc[e];
+      pr[0][e] += r[e] * r[e];
+      pr[1][e] += b[e] * b[e];
+    }
+    st4(R + e0, r);
   });
-  if (col_sum<2>(pr, partials, &ms->ticket) && threadIdx.x < 32) {
+  double tot[2];
+  if (col_sum4<2>(pr, tot, partials, &ms->ticket) && threadIdx.x < 32) {
     if (lane < ms->m) {
       KState *st = &ms->col[lane];
-      const double bn = sqrt(pr[1]);
+      const double bn = sqrt(tot[1]);
       st->bn2 = (bn == 0.0) ? 1.0 : bn;
-      const double p3[3] = {pr[0], 0.0, 0.0};
+      const double p3[3] = {tot[0], 0.0, 0.0};
       finish_dots<kInit>(st, p3, false, nullptr);
     }
     update_alldone(ms);
@@ -196,9 +289,13 @@ __global__ void __launch_bounds__(kBlock)
     k_mv_sweep1(SellView<V> m, int pack, const double *__restrict__ R, const V *__restrict__ d,
                 T *__restrict__ Tm, const MState *ms) {
   if (ms->alldone) return;
-  const int lane = threadIdx.x & 31;
-  for_each_slice(m, pack, R, [&](int row, auto acc) {
-    Tm[(size_t)row * kCols + lane] = (T)(ldd(d + row) * acc);
+  using A = typename Acc<V>::type;
+  for_each_slice(m, pack, R, [&](int row, int c0, const A (&acc)[kColsPerLane]) {
+    const A dr = ldd(d + row);
+    T t[kColsPerLane];
+#pragma unroll
+    for (int e = 0; e < kColsPerLane; e++) t[e] = (T)(dr * acc[e]);
+    st4(Tm + (size_t)row * kCols + c0, t);
   });
 }
 
@@ -208,16 +305,23 @@ __global__ void __launch_bounds__(kBlock)
     k_mv_sweep2(SellView<V> m, int pack, const T *__restrict__ Tm, const double *__restrict__ R,
                 double *__restrict__ Zv, MState *ms, double *partials) {
   if (ms->alldone) return;
+  using A = typename Acc<V>::type;
   const int lane = threadIdx.x & 31;
-  double pr[1] = {0.0};
-  for_each_slice(m, pack, Tm, [&](int row, auto acc) {
-    const size_t e = (size_t)row * kCols + lane;
-    const double zi = (double)acc;
-    Zv[e] = zi;
-    pr[0] += R[e] * zi;
+  double pr[1][kColsPerLane] = {};
+  for_each_slice(m, pack, Tm, [&](int row, int c0, const A (&acc)[kColsPerLane]) {
+    const size_t e0 = (size_t)row * kCols + c0;
+    double r[kColsPerLane], z[kColsPerLane];
+    ldg4(R + e0, r);
+#pragma unroll
+    for (int e = 0; e < kColsPerLane; e++) {
+      z[e] = (double)acc[e];
+      pr[0][e] += r[e] * z[e];
+    }
+    st4(Zv + e0, z);
   });
-  if (col_sum<1>(pr, partials, &ms->ticket) && threadIdx.x < 32) {
-    if (lane < ms->m && !ms->col[lane].done) cg_take_rho(&ms->col[lane], pr[0]);
+  double tot[1];
+  if (col_sum4<1>(pr, tot, partials, &ms->ticket) && threadIdx.x < 32) {
+    if (lane < ms->m && !ms->col[lane].done) cg_take_rho(&ms->col[lane], tot[0]);
     update_alldone(ms);
   }
 }
@@ -261,15 +365,19 @@ __global__ void __launch_bounds__(kBlock)
                     double *__restrict__ Q, MState *ms, double *partials) {
   if (ms->alldone) return;
   const int lane = threadIdx.x & 31;
-  double pr[1] = {0.0};
-  for_each_slice(a, apack, P, [&](int row, double acc) {
-    const size_t e = (size_t)row * kCols + lane;
-    Q[e] = acc;
-    pr[0] += P[e] * acc;
+  double pr[1][kColsPerLane] = {};
+  for_each_slice(a, apack, P, [&](int row, int c0, const double (&acc)[kColsPerLane]) {
+    const size_t e0 = (size_t)row * kCols + c0;
+    double p[kColsPerLane];
+    ldg4(P + e0, p);
+#pragma unroll
+    for (int e = 0; e < kColsPerLane; e++) pr[0][e] += p[e] * acc[e];
+    st4(Q + e0, acc);
   });
-  if (col_sum<1>(pr, partials, &ms->ticket) && threadIdx.x < 32) {
+  double tot[1];
+  if (col_sum4<1>(pr, tot, partials, &ms->ticket) && threadIdx.x < 32) {
     if (lane < ms->m && !ms->col[lane].done) {
-      const double p3[3] = {pr[0], 0.0, 0.0};
+      const double p3[3] = {tot[0], 0.0, 0.0};
       finish_dots<kCgSigma>(&ms->col[lane], p3, false, nullptr);
     }
     update_alldone(ms);
@@ -321,17 +429,24 @@ __global__ void __launch_bounds__(kBlock)
   const bool mine = lane < ms->m && (col_verify(c) || col_periodic(c));
   const bool verify = lane < ms->m && col_verify(c);
   if (!__syncthreads_or(mine)) return;  // no column needs a check
-  double pr[3] = {0.0, 0.0, 0.0};
-  for_each_slice(a, apack, X, [&](int row, double acc) {
-    const size_t e = (size_t)row * kCols + lane;
-    const double ri = B[e] - acc;
-    Rt[e] = ri;
-    pr[0] += ri * ri;
-    const double g = ri - R[e];
-    pr[1] += g * g;
+  double pr[3][kColsPerLane] = {};
+  for_each_slice(a, apack, X, [&](int row, int c0, const double (&acc)[kColsPerLane]) {
+    const size_t e0 = (size_t)row * kCols + c0;
+    double b[kColsPerLane], r[kColsPerLane], rt[kColsPerLane];
+    ldg4(B + e0, b);
+    ldg4(R + e0, r);
+#pragma unroll
+    for (int e = 0; e < kColsPerLane; e++) {
+      rt[e] = b[e] - acc[e];
+      pr[0][e] += rt[e] * rt[e];
+      const double g = rt[e] - r[e];
+      pr[1][e] += g * g;
+    }
+    st4(Rt + e0, rt);
   });
-  if (col_sum<3>(pr, partials, &ms->ticket) && threadIdx.x < 32) {
-    if (mine) finish_dots<kTrueRes>(&ms->col[lane], pr, verify, nullptr);
+  double tot[3];
+  if (col_sum4<3>(pr, tot, partials, &ms->ticket) && threadIdx.x < 32) {
+    if (mine) finish_dots<kTrueRes>(&ms->col[lane], tot, verify, nullptr);
     update_alldone(ms);
   }
 }
@@ -418,7 +533,7 @@ int get_ws(ainv_csr *a, MrhsWs **out) {
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   w->n = a->n;
   w->stride = (size_t)a->n * kCols;
-  w->G = std::max(1, std::min(grid_for(a->a.nslices), 4 * sms));
+  w->G = 8 * sms;  // partials capacity: the largest resident wave (8 blocks per SM)
   cudaError_t e = cudaMalloc(&w->mv, sizeof(double) * kNumMv * w->stride);
   if (e == cudaSuccess) e = cudaMalloc(&w->t, sizeof(double) * w->stride);
   if (e == cudaSuccess) e = cudaMalloc(&w->partials, sizeof(double) * 3 * kCols * (size_t)w->G);
@@ -440,17 +555,20 @@ int get_ws(ainv_csr *a, MrhsWs **out) {
 template <class V, class T>
 void launch_precond(const MrhsWs *w, const ainv_handle *h, cudaStream_t s) {
   const SellView<V> wt = view<V>(h->wt), z = view<V>(h->z);
-  k_mv_sweep1<V, T><<<w->G, kBlock, 0, s>>>(wt, h->wt.pack, w->v(MR), (const V *)h->d, (T *)w->t,
-                                           w->st);
-  k_mv_sweep2<V, T><<<w->G, kBlock, 0, s>>>(z, h->z.pack, (const T *)w->t, w->v(MR), w->v(MZ),
-                                           w->st, w->partials);
+  const int g1 = wave_grid((const void *)k_mv_sweep1<V, T>, w->n);
+  const int g2 = wave_grid((const void *)k_mv_sweep2<V, T>, w->n);
+  k_mv_sweep1<V, T><<<g1, kBlock, 0, s>>>(wt, h->wt.pack, w->v(MR), (const V *)h->d, (T *)w->t,
+                                         w->st);
+  k_mv_sweep2<V, T><<<g2, kBlock, 0, s>>>(z, h->z.pack, (const T *)w->t, w->v(MR), w->v(MZ),
+                                         w->st, w->partials);
 }
 
 int enqueue_iteration(const MrhsWs *w, const ainv_handle *h, const ainv_csr *a) {
   const cudaStream_t s = w->s;
   const long long ne = (long long)w->stride;
-  const int Gv = (int)std::min<long long>((ne + kBlock - 1) / kBlock, (long long)w->G);
   const SellView<double> A = view<double>(a->a);
+  auto gv = [&](const void *k) { return wave_grid(k, ne); };
+  auto gm = [&](const void *k) { return wave_grid(k, w->n); };
   if (h) {
     switch (h->prec) {
       case AINV_PREC_FP64: launch_precond<double, double>(w, h, s); break;
@@ -458,14 +576,17 @@ int enqueue_iteration(const MrhsWs *w, const ainv_handle *h, const ainv_csr *a) 
       default: launch_precond<__nv_bfloat16, float>(w, h, s); break;
     }
   } else {
-    k_mv_ident<<<Gv, kBlock, 0, s>>>(ne, w->v(MR), w->v(MZ), w->st, w->partials);
+    k_mv_ident<<<gv((const void *)k_mv_ident), kBlock, 0, s>>>(ne, w->v(MR), w->v(MZ), w->st,
+                                                               w->partials);
   }
-  k_mv_p<<<Gv, kBlock, 0, s>>>(ne, w->v(MZ), w->v(MP), w->st);
-  k_mv_spmm_sigma<<<w->G, kBlock, 0, s>>>(A, a->a.pack, w->v(MP), w->v(MQ), w->st, w->partials);
-  k_mv_xr<<<Gv, kBlock, 0, s>>>(ne, w->v(MP), w->v(MQ), w->v(MX), w->v(MR), w->st, w->partials);
-  k_mv_trueres<<<w->G, kBlock, 0, s>>>(A, a->a.pack, w->v(MX), w->v(MB), w->v(MR), w->v(MRT),
-                                       w->st, w->partials);
-  k_mv_replace<<<Gv, kBlock, 0, s>>>(ne, w->v(MRT), w->v(MR), w->st);
+  k_mv_p<<<gv((const void *)k_mv_p), kBlock, 0, s>>>(ne, w->v(MZ), w->v(MP), w->st);
+  k_mv_spmm_sigma<<<gm((const void *)k_mv_spmm_sigma), kBlock, 0, s>>>(
+      A, a->a.pack, w->v(MP), w->v(MQ), w->st, w->partials);
+  k_mv_xr<<<gv((const void *)k_mv_xr), kBlock, 0, s>>>(ne, w->v(MP), w->v(MQ), w->v(MX), w->v(MR),
+                                                       w->st, w->partials);
+  k_mv_trueres<<<gm((const void *)k_mv_trueres), kBlock, 0, s>>>(
+      A, a->a.pack, w->v(MX), w->v(MB), w->v(MR), w->v(MRT), w->st, w->partials);
+  k_mv_replace<<<gv((const void *)k_mv_replace), kBlock, 0, s>>>(ne, w->v(MRT), w->v(MR), w->st);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     set_error("block solve launch failed: %s", cudaGetErrorString(e));
@@ -528,7 +649,7 @@ extern "C" int ainv_gpu_block_solve(ainv_handle *h, const ainv_csr *ac, int m, c
   AINV_TRY(get_ws(a, &w));
   const cudaStream_t user = (cudaStream_t)stream;
   const int n = a->n;
-  const int Gc = std::max(1, std::min(w->G, (int)(((long long)n * kCols + kBlock - 1) / kBlock)));
+  const int Gc = wave_grid((const void *)k_mv_gather, (long long)n * kCols);
   AINV_CUDA_TRY(cudaEventRecord(w->ev, user));
   AINV_CUDA_TRY(cudaStreamWaitEvent(w->s, w->ev, 0));
   k_mv_gather<<<Gc, kBlock, 0, w->s>>>(n, m, ldb, B, w->v(MB));
@@ -548,8 +669,8 @@ extern "C" int ainv_gpu_block_solve(ainv_handle *h, const ainv_csr *ac, int m, c
   }
   *w->hst = init;
   AINV_CUDA_TRY(cudaMemcpyAsync(w->st, w->hst, sizeof(MState), cudaMemcpyHostToDevice, w->s));
-  k_mv_init<<<w->G, kBlock, 0, w->s>>>(view<double>(a->a), a->a.pack, w->v(MX), w->v(MB),
-                                       w->v(MR), w->st, w->partials);
+  k_mv_init<<<wave_grid((const void *)k_mv_init, n), kBlock, 0, w->s>>>(
+      view<double>(a->a), a->a.pack, w->v(MX), w->v(MB), w->v(MR), w->st, w->partials);
   AINV_CUDA_TRY(cudaGetLastError());
   const bool use_graph = getenv("AINV_NO_GRAPH") == nullptr;
   const long max_chunks = (long)itmax / kChunk + 2 + 4 * kMaxVerifyFails;

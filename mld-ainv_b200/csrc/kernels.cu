@@ -187,6 +187,33 @@ int stream_plan(const DevSell &m, int xs, int nrv, StreamLayout &L, size_t &smem
   return std::min(m.nstages, per_sm * sm_count());
 }
 
+int wave_grid(const void *kernel, long long rows) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void *>, int> cache;
+  int d = 0;
+  if (cudaGetDevice(&d) != cudaSuccess) d = 0;
+  int wave;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find({d, kernel});
+    if (it != cache.end()) {
+      wave = it->second;
+    } else {
+      int per_sm = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBlock, 0) !=
+              cudaSuccess ||
+          per_sm <= 0) {
+        cudaGetLastError();
+        per_sm = 1;
+      }
+      wave = per_sm * sm_count();
+      cache[{d, kernel}] = wave;
+    }
+  }
+  const long long units = (rows + kBlock - 1) / kBlock;
+  return (int)std::max(1LL, std::min(units, (long long)wave));
+}
+
 int reduction_grid(long long rows) {
   static int sms[64] = {};
   int d = 0;

@@ -15,6 +15,7 @@
 // and t.s) share one kernel; the Z sweep of the preconditioner and the CG
 // dot r.z share one kernel; x/r updates and the residual norm (plus rt.r
 // for BiCGSTAB) share one kernel.
+#include <algorithm>
 #include <atomic>
 #include <cstdint>
 #include <cmath>
@@ -327,7 +328,9 @@ struct CgSweep2Launch {
   cudaStream_t s;
   template <int S, int P>
   void run() const {
-    k_cg_sweep2<V, T, S, P><<<G, kBlock, 0, s>>>(view<V>(m), (const T *)t, r, z, st, partials);
+    auto kern = k_cg_sweep2<V, T, S, P>;
+    kern<<<std::min(G, wave_grid((const void *)kern, m.n)), kBlock, 0, s>>>(
+        view<V>(m), (const T *)t, r, z, st, partials);
   }
 };
 
@@ -387,7 +390,9 @@ struct SpmvDotsLaunch {
   double *pp;
   template <int S, int P>
   void run() const {
-    k_spmv_dots<MODE, S, P><<<G, kBlock, 0, s>>>(A, x, y, w1, w2, w3, st, pp);
+    auto kern = k_spmv_dots<MODE, S, P>;
+    kern<<<std::min(G, wave_grid((const void *)kern, A.n)), kBlock, 0, s>>>(A, x, y, w1, w2, w3,
+                                                                          st, pp);
   }
 };
 
@@ -532,11 +537,13 @@ int enqueue_iteration(KrylovWs *w, const ainv_handle *h, const ainv_csr *a, int 
       AINV_TRY(launch_sweep_dscale(h->wt, h->d, r, h->t, s, stop, &st->timeout));
       precond_sweep2_cg(h, r, z, st, pp, G, s);
     } else {
-      k_cg_ident<<<G, kBlock, 0, s>>>(n, r, z, st, pp);
+      k_cg_ident<<<std::min(G, wave_grid((const void *)k_cg_ident, n)), kBlock, 0, s>>>(n, r, z,
+                                                                                         st, pp);
     }
     k_cg_p<<<Gv, kBlock, 0, s>>>(n, z, p, st);
     spmv_dots<kCgSigma>(A, G, s, p, q, nullptr, nullptr, nullptr, st, pp);
-    k_cg_xr<<<G, kBlock, 0, s>>>(n, p, q, x, r, st, pp);
+    k_cg_xr<<<std::min(G, wave_grid((const void *)k_cg_xr, n)), kBlock, 0, s>>>(n, p, q, x, r,
+                                                                                 st, pp);
     spmv_dots<kTrueRes>(A, G, s, x, w->v(RTRUE), w->v(BW), nullptr, r, st, pp);
     k_replace_r<<<Gv, kBlock, 0, s>>>(n, w->v(RTRUE), r, st);
   } else {
@@ -556,7 +563,8 @@ int enqueue_iteration(KrylovWs *w, const ainv_handle *h, const ainv_csr *a, int 
       AINV_CUDA_TRY(cudaMemcpyAsync(z, sv, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     }
     spmv_dots<kBicgOmega>(A, G, s, z, t, sv, nullptr, nullptr, st, pp);
-    k_bicg_xr<<<G, kBlock, 0, s>>>(n, f, z, sv, t, rt, x, r, st, pp);
+    k_bicg_xr<<<std::min(G, wave_grid((const void *)k_bicg_xr, n)), kBlock, 0, s>>>(
+        n, f, z, sv, t, rt, x, r, st, pp);
     spmv_dots<kTrueRes>(A, G, s, x, w->v(RTRUE), w->v(BW), rt, r, st, pp);
     k_replace_r<<<Gv, kBlock, 0, s>>>(n, w->v(RTRUE), r, st);
   }
@@ -626,7 +634,8 @@ int krylov_solve(const ainv_handle *h, ainv_csr *a, const double *b, double *x, 
   *w->hst = init;
   AINV_CUDA_TRY(cudaMemcpyAsync(w->st, w->hst, sizeof(KState), cudaMemcpyHostToDevice, w->s));
   const DevSell &A = a->a;
-  k_bnorm<<<w->G, kBlock, 0, w->s>>>(n, w->v(BW), w->st, w->partials);
+  k_bnorm<<<std::min(w->G, wave_grid((const void *)k_bnorm, n)), kBlock, 0, w->s>>>(
+      n, w->v(BW), w->st, w->partials);
   spmv_dots<kInit>(A, w->G, w->s, w->v(XW), w->v(R), w->v(BW),
       method == AINV_KRYLOV_BICGSTAB ? w->v(RT) : nullptr, nullptr, w->st, w->partials);
   AINV_CUDA_TRY(cudaGetLastError());

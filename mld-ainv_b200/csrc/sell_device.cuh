@@ -359,6 +359,10 @@ inline int grid_for_groups(int nslices, int S) {
 // wave (8 blocks of 256 threads per SM) so the last block folds few
 // partials; never more blocks than units of 256 rows.
 int reduction_grid(long long rows);
+// Blocks of one full resident wave of `kernel` (256 threads, occupancy from
+// its registers and shared memory), at most one per 256 rows: the grid of a
+// grid-stride kernel, so no partial second wave runs alone.
+int wave_grid(const void *kernel, long long rows);
 
 // ---- deterministic block reduction --------------------------------------
 // Fixed shuffle tree inside each warp, then thread 0 folds the per-warp

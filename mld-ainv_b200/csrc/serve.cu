@@ -748,7 +748,17 @@ int ainv_server_create(ainv_server **out, int max_slots, size_t hbm_bytes, int i
   if (e == cudaSuccess)
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, srv->device);
   if (e != cudaSuccess) return fail(e, "device query");
-  srv->grid = std::min(kMaxGrid, std::max(max_slots, 8 * sms));
+  // one resident wave of the heaviest batched kernel, so every kernel of the
+  // graph runs its blocks in a single wave
+  const long long big = 1LL << 40;
+  int wave = wave_grid((const void *)k_srv_init, big);
+  for (const void *k : {(const void *)k_srv_p, (const void *)k_srv_s, (const void *)k_srv_sweep1,
+                        (const void *)k_srv_sweep2, (const void *)k_srv_spmv<kBicgSigma>,
+                        (const void *)k_srv_spmv<kBicgOmega>, (const void *)k_srv_spmv<kTrueRes>,
+                        (const void *)k_srv_xr, (const void *)k_srv_replace})
+    wave = std::min(wave, wave_grid(k, big));
+  (void)sms;
+  srv->grid = std::min(kMaxGrid, std::max(max_slots, wave));
   // admission budget: the caller's bytes, or half of the free HBM
   size_t fr = 0, tot = 0;
   e = cudaMemGetInfo(&fr, &tot);
