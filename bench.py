@@ -219,6 +219,12 @@ def main():
                     help="mean arrival rates (requests/s) of the serving sweep")
     ap.add_argument("--serve-slots", type=int, default=32)
     ap.add_argument("--serve-iters", type=int, default=4)
+    ap.add_argument("--leg", default="all", choices=["all", "block", "solve", "serve"],
+                    help="run one leg alone (profiler captures of its kernels)")
+    ap.add_argument("--leg-itmax", type=int, default=2000,
+                    help="iteration cap of the solve / block legs run alone")
+    ap.add_argument("--leg-idim", type=int, default=0,
+                    help="grid side of the solve / block legs run alone (0: their default)")
     ap.add_argument("--idim", type=int, default=IDIM,
                     help="grid side (default 200; smaller sizes for profiler captures)")
     args = ap.parse_args()
@@ -249,6 +255,9 @@ def main():
         t = torch.tensor([v], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
+
+    if args.leg != "all":
+        return run_leg(ainv, torch, args)
 
     (irp, ja, val), sv = build_workload(args.idim)
     n = len(irp) - 1
@@ -508,7 +517,7 @@ def run_variants(ainv, torch, dev, irp, ja, val, A, b, bn, xs, x, y, flush, stre
     return out
 
 
-def run_block_cg(ainv, torch, dev, idim=128, m=32):
+def run_block_cg(ainv, torch, dev, idim=128, m=32, itmax=2000, reps=3, single=True):
     """Multi-right-hand-side CG: 3-D Poisson on a 128^3 grid, 32 right-hand
     sides N(0,1) (seed k for column k), AINV drop 0.1 fill 20 with FP32
     factors, FP64 A, CG to 1e-9 per column.  One block solve (SpMM products)
@@ -524,13 +533,13 @@ def run_block_cg(ainv, torch, dev, idim=128, m=32):
     Bh = np.stack([ainv.pde.rand_normal(k, n) for k in range(m)], axis=1)
     B = torch.from_numpy(Bh).to(dev)
     X = torch.zeros_like(B)
-    A.block_solve(B, X, sv.device, 1e-9, 2000)  # warm-up (workspace, graph)
+    A.block_solve(B, X, sv.device, 1e-9, itmax)  # warm-up (workspace, graph)
     times = []
-    for _ in range(3):
+    for _ in range(reps):
         X.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        res = A.block_solve(B, X, sv.device, 1e-9, 2000)
+        res = A.block_solve(B, X, sv.device, 1e-9, itmax)
         torch.cuda.synchronize()
         times.append(time.perf_counter() - t0)
     R = B.clone()
@@ -541,7 +550,7 @@ def run_block_cg(ainv, torch, dev, idim=128, m=32):
     rel = (torch.linalg.vector_norm(R, dim=0) / torch.linalg.vector_norm(B, dim=0)).max()
     # the same systems one at a time through the single-vector loop
     t_single, it_single = 0.0, []
-    for l in range(m):
+    for l in range(m if single else 0):
         b = B[:, l].contiguous()
         x = torch.zeros(n, dtype=torch.float64, device=dev)
         if l == 0:
@@ -558,13 +567,45 @@ def run_block_cg(ainv, torch, dev, idim=128, m=32):
            "rhs": m, "converged": bool(res.converged), "max_true_relres": float(rel),
            "iters_mean": round(float(np.mean(res.iters)), 2), "iters_max": int(max(res.iters)),
            "s_per_block_solve": round(tb, 4), "rhs_solves_per_s": round(m / tb, 2),
-           "single_rhs_s_total": round(t_single, 4),
-           "single_rhs_solves_per_s": round(m / t_single, 2),
-           "single_iters_mean": round(float(np.mean(it_single)), 2),
-           "speedup_vs_single": round(t_single / tb, 3)}
+           "single_rhs_s_total": round(t_single, 4) if single else None,
+           "single_rhs_solves_per_s": round(m / t_single, 2) if single else None,
+           "single_iters_mean": round(float(np.mean(it_single)), 2) if single else None,
+           "speedup_vs_single": round(t_single / tb, 3) if single else None}
     A.close()
     sv.free()
     return out
+
+
+def run_leg(ainv, torch, args):
+    """One leg alone, e.g. under a profiler: `block` (multi-RHS CG),
+    `solve` (one FP32-factor BiCGSTAB solve of the convection-diffusion
+    workload) or `serve` (the serving stream)."""
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    if args.leg == "block":
+        out = run_block_cg(ainv, torch, dev, idim=args.leg_idim or 128, itmax=args.leg_itmax,
+                           reps=1, single=False)
+    elif args.leg == "serve":
+        out = run_serving(ainv, torch, args)
+    else:
+        (irp, ja, val), sv = build_workload(args.leg_idim or IDIM)
+        n = len(irp) - 1
+        assert sv.cnv("FP32") == 0, ainv.last_error()
+        A = ainv.DeviceOperator(irp, ja, val)
+        xs = torch.from_numpy(ainv.pde.rand_uniform(0, n)).to(dev)
+        b = torch.zeros(n, dtype=torch.float64, device=dev)
+        A.spmv(xs, b, 1.0, 0.0)
+        x = torch.zeros_like(b)
+        A.solve(b, x, sv.device, "BICGSTAB", 1e-9, args.leg_itmax)
+        x.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = A.solve(b, x, sv.device, "BICGSTAB", 1e-9, args.leg_itmax)
+        torch.cuda.synchronize()
+        out = {"n": n, "iters": res.iter, "info": res.info, "relres": res.err,
+               "s": round(time.perf_counter() - t0, 5)}
+        A.close()
+    print(json.dumps({"leg": args.leg, **out}), flush=True)
+    return 0
 
 
 def run_serving(ainv, torch, args):

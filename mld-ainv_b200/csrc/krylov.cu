@@ -105,8 +105,7 @@ __global__ void __launch_bounds__(kBlock)
     k_replace_r(int n, const double *__restrict__ rtrue, double *__restrict__ r,
                 const KState *st) {
   if (!st->replace) return;
-  const int i = blockIdx.x * kBlock + threadIdx.x;
-  if (i < n) r[i] = rtrue[i];
+  for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) r[i] = rtrue[i];
 }
 
 // ---- streaming variants (stream.cuh) ----------------------------------------
@@ -545,7 +544,8 @@ int enqueue_iteration(KrylovWs *w, const ainv_handle *h, const ainv_csr *a, int 
     k_cg_xr<<<std::min(G, wave_grid((const void *)k_cg_xr, n)), kBlock, 0, s>>>(n, p, q, x, r,
                                                                                  st, pp);
     spmv_dots<kTrueRes>(A, G, s, x, w->v(RTRUE), w->v(BW), nullptr, r, st, pp);
-    k_replace_r<<<Gv, kBlock, 0, s>>>(n, w->v(RTRUE), r, st);
+    k_replace_r<<<wave_grid((const void *)k_replace_r, n), kBlock, 0, s>>>(n, w->v(RTRUE), r,
+                                                                         st);
   } else {
     double *r = w->v(R), *rt = w->v(RT), *p = w->v(P), *v = w->v(V), *f = w->v(F),
            *sv = w->v(S), *z = w->v(Z), *t = w->v(T), *x = w->v(XW);
@@ -566,7 +566,8 @@ int enqueue_iteration(KrylovWs *w, const ainv_handle *h, const ainv_csr *a, int 
     k_bicg_xr<<<std::min(G, wave_grid((const void *)k_bicg_xr, n)), kBlock, 0, s>>>(
         n, f, z, sv, t, rt, x, r, st, pp);
     spmv_dots<kTrueRes>(A, G, s, x, w->v(RTRUE), w->v(BW), rt, r, st, pp);
-    k_replace_r<<<Gv, kBlock, 0, s>>>(n, w->v(RTRUE), r, st);
+    k_replace_r<<<wave_grid((const void *)k_replace_r, n), kBlock, 0, s>>>(n, w->v(RTRUE), r,
+                                                                         st);
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
