@@ -163,6 +163,14 @@ int ainv_gpu_solve(ainv_handle *h, const ainv_csr *a, const double *b_dev,
  * recurrence residual was replaced by b - A x. */
 int ainv_csr_solve_info(const ainv_csr *a, int *verify_fails, int *replacements);
 
+/* update_a (src/impl/mld_d_base_ainv_update_a.f90:53-79): reuse the factors
+ * for the shifted system A + diag(x) by refreshing the diagonal,
+ *   d <- 1 / (1/d + diag(W^T diag(x) Z)),
+ * on the device.  x_dev: n doubles on the device.  d_dev_out (may be NULL):
+ * n doubles on the device receiving the new d in FP64 (the handle keeps it
+ * in its own precision).  Asynchronous on `stream`. */
+int ainv_gpu_update_a(ainv_handle *h, const double *x_dev, double *d_dev_out, void *stream);
+
 /* Preconditioned CG on m (1..32) right-hand sides at once: column l solves
  * A x_l = b_l with its own CG recurrence (psb_dcg, istop=2, as
  * ainv_gpu_solve) while every product with A and with the factors is one
@@ -219,6 +227,20 @@ long long mld_d_solver_get_nzeros(const mld_d_solver *sv);
 int mld_d_solver_get_wrksz(void);              /* 2, like get_wrksz */
 /* Human-readable description into buf (always NUL-terminated). */
 int mld_d_solver_descr(const mld_d_solver *sv, char *buf, size_t len);
+/* Load factors from the MatrixMarket files of a dump: <prefix>_wmat.mtx
+ * (W^T), <prefix>_diag.mtx (d) and <prefix>_zmat.mtx (Z), as this library's
+ * dump and the reference's (src/impl/mld_d_base_ainv_solver_dmp.f90:82-108,
+ * full prefix such as "dump_ainv_d_p000_l001") write them.  The solver is
+ * then built (and uploaded if cnv was called), whatever its type. */
+int mld_d_solver_load(mld_d_solver *sv, const char *prefix);
+/* Binary factor cache (host factors + settings, checksummed): save writes
+ * it, restore reads it into a solver of the same type.  No counterpart in
+ * the reference; it skips the host build when factors are reused. */
+int mld_d_solver_save(const mld_d_solver *sv, const char *path);
+int mld_d_solver_restore(mld_d_solver *sv, const char *path);
+/* update(x) of the plugin type: the device update_a on the uploaded factors
+ * (x: n host doubles), the new d copied back to the host factors. */
+int mld_d_solver_update_a(mld_d_solver *sv, const double *x);
 /* MatrixMarket dump of W^T, D^-1 and Z as <prefix>_wmat.mtx,
  * <prefix>_diag.mtx, <prefix>_zmat.mtx. */
 int mld_d_solver_dump(const mld_d_solver *sv, const char *prefix);

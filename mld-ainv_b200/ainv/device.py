@@ -72,6 +72,13 @@ class DeviceFactors:
                                          dptr(x) if x is not None else None, beta,
                                          dptr(y) if y is not None else None, _stream(stream)))
 
+    def update_a(self, x, d_out=None, stream=None) -> None:
+        """update_a on the device: d <- 1/(1/d + diag(W^T diag(x) Z)); x a
+        CUDA float64 tensor of n entries, d_out (optional) receives the new d
+        in FP64."""
+        check(lib().ainv_gpu_update_a(self._h, dptr(x), dptr(d_out) if d_out is not None else None,
+                                      _stream(stream)))
+
     def apply_host(self, x, alpha=1.0, beta=0.0, y=None, trans="N") -> np.ndarray:
         x = _np(x, np.float64)
         y = np.zeros_like(x) if y is None else _np(y, np.float64).copy()

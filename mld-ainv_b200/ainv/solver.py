@@ -73,6 +73,24 @@ class _SolverType:
         return lib().mld_d_solver_cnv(self._h, PREC[prec.upper()])
 
     # -- apply --------------------------------------------------------------
+    def load(self, prefix: str) -> int:
+        """Factors from <prefix>_{wmat,diag,zmat}.mtx (a dump of this library
+        or of the reference)."""
+        return lib().mld_d_solver_load(self._h, prefix.encode())
+
+    def save(self, path: str) -> int:
+        """Binary factor cache (host factors and settings)."""
+        return lib().mld_d_solver_save(self._h, path.encode())
+
+    def restore(self, path: str) -> int:
+        return lib().mld_d_solver_restore(self._h, path.encode())
+
+    def update_a(self, x) -> int:
+        """update(x) of the plugin type (shifted system A + diag(x)) on the
+        uploaded factors; the host d follows."""
+        x = np.ascontiguousarray(x, np.float64)
+        return lib().mld_d_solver_update_a(self._h, C.c_void_p(x.ctypes.data))
+
     def apply(self, alpha, x, beta, y, trans: str = "N", stream=None) -> int:
         """apply_v: y = alpha * M x + beta * y on device tensors."""
         return lib().mld_d_solver_apply(self._h, float(alpha), dptr(x), float(beta), dptr(y),

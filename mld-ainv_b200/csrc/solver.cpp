@@ -13,11 +13,15 @@
 #include <new>
 #include <string>
 
-#include "host_build.h"
+#include <cuda_runtime.h>
+
+#include "solver_impl.h"
 
 namespace {
 
-enum Kind { kAinv = 0, kInvk = 1, kInvt = 2 };
+using ainv::kAinv;
+using ainv::kInvk;
+using ainv::kInvt;
 
 std::string upper(const char *s) {
   std::string u = s ? s : "";
@@ -31,20 +35,6 @@ std::string upper(const char *s) {
 
 }  // namespace
 
-struct mld_d_solver {
-  int kind = kAinv;
-  // AINV: alg, fill_in, thresh.  INVK: fill_in, inv_fill.  INVT: all four.
-  int alg = ainv::kAlgLLK;
-  int fill_in = 0;
-  double thresh = 0.0;
-  int inv_fill = 0;
-  double inv_thresh = 0.0;
-  bool built = false;
-  ainv::HostCsr wt, z;  // wt holds W^T (sv%w), z holds Z (sv%z)
-  std::vector<double> d;
-  int dev_prec = -1;  // device storage requested by cnv (-1: none yet)
-  ainv_handle *h = nullptr;
-};
 
 namespace {
 
@@ -69,6 +59,20 @@ int upload(mld_d_solver *sv) {
                          z.irp.data(), z.ja.data(), z.val.data(), sv->d.data(),
                          sv->dev_prec, 0);
 }
+
+}  // namespace
+
+int ainv::install_factors(mld_d_solver *sv, HostCsr wt, HostCsr z, std::vector<double> d) {
+  clear_data(sv);
+  sv->wt = std::move(wt);
+  sv->z = std::move(z);
+  sv->d = std::move(d);
+  sv->built = true;
+  if (sv->dev_prec >= 0) return upload(sv);
+  return AINV_SUCCESS;
+}
+
+namespace {
 
 // d_ainv_stringval (src/mld_d_ainv_solver.F90:232-258); unknown names map
 // to an invalid algorithm, which build rejects as "Invalid alg".
@@ -241,6 +245,21 @@ int mld_d_solver_build(mld_d_solver *sv, int n, const int *irp, const int *ja,
   return AINV_SUCCESS;
 }
 
+int mld_d_solver_load(mld_d_solver *sv, const char *prefix) {
+  if (!sv || !prefix) return AINV_ERR_ARG;
+  return ainv::load_matrix_market(sv, prefix);
+}
+
+int mld_d_solver_save(const mld_d_solver *sv, const char *path) {
+  if (!sv || !path) return AINV_ERR_ARG;
+  return ainv::save_cache(sv, path);
+}
+
+int mld_d_solver_restore(mld_d_solver *sv, const char *path) {
+  if (!sv || !path) return AINV_ERR_ARG;
+  return ainv::load_cache(sv, path);
+}
+
 int mld_d_solver_cnv(mld_d_solver *sv, int prec) {
   if (!sv) return AINV_ERR_ARG;
   if (ainv::prec_size(prec) == 0) {
@@ -270,6 +289,32 @@ int mld_d_solver_apply_host(mld_d_solver *sv, double alpha, const double *x, dou
     return AINV_ERR_NOT_BUILT;
   }
   return ainv_gpu_apply_host(sv->h, trans, alpha, x, beta, y);
+}
+
+int mld_d_solver_update_a(mld_d_solver *sv, const double *x) {
+  if (!sv || !x) return AINV_ERR_ARG;
+  if (!sv->h) {
+    ainv::set_error("update_a: factors are not on the device (build, then cnv)");
+    return AINV_ERR_NOT_BUILT;
+  }
+  // src/impl/mld_d_base_ainv_update_a.f90:53-79 on the device; sv%d and the
+  // device copy are both replaced
+  const size_t bytes = sizeof(double) * sv->d.size();
+  double *xd = nullptr, *dd = nullptr;
+  cudaError_t e = cudaMalloc(&xd, bytes);
+  if (e == cudaSuccess) e = cudaMalloc(&dd, bytes);
+  if (e == cudaSuccess) e = cudaMemcpy(xd, x, bytes, cudaMemcpyHostToDevice);
+  int rc = AINV_SUCCESS;
+  if (e == cudaSuccess) rc = ainv_gpu_update_a(sv->h, xd, dd, nullptr);
+  if (e == cudaSuccess && rc == AINV_SUCCESS)
+    e = cudaMemcpy(sv->d.data(), dd, bytes, cudaMemcpyDeviceToHost);
+  if (xd) cudaFree(xd);
+  if (dd) cudaFree(dd);
+  if (e != cudaSuccess) {
+    ainv::set_error("update_a: %s", cudaGetErrorString(e));
+    return AINV_ERR_CUDA;
+  }
+  return rc;
 }
 
 ainv_handle *mld_d_solver_handle(mld_d_solver *sv) { return sv ? sv->h : nullptr; }

@@ -1049,3 +1049,38 @@ int orc_invt_build(int n, const int *irp, const int *ja, const double *val,
 }
 
 void orc_free(void *p) { free(p); }
+
+/* mld_d_base_ainv_update_a (src/impl/mld_d_base_ainv_update_a.f90:53-79):
+ * ee = x; Z (as CSC) scaled on the left by ee; ee(i) = spdot_srtd(row i of
+ * W^T, column i of the scaled Z); d = 1/(1/d + ee). */
+int orc_update_a(int n, const int *wt_irp, const int *wt_ja, const double *wt_val,
+                 const int *z_irp, const int *z_ja, const double *z_val,
+                 const double *d, const double *x, double *d_out) {
+  if (n <= 0) return -1;
+  long nz = z_irp[n];
+  int *cp = (int *)malloc(sizeof(int) * (size_t)(n + 1));
+  int *ri = (int *)malloc(sizeof(int) * (size_t)(nz > 0 ? nz : 1));
+  double *cv = (double *)malloc(sizeof(double) * (size_t)(nz > 0 ? nz : 1));
+  csr_transpose(n, z_irp, z_ja, z_val, cp, ri, cv); /* CSC of Z */
+  for (long k = 0; k < nz; k++) cv[k] = x[ri[k]] * cv[k]; /* scal, side='L' */
+  for (int i = 0; i < n; i++) {
+    double dot = 0.0;
+    int p1 = wt_irp[i], e1 = wt_irp[i + 1], p2 = cp[i], e2 = cp[i + 1];
+    while (p1 < e1 && p2 < e2) {
+      if (wt_ja[p1] == ri[p2]) {
+        dot = dot + wt_val[p1] * cv[p2];
+        p1++;
+        p2++;
+      } else if (wt_ja[p1] < ri[p2]) {
+        p1++;
+      } else {
+        p2++;
+      }
+    }
+    double dd = 1.0 / d[i];
+    dd = dd + dot;
+    d_out[i] = 1.0 / dd;
+  }
+  free(cp); free(ri); free(cv);
+  return 0;
+}

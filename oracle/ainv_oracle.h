@@ -72,6 +72,12 @@ int orc_invt_build(int n, const int *irp, const int *ja, const double *val,
                    int **z_irp, int **z_ja, double **z_val, long *nnz_z, double *d);
 void orc_free(void *p);
 
+/* mld_d_base_ainv_update_a (src/impl/mld_d_base_ainv_update_a.f90:53-79):
+ * d_out = 1 / (1/d + diag(W^T diag(x) Z)), Wt and Z in CSR. */
+int orc_update_a(int n, const int *wt_irp, const int *wt_ja, const double *wt_val,
+                 const int *z_irp, const int *z_ja, const double *z_val,
+                 const double *d, const double *x, double *d_out);
+
 /* ---- application phase --------------------------------------------------*/
 /* y = alpha*A*x + beta*y (PSBLAS CSR csmv, trans='N'); OpenMP over rows. */
 void orc_csr_spmv(int n, const int *irp, const int *ja, const double *val,

@@ -73,6 +73,9 @@ def lib():
         L.orc_invt_build.argtypes = [C.c_int, _i32p, _i32p, _f64p, C.c_int,
                                      C.c_double, C.c_int, C.c_double] + outs
         L.orc_free.argtypes = [C.c_void_p]
+        L.orc_update_a.restype = C.c_int
+        L.orc_update_a.argtypes = [C.c_int, _i32p, _i32p, _f64p, _i32p, _i32p, _f64p,
+                                   _f64p, _f64p, _f64p]
         L.orc_set_threads.argtypes = [C.c_int]
         L.orc_get_threads.restype = C.c_int
         _lib = L
@@ -175,6 +178,18 @@ def invt_build(a: CSR, fillin: int = 20, thresh: float = 0.05,
     return _owned_factors(a.n, lambda *o: lib().orc_invt_build(
         a.n, a.irp, a.ja, a.val, fillin, float(thresh), invfill,
         float(invthresh), *o))
+
+
+def update_a(f: Factors, x) -> np.ndarray:
+    """New d after update_a(x): 1 / (1/d + diag(W^T diag(x) Z))."""
+    n = f.d.shape[0]
+    out = np.empty(n)
+    rc = lib().orc_update_a(n, f.wt.irp, f.wt.ja, f.wt.val, f.z.irp, f.z.ja, f.z.val,
+                            np.ascontiguousarray(f.d, np.float64),
+                            np.ascontiguousarray(x, np.float64), out)
+    if rc != 0:
+        raise RuntimeError(f"orc_update_a failed: {rc}")
+    return out
 
 
 def spmv(a: CSR, x, alpha=1.0, beta=0.0, y=None, trans="N") -> np.ndarray:
