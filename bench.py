@@ -9,8 +9,13 @@ biconjugation with drop tolerance 0.1 and fill cap 20 per column.  Synthetic
 input x ~ U(-1,1) (splitmix64, seed 0).  L2 (126 MB) is flushed between
 timed steps by writing a 256 MB buffer outside the timed events.
 
-value = algorithmic bytes of one apply (nnz_wt*12 + nnz_z*12 + 2*(n+1)*4
-+ n*8 [x] + n*8 [D^-1] + 2*n*8 [t write+read] + n*8 [y]) / device time.
+value = algorithmic bytes of one apply, the unfused CSR minimum of the
+        reference's data structure: nnz_wt*(s_v+4) + nnz_z*(s_v+4)
+        + 2*(n+1)*4 + n*8 [x] + n*s_d [D^-1] + 2*n*s_t [t write+read]
+        + n*8 [y] (FP64: s_v = s_d = s_t = 8), over the device time.  The
+        sliced layout moves fewer bytes than that minimum (offset-mode slices
+        store no per-entry index); those layout bytes are reported next to it
+        (config.layout_*), and the measured DRAM traffic in `roofline`.
 e2e   = the same bytes / time of the host-array entry point
         (ainv_gpu_apply_host: H2D of x, apply, D2H of y; pinned buffers).
 
@@ -42,9 +47,18 @@ WORKLOAD = "convdiff3d_200_upwind_ainv_llk_drop0.1_fill20_apply_N"
 METRIC = "AINV apply GB/s (% HBM peak)"
 
 
-def csr_apply_bytes(n, nnz_wt, nnz_z):
-    """FP64 CSR bytes of one 'N' apply (the reference format, int32 indices)."""
-    return 12 * nnz_wt + 12 * nnz_z + 2 * 4 * (n + 1) + 8 * n + 8 * n + 16 * n + 8 * n
+def csr_stage_bytes(n, nnz_wt, nnz_z, sv=8, sd=8, st=8, si=4):
+    """Algorithmic bytes of the two 'N' sweeps, the per-unit figures of the
+    unfused CSR minimum: (W^T entries + row pointers + x + D^-1 + t write,
+    Z entries + row pointers + t read + y write)."""
+    s1 = nnz_wt * (sv + si) + 4 * (n + 1) + 8 * n + sd * n + st * n
+    s2 = nnz_z * (sv + si) + 4 * (n + 1) + st * n + 8 * n
+    return s1, s2
+
+
+def csr_apply_bytes(n, nnz_wt, nnz_z, sv=8, sd=8, st=8):
+    """Algorithmic bytes of one 'N' apply (reference CSR format, int32 indices)."""
+    return sum(csr_stage_bytes(n, nnz_wt, nnz_z, sv, sd, st))
 
 
 def layout_bytes(n, lay, vsize, tsize):
@@ -215,7 +229,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
     ap.add_argument("--serve-requests", type=int, default=2000)
-    ap.add_argument("--serve-rates", default="50,200,2000",
+    ap.add_argument("--serve-rates", default="50,100,140,2000",
                     help="mean arrival rates (requests/s) of the serving sweep")
     ap.add_argument("--serve-slots", type=int, default=32)
     ap.add_argument("--serve-iters", type=int, default=4)
@@ -266,9 +280,11 @@ def main():
     df = sv.device
     nnz = (len(f["wt_ja"]), len(f["z_ja"]))
     lay = {k: df.layout_info(k) for k in ("wt", "z")}
-    sb = layout_bytes(n, lay, 8, 8)
+    lb = layout_bytes(n, lay, 8, 8)
+    B_lay = lb[0] + lb[1]
+    sb = csr_stage_bytes(n, *nnz)
     B = sb[0] + sb[1]
-    B_csr = csr_apply_bytes(n, *nnz)
+    B_csr = B
     dev = torch.device("cuda", local)
     x = torch.from_numpy(ainv.pde.rand_uniform(0, n)).to(dev)
     y = torch.zeros(n, dtype=torch.float64, device=dev)
@@ -368,8 +384,9 @@ def main():
                "config": {"workload": WORKLOAD if args.idim == IDIM else
                           WORKLOAD.replace("_200_", f"_{args.idim}_"), "n": n, "nnz_A": int(len(ja)),
                           "nnz_wt": nnz[0], "nnz_z": nnz[1], "bytes_per_apply": B,
-                          "csr_bytes_per_apply": B_csr,
-                          "csr_equivalent_GBps": round(B_csr * world / (ms * 1e-3) / 1e9, 1),
+                          "bytes_model": "unfused CSR minimum (12 B per FP64 entry)",
+                          "layout_bytes_per_apply": B_lay,
+                          "layout_GBps": round(B_lay * world / (ms * 1e-3) / 1e9, 1),
                           "layout": "32-row slices, shared column offsets per slice",
                           "offset_slices": [lay["wt"]["offset_slices"], lay["z"]["offset_slices"]],
                           "nslices": lay["wt"]["nslices"],
@@ -380,6 +397,8 @@ def main():
                             "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                             "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
                             "traffic": traffic, "algorithmic_bytes": sb[dom - 1],
+                            "layout_bytes": lb[dom - 1],
+                            "layout_frac": round(lb[dom - 1] / (st_ms[dom] * 1e-3) / 1e9 / peak, 4),
                             "stage_ms": {"k_sweep_dscale": round(st_ms[1], 5),
                                          "k_sweep_axpby": round(st_ms[2], 5)}},
                "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
@@ -399,7 +418,8 @@ def run_extras(ainv, torch, dev, irp, ja, val, f, sv, flush, stream, fp64_ms):
     out = {"mixed": {}, "solve": {}}
     x = torch.from_numpy(ainv.pde.rand_uniform(0, n)).to(dev)
     y = torch.zeros(n, dtype=torch.float64, device=dev)
-    for prec, vs in [("FP32", 4), ("BF16", 2)]:
+    for prec, vs, ts in [("FP32", 4, 4), ("BF16", 2, 4), ("FP32_ACC64", 4, 8),
+                         ("BF16_ACC64", 2, 8)]:
         df = ainv.DeviceFactors((f["wt_irp"], f["wt_ja"], f["wt_val"]),
                                 (f["z_irp"], f["z_ja"], f["z_val"]), f["d"], prec=prec)
         for _ in range(5):
@@ -414,9 +434,11 @@ def run_extras(ainv, torch, dev, irp, ja, val, f, sv, flush, stream, fp64_ms):
             evs.append((a, b))
         torch.cuda.synchronize()
         ms = sum(a.elapsed_time(b) for a, b in evs) / len(evs)
-        Bm = sum(layout_bytes(n, {k: df.layout_info(k) for k in ("wt", "z")}, vs, 4))
+        Bl = sum(layout_bytes(n, {k: df.layout_info(k) for k in ("wt", "z")}, vs, ts))
+        Bm = csr_apply_bytes(n, nnz[0], nnz[1], sv=vs, sd=vs, st=ts)
         out["mixed"][prec] = {"ms": round(ms, 5), "GB/s": round(Bm / (ms * 1e-3) / 1e9, 2),
-                              "bytes": Bm,
+                              "bytes": Bm, "layout_bytes": Bl,
+                              "layout_GBps": round(Bl / (ms * 1e-3) / 1e9, 2),
                               "speedup_vs_fp64": round(fp64_ms / ms, 3)}
         df.close()
     # BiCGSTAB to 1e-9, b = A x*, x* ~ U(-1,1) seed 0
@@ -425,7 +447,7 @@ def run_extras(ainv, torch, dev, irp, ja, val, f, sv, flush, stream, fp64_ms):
     b = torch.zeros(n, dtype=torch.float64, device=dev)
     A.spmv(xs, b, 1.0, 0.0, stream)
     bn = float(torch.linalg.vector_norm(b))
-    for prec in ["FP64", "FP32"]:
+    for prec in ["FP64", "FP32", "BF16", "FP32_ACC64", "BF16_ACC64"]:
         if prec != "FP64":
             sv.cnv(prec)
         df = sv.device
@@ -445,6 +467,27 @@ def run_extras(ainv, torch, dev, irp, ja, val, f, sv, flush, stream, fp64_ms):
                               "true_relres": true_rel, "max_err_vs_xstar": err_x,
                               "s_per_solve": round(min(times), 5),
                               "solves_per_s": round(1.0 / min(times), 3)}
+    # iteration counts move by ~20% under rounding-level changes, so the
+    # precisions are also compared over three right-hand sides (x* seeds 0-2)
+    seeds = {}
+    for prec in ["FP64", "FP32", "BF16", "FP32_ACC64", "BF16_ACC64"]:
+        sv.cnv(prec)
+        its, ts = [], []
+        for seed in range(3):
+            xs_k = torch.from_numpy(ainv.pde.rand_uniform(seed, n)).to(dev)
+            b_k = torch.zeros(n, dtype=torch.float64, device=dev)
+            A.spmv(xs_k, b_k, 1.0, 0.0, stream)
+            xx = torch.zeros(n, dtype=torch.float64, device=dev)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            r_k = A.solve(b_k, xx, sv.device, "BICGSTAB", 1e-9, 2000, stream)
+            ts.append(time.perf_counter() - t0)
+            its.append(r_k.iter)
+        seeds[prec] = {"iters": its, "s_total": round(sum(ts), 4),
+                       "solves_per_s": round(3 / sum(ts), 3)}
+    for prec in ("FP32", "BF16", "FP32_ACC64", "BF16_ACC64"):
+        seeds[prec]["speedup_vs_fp64"] = round(seeds["FP64"]["s_total"] / seeds[prec]["s_total"], 3)
+    out["solve_3rhs"] = seeds
     sv.cnv("FP64")
     out["variants"] = run_variants(ainv, torch, dev, irp, ja, val, A, b, bn, xs, x, y,
                                    flush, stream)
@@ -490,10 +533,11 @@ def run_variants(ainv, torch, dev, irp, ja, val, A, b, bn, xs, x, y, flush, stre
             evs.append((a, e))
         torch.cuda.synchronize()
         ms = sum(a.elapsed_time(e) for a, e in evs) / len(evs)
-        Bv = sum(layout_bytes(n, {k: df.layout_info(k) for k in ("wt", "z")}, 8, 8))
+        Bl = sum(layout_bytes(n, {k: df.layout_info(k) for k in ("wt", "z")}, 8, 8))
+        Bv = csr_apply_bytes(n, rec["nnz_wt"], rec["nnz_z"])
         rec["apply"] = {"ms": round(ms, 5), "GB/s": round(Bv / (ms * 1e-3) / 1e9, 2),
-                        "bytes": Bv,
-                        "csr_bytes": csr_apply_bytes(n, rec["nnz_wt"], rec["nnz_z"])}
+                        "bytes": Bv, "layout_bytes": Bl,
+                        "layout_GBps": round(Bl / (ms * 1e-3) / 1e9, 2)}
         rec["solve"] = {}
         for prec in ("FP64", "FP32"):
             if prec != "FP64":

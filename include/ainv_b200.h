@@ -60,6 +60,10 @@ extern "C" {
 #define AINV_PREC_FP64 0
 #define AINV_PREC_FP32 1
 #define AINV_PREC_BF16 2
+/* FP32 / BF16 storage with FP64 accumulation and an FP64 intermediate: the
+ * same factor bytes as FP32 / BF16, arithmetic as the FP64 apply. */
+#define AINV_PREC_FP32_ACC64 3
+#define AINV_PREC_BF16_ACC64 4
 
 /* ---- Krylov methods --------------------------------------------------- */
 #define AINV_KRYLOV_CG       0

@@ -25,7 +25,7 @@ ERR_NOCONV = 4104
 ERR_UNSUPPORTED = 4105
 ERR_TIMEOUT = 4106
 
-PREC = {"FP64": 0, "FP32": 1, "BF16": 2}
+PREC = {"FP64": 0, "FP32": 1, "BF16": 2, "FP32_ACC64": 3, "BF16_ACC64": 4}
 KRYLOV = {"CG": 0, "BICGSTAB": 1}
 AINV_ALG = {"LLK": 0, "SYM-LLK": 1, "STAB-LLK": 2, "LLK-NOTH": 3, "MLK": 4}
 

@@ -573,6 +573,8 @@ int enqueue_iteration(const MrhsWs *w, const ainv_handle *h, const ainv_csr *a) 
     switch (h->prec) {
       case AINV_PREC_FP64: launch_precond<double, double>(w, h, s); break;
       case AINV_PREC_FP32: launch_precond<float, float>(w, h, s); break;
+      case AINV_PREC_FP32_ACC64: launch_precond<f32w, double>(w, h, s); break;
+      case AINV_PREC_BF16_ACC64: launch_precond<b16w, double>(w, h, s); break;
       default: launch_precond<__nv_bfloat16, float>(w, h, s); break;
     }
   } else {

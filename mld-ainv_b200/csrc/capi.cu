@@ -86,7 +86,7 @@ int ainv_gpu_create(ainv_handle **hp, int n, const int *wt_irp, const int *wt_ja
   if (rc == AINV_SUCCESS) rc = ainv::upload_sell(ainv::transpose(wt), prec, h->w);
   if (rc == AINV_SUCCESS) rc = ainv::upload_values(dinv, (size_t)n, prec, &h->d);
   if (rc == AINV_SUCCESS) {
-    const size_t ts = (prec == AINV_PREC_FP64) ? 8 : 4;
+    const size_t ts = (prec == AINV_PREC_FP32 || prec == AINV_PREC_BF16) ? 4 : 8;
     cudaError_t e = cudaMalloc(&h->t, ts * (size_t)n);
     if (e == cudaSuccess) e = cudaMalloc(&h->status, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(h->status, 0, sizeof(int));
@@ -158,7 +158,7 @@ size_t ainv_gpu_sizeof(const ainv_handle *h) {
   if (!h) return 0;
   size_t b = sizeof(*h) + h->wt.bytes() + h->z.bytes() + h->zt.bytes() + h->w.bytes();
   b += ainv::prec_size(h->prec) * (size_t)h->n;                    // D^-1
-  b += (h->prec == AINV_PREC_FP64 ? 8 : 4) * (size_t)h->n;         // t
+  b += (h->prec == AINV_PREC_FP32 || h->prec == AINV_PREC_BF16 ? 4 : 8) * (size_t)h->n;  // t
   if (h->xs) b += 2 * sizeof(double) * (size_t)h->n;
   return b;
 }

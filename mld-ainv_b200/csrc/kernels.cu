@@ -124,7 +124,7 @@ bool stream_enabled(int prec) {
     return e ? (std::atoi(e) != 0 ? 1 : 0) : -1;
   }();
   if (forced >= 0) return forced == 1;
-  return prec != AINV_PREC_FP64;
+  return prec == AINV_PREC_FP32 || prec == AINV_PREC_BF16;
 }
 
 int sm_count() {
@@ -297,6 +297,9 @@ struct StreamLaunch {
 template <class V, class X, class Epi>
 bool try_stream(const DevSell &m, const X *x, const Epi &epi, int *status, cudaStream_t s,
                 const int *stop) {
+  if constexpr (is_acc64<V>()) {
+    return false;  // register path only
+  } else {
   if (!status || !stream_enabled(m.prec)) return false;
   if ((reinterpret_cast<uintptr_t>(x) & 15u) != 0) return false;  // bulk copies need 16 B
   const RowVecs rv = host_row_vecs(epi);
@@ -310,6 +313,7 @@ bool try_stream(const DevSell &m, const X *x, const Epi &epi, int *status, cudaS
   with_pack<V, 1>(m.pack, StreamLaunch<V, X, Epi>{m, x, epi, status, s, stop, grid, L, smem,
                                                    &launched});
   return launched;
+  }
 }
 
 template <class V, class T>
@@ -336,6 +340,8 @@ int launch_sweep_dscale(const DevSell &m, const void *d, const double *x, void *
     case AINV_PREC_FP64: sweep_dscale<double, double>(m, d, x, t, s, stop, status); break;
     case AINV_PREC_FP32: sweep_dscale<float, float>(m, d, x, t, s, stop, status); break;
     case AINV_PREC_BF16: sweep_dscale<__nv_bfloat16, float>(m, d, x, t, s, stop, status); break;
+    case AINV_PREC_FP32_ACC64: sweep_dscale<f32w, double>(m, d, x, t, s, stop, status); break;
+    case AINV_PREC_BF16_ACC64: sweep_dscale<b16w, double>(m, d, x, t, s, stop, status); break;
     default:
       set_error("unknown precision %d", m.prec);
       return AINV_ERR_ARG;
@@ -350,6 +356,8 @@ int launch_sweep_axpby(const DevSell &m, const void *t, double alpha, double bet
     case AINV_PREC_FP64: sweep_axpby<double, double>(m, t, alpha, beta, y, s, stop, status); break;
     case AINV_PREC_FP32: sweep_axpby<float, float>(m, t, alpha, beta, y, s, stop, status); break;
     case AINV_PREC_BF16: sweep_axpby<__nv_bfloat16, float>(m, t, alpha, beta, y, s, stop, status); break;
+    case AINV_PREC_FP32_ACC64: sweep_axpby<f32w, double>(m, t, alpha, beta, y, s, stop, status); break;
+    case AINV_PREC_BF16_ACC64: sweep_axpby<b16w, double>(m, t, alpha, beta, y, s, stop, status); break;
     default:
       set_error("unknown precision %d", m.prec);
       return AINV_ERR_ARG;

@@ -361,15 +361,17 @@ struct StreamCgSweep2Launch {
 template <class V, class T>
 void launch_cg_sweep2(const DevSell &m, const void *t, const double *r, double *z,
                       KState *st, double *partials, int G, cudaStream_t s) {
-  if (stream_enabled(m.prec)) {
-    StreamLayout L;
-    size_t smem = 0;
-    const int grid = stream_plan(m, (int)sizeof(T), EpiCgZ<T>::kRowVecs, L, smem);
-    bool launched = false;
-    if (grid > 0 && grid <= G && aligned16(t) && aligned16(r))
-      with_pack<V, 1>(m.pack, StreamCgSweep2Launch<V, T>{m, L, grid, smem, t, r, z, st, partials,
-                                                          s, &launched});
-    if (launched) return;
+  if constexpr (!is_acc64<V>()) {
+    if (stream_enabled(m.prec)) {
+      StreamLayout L;
+      size_t smem = 0;
+      const int grid = stream_plan(m, (int)sizeof(T), EpiCgZ<T>::kRowVecs, L, smem);
+      bool launched = false;
+      if (grid > 0 && grid <= G && aligned16(t) && aligned16(r))
+        with_pack<V, 1>(m.pack, StreamCgSweep2Launch<V, T>{m, L, grid, smem, t, r, z, st,
+                                                            partials, s, &launched});
+      if (launched) return;
+    }
   }
   with_group_pack<V>(group_size(m.prec), m.pack,
                      CgSweep2Launch<V, T>{m, t, r, z, st, partials, G, s});
@@ -515,6 +517,8 @@ void precond_sweep2_cg(const ainv_handle *h, const double *r, double *z, KState 
   switch (h->prec) {
     case AINV_PREC_FP64: launch_cg_sweep2<double, double>(h->z, h->t, r, z, st, partials, G, s); break;
     case AINV_PREC_FP32: launch_cg_sweep2<float, float>(h->z, h->t, r, z, st, partials, G, s); break;
+    case AINV_PREC_FP32_ACC64: launch_cg_sweep2<f32w, double>(h->z, h->t, r, z, st, partials, G, s); break;
+    case AINV_PREC_BF16_ACC64: launch_cg_sweep2<b16w, double>(h->z, h->t, r, z, st, partials, G, s); break;
     default: launch_cg_sweep2<__nv_bfloat16, float>(h->z, h->t, r, z, st, partials, G, s); break;
   }
 }

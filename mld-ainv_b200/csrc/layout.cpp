@@ -32,6 +32,8 @@ size_t prec_size(int prec) {
     case AINV_PREC_FP64: return 8;
     case AINV_PREC_FP32: return 4;
     case AINV_PREC_BF16: return 2;
+    case AINV_PREC_FP32_ACC64: return 4;
+    case AINV_PREC_BF16_ACC64: return 2;
     default: return 0;
   }
 }
@@ -315,6 +317,8 @@ int upload_sell(const HostCsr &a, int prec, DevSell &out) {
     case AINV_PREC_FP64: return upload_sell_t<double>(a, prec, out);
     case AINV_PREC_FP32: return upload_sell_t<float>(a, prec, out);
     case AINV_PREC_BF16: return upload_sell_t<uint16_t>(a, prec, out);
+    case AINV_PREC_FP32_ACC64: return upload_sell_t<float>(a, prec, out);
+    case AINV_PREC_BF16_ACC64: return upload_sell_t<uint16_t>(a, prec, out);
     default:
       set_error("unknown precision %d", prec);
       return AINV_ERR_ARG;
@@ -341,7 +345,7 @@ int upload_values(const double *h, size_t n, int prec, void **dptr) {
   for (size_t i = 0; i < n; i++) {
     if (prec == AINV_PREC_FP64) {
       std::memcpy(&buf[i * es], &h[i], 8);
-    } else if (prec == AINV_PREC_FP32) {
+    } else if (prec == AINV_PREC_FP32 || prec == AINV_PREC_FP32_ACC64) {
       float f = (float)h[i];
       std::memcpy(&buf[i * es], &f, 4);
     } else {

@@ -4,6 +4,8 @@
 
 #include <cuda_bf16.h>
 
+#include <type_traits>
+
 #include "internal.h"
 
 namespace ainv {
@@ -33,6 +35,35 @@ __device__ __forceinline__ float ldd(const __nv_bfloat16 *p) {
   unsigned short u = __ldg(reinterpret_cast<const unsigned short *>(p));
   return __uint_as_float(((unsigned)u) << 16);
 }
+
+// Storage types of the FP64-accumulating modes (AINV_PREC_FP32_ACC64,
+// AINV_PREC_BF16_ACC64): FP32 / BF16 values whose loads yield FP64, so the
+// products, sums and the intermediate are those of the FP64 apply.
+struct f32w {
+  float v;
+  f32w() = default;
+  __host__ __device__ explicit f32w(double x) : v((float)x) {}
+};
+struct b16w {
+  unsigned short v;
+  b16w() = default;
+  __host__ __device__ explicit b16w(double x)
+      : v(__bfloat16_as_ushort(__double2bfloat16(x))) {}
+};
+template <>
+struct Acc<f32w> { using type = double; };
+template <>
+struct Acc<b16w> { using type = double; };
+__device__ __forceinline__ double ldv(const f32w *p) { return (double)__ldcs(&p->v); }
+__device__ __forceinline__ double ldv(const b16w *p) {
+  return (double)__uint_as_float(((unsigned)__ldcs(&p->v)) << 16);
+}
+__device__ __forceinline__ double ldd(const f32w *p) { return (double)__ldg(&p->v); }
+__device__ __forceinline__ double ldd(const b16w *p) {
+  return (double)__uint_as_float(((unsigned)__ldg(&p->v)) << 16);
+}
+template <class V>
+constexpr bool is_acc64() { return std::is_same<V, f32w>::value || std::is_same<V, b16w>::value; }
 
 // Kernel-side view of a DevSell with typed values.
 template <class V>
@@ -127,6 +158,25 @@ struct Pack<__nv_bfloat16, 8> {
   }
 };
 
+template <int P>
+struct Pack<f32w, P> {
+  static __device__ __forceinline__ void load(const f32w *p, double (&o)[P]) {
+    float f[P];
+    Pack<float, P>::load(reinterpret_cast<const float *>(p), f);
+#pragma unroll
+    for (int e = 0; e < P; e++) o[e] = (double)f[e];
+  }
+};
+template <int P>
+struct Pack<b16w, P> {
+  static __device__ __forceinline__ void load(const b16w *p, double (&o)[P]) {
+    float f[P];
+    Pack<__nv_bfloat16, P>::load(reinterpret_cast<const __nv_bfloat16 *>(p), f);
+#pragma unroll
+    for (int e = 0; e < P; e++) o[e] = (double)f[e];
+  }
+};
+
 // P adjacent int32 words: streaming (per-slot columns) or cached (offsets).
 template <int P, bool STREAM>
 __device__ __forceinline__ void load_ints(const int *p, int (&o)[P]) {
@@ -218,22 +268,22 @@ __device__ __forceinline__ void group_ctx(const SellView<V> &m, int g, GroupCtx<
   }
 }
 
-// Packs per loop step: 4 slots for P <= 4, one pack for P = 8.
-template <int P>
-struct Step { static constexpr int kPacks = P >= 4 ? 1 : 4 / P; };
+// Packs per loop step: K slots (K = 4 or 8), at least one pack.
+template <int P, int K = 4>
+struct Step { static constexpr int kPacks = P >= K ? 1 : K / P; };
 
 // Slots [k0, k0 + kPacks*P) of the S slices of a group, all in the same
 // index encoding (OM: shared offsets; else per-slot columns).  Loads are
 // predicated per pack (w is a multiple of P), so all value / index loads of
 // the step are in flight before the first dependent gather; the FMAs then
 // run in slot order, which is the row's column order.
-template <bool OM, int P, class V, class X, int S>
+template <bool OM, int P, int K, class V, class X, int S>
 __device__ __forceinline__ void group_slots(const SellView<V> &m, const GroupCtx<S> &c,
                                             const int (&row)[S], int k0,
                                             const X *__restrict__ x,
                                             typename Acc<V>::type (&acc)[S]) {
   using A = typename Acc<V>::type;
-  constexpr int J = Step<P>::kPacks;
+  constexpr int J = Step<P, K>::kPacks;
   const int lane = threadIdx.x & 31;
   int col[S][J][P];
   A vv[S][J][P];
@@ -283,12 +333,12 @@ __device__ __forceinline__ void group_slots(const SellView<V> &m, const GroupCtx
 // acc[q] = row (g*S+q)*32+lane of M dotted with x.  The encoding test is
 // warp-uniform and sits outside the slot loop; a group mixing both
 // encodings is walked one slice at a time.
-template <int P, class V, class X, int S>
+template <int P, int K = 4, class V, class X, int S>
 __device__ __forceinline__ void group_dot(const SellView<V> &m, const GroupCtx<S> &c, int g,
                                           const X *__restrict__ x,
                                           typename Acc<V>::type (&acc)[S]) {
   using A = typename Acc<V>::type;
-  constexpr int KS = Step<P>::kPacks * P;
+  constexpr int KS = Step<P, K>::kPacks * P;
   const int lane = threadIdx.x & 31;
   int row[S];
   bool all_om = true, all_col = true;
@@ -302,9 +352,9 @@ __device__ __forceinline__ void group_dot(const SellView<V> &m, const GroupCtx<S
     }
   }
   if (all_om) {
-    for (int k0 = 0; k0 < c.maxw; k0 += KS) group_slots<true, P>(m, c, row, k0, x, acc);
+    for (int k0 = 0; k0 < c.maxw; k0 += KS) group_slots<true, P, K>(m, c, row, k0, x, acc);
   } else if (all_col) {
-    for (int k0 = 0; k0 < c.maxw; k0 += KS) group_slots<false, P>(m, c, row, k0, x, acc);
+    for (int k0 = 0; k0 < c.maxw; k0 += KS) group_slots<false, P, K>(m, c, row, k0, x, acc);
   } else {
 #pragma unroll
     for (int q = 0; q < S; q++) {
@@ -317,9 +367,9 @@ __device__ __forceinline__ void group_dot(const SellView<V> &m, const GroupCtx<S
       const int r1[1] = {row[q]};
       A a1[1] = {A(0)};
       if (c.om[q]) {
-        for (int k0 = 0; k0 < c1.maxw; k0 += KS) group_slots<true, P>(m, c1, r1, k0, x, a1);
+        for (int k0 = 0; k0 < c1.maxw; k0 += KS) group_slots<true, P, K>(m, c1, r1, k0, x, a1);
       } else {
-        for (int k0 = 0; k0 < c1.maxw; k0 += KS) group_slots<false, P>(m, c1, r1, k0, x, a1);
+        for (int k0 = 0; k0 < c1.maxw; k0 += KS) group_slots<false, P, K>(m, c1, r1, k0, x, a1);
       }
       acc[q] = a1[0];
     }
@@ -328,7 +378,7 @@ __device__ __forceinline__ void group_dot(const SellView<V> &m, const GroupCtx<S
 
 // Visit every row of M: epi(row, acc) for rows < n, S slices per warp step,
 // warps striding over the grid.
-template <int S, int P, class V, class X, class Epi>
+template <int S, int P, int K = 4, class V, class X, class Epi>
 __device__ __forceinline__ void for_each_row(const SellView<V> &m, const X *__restrict__ x,
                                              Epi &&epi) {
   const int ngroups = (m.nslices + S - 1) / S;
@@ -337,7 +387,7 @@ __device__ __forceinline__ void for_each_row(const SellView<V> &m, const X *__re
     GroupCtx<S> c;
     group_ctx(m, g, c);
     typename Acc<V>::type acc[S];
-    group_dot<P>(m, c, g, x, acc);
+    group_dot<P, K>(m, c, g, x, acc);
 #pragma unroll
     for (int q = 0; q < S; q++) {
       const int row = (g * S + q) * kSlice + lane;

@@ -247,6 +247,8 @@ __global__ void __launch_bounds__(kBlock) k_srv_sweep1(const Table *tab, SlotSta
   switch (sd.wt.prec) {
     case AINV_PREC_FP64: sweep1_body<double, double>(sd, x, lb, nb); break;
     case AINV_PREC_FP32: sweep1_body<float, float>(sd, x, lb, nb); break;
+    case AINV_PREC_FP32_ACC64: sweep1_body<f32w, double>(sd, x, lb, nb); break;
+    case AINV_PREC_BF16_ACC64: sweep1_body<b16w, double>(sd, x, lb, nb); break;
     default: sweep1_body<__nv_bfloat16, float>(sd, x, lb, nb); break;
   }
 }
@@ -266,6 +268,8 @@ __global__ void __launch_bounds__(kBlock) k_srv_sweep2(const Table *tab, SlotSta
   switch (sd.z.prec) {
     case AINV_PREC_FP64: sweep2_body<double, double>(sd, y, lb, nb); break;
     case AINV_PREC_FP32: sweep2_body<float, float>(sd, y, lb, nb); break;
+    case AINV_PREC_FP32_ACC64: sweep2_body<f32w, double>(sd, y, lb, nb); break;
+    case AINV_PREC_BF16_ACC64: sweep2_body<b16w, double>(sd, y, lb, nb); break;
     default: sweep2_body<__nv_bfloat16, float>(sd, y, lb, nb); break;
   }
 }
@@ -400,7 +404,7 @@ int chunks_of(int n) { return (n + kChunkRows - 1) / kChunkRows; }
 // intermediate and the chunk partials.
 size_t request_bytes(int n) {
   const size_t st = vec_stride(n) * sizeof(double);
-  return round256(kNumVec * st + st + 3 * sizeof(double) * (size_t)chunks_of(n));
+  return round256(kNumVec * st + st + 3 * sizeof(double) * (size_t)chunks_of(n));  // t: <= 8 B/row
 }
 
 // First-fit allocator over the server's device arena (offsets only).
@@ -748,17 +752,11 @@ int ainv_server_create(ainv_server **out, int max_slots, size_t hbm_bytes, int i
   if (e == cudaSuccess)
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, srv->device);
   if (e != cudaSuccess) return fail(e, "device query");
-  // one resident wave of the heaviest batched kernel, so every kernel of the
-  // graph runs its blocks in a single wave
-  const long long big = 1LL << 40;
-  int wave = wave_grid((const void *)k_srv_init, big);
-  for (const void *k : {(const void *)k_srv_p, (const void *)k_srv_s, (const void *)k_srv_sweep1,
-                        (const void *)k_srv_sweep2, (const void *)k_srv_spmv<kBicgSigma>,
-                        (const void *)k_srv_spmv<kBicgOmega>, (const void *)k_srv_spmv<kTrueRes>,
-                        (const void *)k_srv_xr, (const void *)k_srv_replace})
-    wave = std::min(wave, wave_grid(k, big));
-  (void)sms;
-  srv->grid = std::min(kMaxGrid, std::max(max_slots, wave));
+  // 8 blocks of 256 threads per SM: a full wave for the light batched
+  // kernels; the register-heavy SpMV / sweep kernels run it in a few waves.
+  // (A grid of one wave of the heaviest kernel measured 35% fewer solves/s:
+  // the light kernels, latency-bound, then had too few blocks.)
+  srv->grid = std::min(kMaxGrid, std::max(max_slots, 8 * sms));
   // admission budget: the caller's bytes, or half of the free HBM
   size_t fr = 0, tot = 0;
   e = cudaMemGetInfo(&fr, &tot);

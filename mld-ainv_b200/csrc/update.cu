@@ -80,6 +80,14 @@ int update_a_async(ainv_handle *h, const double *x, double *d64, cudaStream_t s)
       k_update_a<float><<<G, kBlock, 0, s>>>(view<float>(h->wt), h->wt.pack, view<float>(h->zt),
                                               h->zt.pack, x, (float *)h->d, d64);
       break;
+    case AINV_PREC_FP32_ACC64:
+      k_update_a<f32w><<<G, kBlock, 0, s>>>(view<f32w>(h->wt), h->wt.pack, view<f32w>(h->zt),
+                                             h->zt.pack, x, (f32w *)h->d, d64);
+      break;
+    case AINV_PREC_BF16_ACC64:
+      k_update_a<b16w><<<G, kBlock, 0, s>>>(view<b16w>(h->wt), h->wt.pack, view<b16w>(h->zt),
+                                             h->zt.pack, x, (b16w *)h->d, d64);
+      break;
     default:
       k_update_a<__nv_bfloat16><<<G, kBlock, 0, s>>>(view<__nv_bfloat16>(h->wt), h->wt.pack,
                                                       view<__nv_bfloat16>(h->zt), h->zt.pack, x,
