@@ -52,6 +52,14 @@ __global__ void __launch_bounds__(kBlock)
 template <class V>
 __device__ __forceinline__ typename Acc<V>::type to_acc(V v) { return v; }
 template <>
+__device__ __forceinline__ double to_acc<f32w>(f32w v) {
+  return (double)v.v;
+}
+template <>
+__device__ __forceinline__ double to_acc<b16w>(b16w v) {
+  return (double)__uint_as_float(((unsigned)v.v) << 16);
+}
+template <>
 __device__ __forceinline__ float to_acc<__nv_bfloat16>(__nv_bfloat16 v) {
   return __uint_as_float(((unsigned)__bfloat16_as_ushort(v)) << 16);
 }
@@ -124,7 +132,7 @@ bool stream_enabled(int prec) {
     return e ? (std::atoi(e) != 0 ? 1 : 0) : -1;
   }();
   if (forced >= 0) return forced == 1;
-  return prec == AINV_PREC_FP32 || prec == AINV_PREC_BF16;
+  return prec != AINV_PREC_FP64;
 }
 
 int sm_count() {
@@ -297,9 +305,6 @@ struct StreamLaunch {
 template <class V, class X, class Epi>
 bool try_stream(const DevSell &m, const X *x, const Epi &epi, int *status, cudaStream_t s,
                 const int *stop) {
-  if constexpr (is_acc64<V>()) {
-    return false;  // register path only
-  } else {
   if (!status || !stream_enabled(m.prec)) return false;
   if ((reinterpret_cast<uintptr_t>(x) & 15u) != 0) return false;  // bulk copies need 16 B
   const RowVecs rv = host_row_vecs(epi);
@@ -313,7 +318,6 @@ bool try_stream(const DevSell &m, const X *x, const Epi &epi, int *status, cudaS
   with_pack<V, 1>(m.pack, StreamLaunch<V, X, Epi>{m, x, epi, status, s, stop, grid, L, smem,
                                                    &launched});
   return launched;
-  }
 }
 
 template <class V, class T>

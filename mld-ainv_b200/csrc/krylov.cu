@@ -361,17 +361,15 @@ struct StreamCgSweep2Launch {
 template <class V, class T>
 void launch_cg_sweep2(const DevSell &m, const void *t, const double *r, double *z,
                       KState *st, double *partials, int G, cudaStream_t s) {
-  if constexpr (!is_acc64<V>()) {
-    if (stream_enabled(m.prec)) {
-      StreamLayout L;
-      size_t smem = 0;
-      const int grid = stream_plan(m, (int)sizeof(T), EpiCgZ<T>::kRowVecs, L, smem);
-      bool launched = false;
-      if (grid > 0 && grid <= G && aligned16(t) && aligned16(r))
-        with_pack<V, 1>(m.pack, StreamCgSweep2Launch<V, T>{m, L, grid, smem, t, r, z, st,
-                                                            partials, s, &launched});
-      if (launched) return;
-    }
+  if (stream_enabled(m.prec)) {
+    StreamLayout L;
+    size_t smem = 0;
+    const int grid = stream_plan(m, (int)sizeof(T), EpiCgZ<T>::kRowVecs, L, smem);
+    bool launched = false;
+    if (grid > 0 && grid <= G && aligned16(t) && aligned16(r))
+      with_pack<V, 1>(m.pack, StreamCgSweep2Launch<V, T>{m, L, grid, smem, t, r, z, st, partials,
+                                                          s, &launched});
+    if (launched) return;
   }
   with_group_pack<V>(group_size(m.prec), m.pack,
                      CgSweep2Launch<V, T>{m, t, r, z, st, partials, G, s});

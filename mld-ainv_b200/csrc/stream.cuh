@@ -225,7 +225,24 @@ struct SPack<__nv_bfloat16, P> {
     }
   }
 };
-
+template <int P>
+struct SPack<f32w, P> {
+  static __device__ __forceinline__ void load(const f32w *p, double (&o)[P]) {
+    float f[P];
+    SPack<float, P>::load(reinterpret_cast<const float *>(p), f);
+#pragma unroll
+    for (int e = 0; e < P; e++) o[e] = (double)f[e];
+  }
+};
+template <int P>
+struct SPack<b16w, P> {
+  static __device__ __forceinline__ void load(const b16w *p, double (&o)[P]) {
+    float f[P];
+    SPack<__nv_bfloat16, P>::load(reinterpret_cast<const __nv_bfloat16 *>(p), f);
+#pragma unroll
+    for (int e = 0; e < P; e++) o[e] = (double)f[e];
+  }
+};
 
 // Element range [a, e) of the window of offset o for rows [r0, r1) of an
 // n-element vector: the rows' columns, widened to whole 16-byte granules.
