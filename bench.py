@@ -179,6 +179,23 @@ def cpu_baseline_apply(f, n, budget_s=10.0, max_reps=200):
     return dt, reps, O.get_threads()
 
 
+def max_over_ranks(v, world, torch, dist, device):
+    """The largest v over the ranks (every rank receives it)."""
+    if world == 1:
+        return v
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(ms_local, bytes_per_step, world, allmax):
+    """Replicas only: every rank applies its own copy of the factors, with no
+    data-path collective.  The job's step time is the slowest rank's, and the
+    job moved world x bytes_per_step in it.  Returns (ms, GB/s)."""
+    ms = allmax(ms_local)
+    return ms, bytes_per_step * world / (ms * 1e-3) / 1e9
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -264,11 +281,7 @@ def main():
             dist.barrier()
 
     def allmax(v):
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks(v, world, torch, dist, "cuda")
 
     if args.leg != "all":
         return run_leg(ainv, torch, args)
@@ -308,9 +321,7 @@ def main():
             ev[k][1].record(stream)
         torch.cuda.synchronize()
         barrier()
-    ms = sum(a.elapsed_time(b) for a, b in ev) / K
-    ms = allmax(ms)
-    value = B * world / (ms * 1e-3) / 1e9
+    ms, value = replica_value(sum(a.elapsed_time(b) for a, b in ev) / K, B, world, allmax)
 
     # per-sweep timing (roofline of the dominant kernel)
     K2 = min(K, 100)
@@ -360,13 +371,13 @@ def main():
            "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
            "ms_per_step": round(e2e_ms, 4)}
 
+    # the extra legs (solves, variants, block CG, serving) describe one GPU;
+    # replica runs (N > 1) report the apply metric only
     extras = {}
-    if not args.no_extras:
+    if not args.no_extras and world == 1:
         extras = run_extras(ainv, torch, dev, irp, ja, val, f, sv, flush, stream, ms)
-
-    if not args.no_extras:
         extras["block_cg"] = run_block_cg(ainv, torch, dev)
-    if not args.no_serve:
+    if not args.no_serve and world == 1:
         extras["serving"] = run_serving(ainv, torch, args)
 
     cpu = None
