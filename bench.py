@@ -249,6 +249,10 @@ def main():
     ap.add_argument("--serve-rates", default="50,100,140,2000",
                     help="mean arrival rates (requests/s) of the serving sweep")
     ap.add_argument("--serve-slots", type=int, default=32)
+    ap.add_argument("--serve-hbm-gb", type=float, default=0.0,
+                    help="device memory for admitted requests (0: half of the free HBM)")
+    ap.add_argument("--serve-prec", default="FP32",
+                    help="factor precision of the served operators (FP32: the workload's)")
     ap.add_argument("--serve-iters", type=int, default=4)
     ap.add_argument("--leg", default="all", choices=["all", "block", "solve", "serve"],
                     help="run one leg alone (profiler captures of its kernels)")
@@ -683,7 +687,7 @@ def run_serving(ainv, torch, args):
         ops.append((ainv.DeviceOperator(irp, ja, val),
                     ainv.DeviceFactors((f["wt_irp"], f["wt_ja"], f["wt_val"]),
                                        (f["z_irp"], f["z_ja"], f["z_val"]), f["d"],
-                                       prec="FP32"), sp.n))
+                                       prec=args.serve_prec), sp.n))
     t_build = time.perf_counter() - t0
     nreq = args.serve_requests
     opsel = workload.request_ops(nreq, len(ops))
@@ -693,7 +697,8 @@ def run_serving(ainv, torch, args):
 
     def stream(rate, count, slots):
         arr = workload.poisson_arrivals(rate, count)
-        with serve.SolveServer(max_slots=slots, iters_per_launch=args.serve_iters) as srv:
+        with serve.SolveServer(max_slots=slots, iters_per_launch=args.serve_iters,
+                               hbm_bytes=int(args.serve_hbm_gb * 2**30)) as srv:
             ids = [srv.add_operator(a, f) for a, f, _ in ops]
             srv.wait(srv.submit(ids[0], rhs[0], xs[0]))  # warm-up
             start = time.perf_counter()
@@ -729,7 +734,7 @@ def run_serving(ainv, torch, args):
         a.close()
     return {"operators": [{"idim": sp.idim, "kind": sp.kind,
                            "beta": [round(b, 3) for b in sp.beta]} for sp in specs],
-            "factors": "AINV LLK drop 0.1 fill 20, FP32", "tol": 1e-8,
+            "factors": f"AINV LLK drop 0.1 fill 20, {args.serve_prec}", "tol": 1e-8,
             "slots": args.serve_slots, "iters_per_launch": args.serve_iters,
             "build_s": round(t_build, 1), "sweep": sweep, "unbatched_one_slot": unbatched}
 

@@ -137,6 +137,47 @@ __device__ __forceinline__ void chunk_store(double (&v)[NV], double *__restrict_
   }
 }
 
+// The block's chunks lb, lb+nb, ... in batches of kChunkBatch: body(c, pr)
+// accumulates chunk c's NV sums in pr; each warp folds its lanes (fixed
+// shuffle tree) into a shared slot without waiting, and one barrier per
+// batch lets the block fold its warps in order and store the chunk sums at
+// partials[i*nchunks + c] -- the same values chunk_store gives.
+constexpr int kChunkBatch = 4;
+template <int NV, class Body>
+__device__ __forceinline__ void for_chunks(int lb, int nb, int nchunks,
+                                           double *__restrict__ partials, Body &&body) {
+  __shared__ double sh[kChunkBatch][NV][kWarps];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int c0 = lb; c0 < nchunks; c0 += kChunkBatch * nb) {
+#pragma unroll
+    for (int q = 0; q < kChunkBatch; q++) {
+      const int c = c0 + q * nb;
+      if (c >= nchunks) break;  // block-uniform
+      double pr[NV];
+#pragma unroll
+      for (int i = 0; i < NV; i++) pr[i] = 0.0;
+      body(c, pr);
+#pragma unroll
+      for (int i = 0; i < NV; i++) {
+        double v = pr[i];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) sh[q][i][warp] = v;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x < kChunkBatch * NV) {
+      const int q = threadIdx.x / NV, i = threadIdx.x % NV, c = c0 + q * nb;
+      if (c < nchunks) {
+        double s = 0.0;
+        for (int w = 0; w < kWarps; w++) s += sh[q][i][w];
+        partials[i * nchunks + c] = s;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // The slot's last block (atomic ticket, no waiting) folds the chunk sums in
 // chunk order; true in that block, totals in thread 0.
 template <int NV>
@@ -183,8 +224,7 @@ __global__ void __launch_bounds__(kBlock) k_srv_init(const Table *tab, SlotState
   SRV_PROLOGUE(ss->phase == kInitPhase)
   double *x = sd.vec[VX], *r = sd.vec[VR], *rt = sd.vec[VRT], *p = sd.vec[VP], *v = sd.vec[VV];
   const double *b = sd.vec[VB];
-  for (int c = lb; c < sd.nchunks; c += nb) {
-    double pr[1] = {0.0};
+  for_chunks<1>(lb, nb, sd.nchunks, sd.partials, [&](int c, double (&pr)[1]) {
 #pragma unroll
     for (int h = 0; h < kGroupS; h++) {
       const int i = c * kChunkRows + h * kBlock + threadIdx.x;
@@ -198,8 +238,7 @@ __global__ void __launch_bounds__(kBlock) k_srv_init(const Table *tab, SlotState
         pr[0] += bi * bi;
       }
     }
-    chunk_store<1>(pr, sd.partials, sd.nchunks, c);
-  }
+  });
   double tot[1] = {0.0};
   if (slot_fold<1>(tot, sd.partials, sd.nchunks, nb, &st->ticket[0]) && threadIdx.x == 0) {
     const double bn = sqrt(tot[0]);
@@ -240,16 +279,29 @@ __device__ __forceinline__ void sweep1_body(const SlotDesc &sd, const double *sr
   for (int c = lb; c < sd.nchunks; c += nb) chunk_rows<V>(sd.wt, c, src, epi);
 }
 
+// Factor precisions come in two kernel families, so each kernel's register
+// budget is that of its own value types: FP64 / FP32 / BF16 (ACC = false)
+// and the FP64-accumulating FP32 / BF16 storage (ACC = true).
+__host__ __device__ inline bool acc64_prec(int prec) {
+  return prec == AINV_PREC_FP32_ACC64 || prec == AINV_PREC_BF16_ACC64;
+}
+
+template <bool ACC>
 __global__ void __launch_bounds__(kBlock) k_srv_sweep1(const Table *tab, SlotState *sts,
                                                        int src) {
-  SRV_PROLOGUE(SRV_RUNNING)
+  SRV_PROLOGUE(SRV_RUNNING && acc64_prec(tab->slot[slot].wt.prec) == ACC)
   const double *x = sd.vec[src];
-  switch (sd.wt.prec) {
-    case AINV_PREC_FP64: sweep1_body<double, double>(sd, x, lb, nb); break;
-    case AINV_PREC_FP32: sweep1_body<float, float>(sd, x, lb, nb); break;
-    case AINV_PREC_FP32_ACC64: sweep1_body<f32w, double>(sd, x, lb, nb); break;
-    case AINV_PREC_BF16_ACC64: sweep1_body<b16w, double>(sd, x, lb, nb); break;
-    default: sweep1_body<__nv_bfloat16, float>(sd, x, lb, nb); break;
+  if constexpr (ACC) {
+    if (sd.wt.prec == AINV_PREC_FP32_ACC64)
+      sweep1_body<f32w, double>(sd, x, lb, nb);
+    else
+      sweep1_body<b16w, double>(sd, x, lb, nb);
+  } else {
+    switch (sd.wt.prec) {
+      case AINV_PREC_FP64: sweep1_body<double, double>(sd, x, lb, nb); break;
+      case AINV_PREC_FP32: sweep1_body<float, float>(sd, x, lb, nb); break;
+      default: sweep1_body<__nv_bfloat16, float>(sd, x, lb, nb); break;
+    }
   }
 }
 
@@ -261,16 +313,22 @@ __device__ __forceinline__ void sweep2_body(const SlotDesc &sd, double *dst, int
   for (int c = lb; c < sd.nchunks; c += nb) chunk_rows<V>(sd.z, c, t, epi);
 }
 
+template <bool ACC>
 __global__ void __launch_bounds__(kBlock) k_srv_sweep2(const Table *tab, SlotState *sts,
                                                        int dst) {
-  SRV_PROLOGUE(SRV_RUNNING)
+  SRV_PROLOGUE(SRV_RUNNING && acc64_prec(tab->slot[slot].z.prec) == ACC)
   double *y = sd.vec[dst];
-  switch (sd.z.prec) {
-    case AINV_PREC_FP64: sweep2_body<double, double>(sd, y, lb, nb); break;
-    case AINV_PREC_FP32: sweep2_body<float, float>(sd, y, lb, nb); break;
-    case AINV_PREC_FP32_ACC64: sweep2_body<f32w, double>(sd, y, lb, nb); break;
-    case AINV_PREC_BF16_ACC64: sweep2_body<b16w, double>(sd, y, lb, nb); break;
-    default: sweep2_body<__nv_bfloat16, float>(sd, y, lb, nb); break;
+  if constexpr (ACC) {
+    if (sd.z.prec == AINV_PREC_FP32_ACC64)
+      sweep2_body<f32w, double>(sd, y, lb, nb);
+    else
+      sweep2_body<b16w, double>(sd, y, lb, nb);
+  } else {
+    switch (sd.z.prec) {
+      case AINV_PREC_FP64: sweep2_body<double, double>(sd, y, lb, nb); break;
+      case AINV_PREC_FP32: sweep2_body<float, float>(sd, y, lb, nb); break;
+      default: sweep2_body<__nv_bfloat16, float>(sd, y, lb, nb); break;
+    }
   }
 }
 
@@ -293,7 +351,7 @@ __device__ __forceinline__ bool srv_spmv_active(const SlotState *ss, bool *verif
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(kBlock) k_srv_spmv(const Table *tab, SlotState *sts) {
+__global__ void __launch_bounds__(kBlock, 4) k_srv_spmv(const Table *tab, SlotState *sts) {
   bool verify;
   SRV_PROLOGUE(srv_spmv_active<MODE>(ss, &verify))
   const double *x, *w1, *w3 = nullptr;
@@ -313,8 +371,7 @@ __global__ void __launch_bounds__(kBlock) k_srv_spmv(const Table *tab, SlotState
     w2 = sd.vec[VRT];
     w3 = sd.vec[VR];
   }
-  for (int c = lb; c < sd.nchunks; c += nb) {
-    double pr[3] = {0.0, 0.0, 0.0};
+  for_chunks<3>(lb, nb, sd.nchunks, sd.partials, [&](int c, double (&pr)[3]) {
     auto epi = [&](int i, double acc) {
       if (MODE == kTrueRes) {
         const double ri = w1[i] - acc;
@@ -333,8 +390,7 @@ __global__ void __launch_bounds__(kBlock) k_srv_spmv(const Table *tab, SlotState
       }
     };
     chunk_rows<double>(sd.A, c, x, epi);
-    chunk_store<3>(pr, sd.partials, sd.nchunks, c);
-  }
+  });
   double tot[3] = {0.0, 0.0, 0.0};
   if (slot_fold<3>(tot, sd.partials, sd.nchunks, nb, &st->ticket[0]) && threadIdx.x == 0)
     finish_dots<MODE>(st, tot, verify, w2);
@@ -347,8 +403,7 @@ __global__ void __launch_bounds__(kBlock) k_srv_xr(const Table *tab, SlotState *
                *rt = sd.vec[VRT];
   double *x = sd.vec[VX], *r = sd.vec[VR];
   const double alpha = st->alpha, omega = st->omega;
-  for (int c = lb; c < sd.nchunks; c += nb) {
-    double pr[2] = {0.0, 0.0};
+  for_chunks<2>(lb, nb, sd.nchunks, sd.partials, [&](int c, double (&pr)[2]) {
 #pragma unroll
     for (int h = 0; h < kGroupS; h++) {
       const int i = c * kChunkRows + h * kBlock + threadIdx.x;
@@ -360,8 +415,7 @@ __global__ void __launch_bounds__(kBlock) k_srv_xr(const Table *tab, SlotState *
         pr[1] += rt[i] * ri;
       }
     }
-    chunk_store<2>(pr, sd.partials, sd.nchunks, c);
-  }
+  });
   double tot[2] = {0.0, 0.0};
   if (slot_fold<2>(tot, sd.partials, sd.nchunks, nb, &st->ticket[0]) && threadIdx.x == 0) {
     finish_iteration(st, tot[0]);
@@ -377,15 +431,25 @@ __global__ void __launch_bounds__(kBlock) k_srv_replace(const Table *tab, SlotSt
   for (int i = lb * kBlock + threadIdx.x; i < n; i += nb * kBlock) r[i] = rtrue[i];
 }
 
-// One batched iteration on stream s (11 launches over the whole grid).
-cudaError_t enqueue_iteration(const Table *tab, SlotState *sts, int grid, cudaStream_t s) {
+enum Family { kFamStd = 1, kFamAcc64 = 2 };
+
+void sweeps(const Table *tab, SlotState *sts, int grid, cudaStream_t s, int fam, int src,
+            int dst) {
+  if (fam & kFamStd) k_srv_sweep1<false><<<grid, kBlock, 0, s>>>(tab, sts, src);
+  if (fam & kFamAcc64) k_srv_sweep1<true><<<grid, kBlock, 0, s>>>(tab, sts, src);
+  if (fam & kFamStd) k_srv_sweep2<false><<<grid, kBlock, 0, s>>>(tab, sts, dst);
+  if (fam & kFamAcc64) k_srv_sweep2<true><<<grid, kBlock, 0, s>>>(tab, sts, dst);
+}
+
+// One batched iteration on stream s (11 launches over the whole grid, plus
+// the second family's two sweeps when both families are registered).
+cudaError_t enqueue_iteration(const Table *tab, SlotState *sts, int grid, cudaStream_t s,
+                              int fam) {
   k_srv_p<<<grid, kBlock, 0, s>>>(tab, sts);
-  k_srv_sweep1<<<grid, kBlock, 0, s>>>(tab, sts, VP);
-  k_srv_sweep2<<<grid, kBlock, 0, s>>>(tab, sts, VF);
+  sweeps(tab, sts, grid, s, fam, VP, VF);
   k_srv_spmv<kBicgSigma><<<grid, kBlock, 0, s>>>(tab, sts);
   k_srv_s<<<grid, kBlock, 0, s>>>(tab, sts);
-  k_srv_sweep1<<<grid, kBlock, 0, s>>>(tab, sts, VS);
-  k_srv_sweep2<<<grid, kBlock, 0, s>>>(tab, sts, VZ);
+  sweeps(tab, sts, grid, s, fam, VS, VZ);
   k_srv_spmv<kBicgOmega><<<grid, kBlock, 0, s>>>(tab, sts);
   k_srv_xr<<<grid, kBlock, 0, s>>>(tab, sts);
   k_srv_spmv<kTrueRes><<<grid, kBlock, 0, s>>>(tab, sts);
@@ -488,6 +552,8 @@ struct ainv_server {
   cudaStream_t s = nullptr;
   cudaGraphExec_t exec = nullptr;
   ainv::srv::Table *tab_d = nullptr, *tab_h = nullptr;
+  ainv::srv::Table *tab_empty_d = nullptr;  // all blocks idle: settles new kernels
+  int fam = 0, graph_fam = 0;               // kernel families registered / in the graph
   ainv::srv::SlotState *st_d = nullptr, *st_h = nullptr;
   char *arena_d = nullptr;
   ainv::srv::Arena arena;
@@ -515,6 +581,37 @@ struct ainv_server {
 namespace ainv {
 namespace srv {
 namespace {
+
+// Capture (or re-capture) the step graph for the kernel families `fam`: the
+// init kernel and `iters` batched iterations.  Every kernel of the graph is
+// first launched once on an all-idle table, so nothing loads during capture
+// and no admitted request is advanced.
+cudaError_t capture_graph(ainv_server *srv, int fam) {
+  k_srv_init<<<srv->grid, kBlock, 0, srv->s>>>(srv->tab_empty_d, srv->st_d);
+  cudaError_t e = enqueue_iteration(srv->tab_empty_d, srv->st_d, srv->grid, srv->s, fam);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(srv->s);
+  if (e != cudaSuccess) return e;
+  e = cudaStreamBeginCapture(srv->s, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return e;
+  k_srv_init<<<srv->grid, kBlock, 0, srv->s>>>(srv->tab_d, srv->st_d);
+  cudaError_t ce = cudaGetLastError();
+  for (int k = 0; k < srv->iters && ce == cudaSuccess; k++)
+    ce = enqueue_iteration(srv->tab_d, srv->st_d, srv->grid, srv->s, fam);
+  cudaGraph_t g = nullptr;
+  e = cudaStreamEndCapture(srv->s, &g);
+  if (ce != cudaSuccess || e != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return ce != cudaSuccess ? ce : e;
+  }
+  cudaGraphExec_t exec = nullptr;
+  e = cudaGraphInstantiate(&exec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return e;
+  if (srv->exec) cudaGraphExecDestroy(srv->exec);
+  srv->exec = exec;
+  srv->graph_fam = fam;
+  return cudaSuccess;
+}
 
 int plan(int nslots, const int *nchunks, int grid, int *b0, int *nb) {
   if (nslots < 0 || grid < 1 || nslots > grid) {
@@ -660,6 +757,12 @@ void engine_loop(ainv_server *srv) {
                               srv->s));
       dirty = false;
     }
+    int fam;
+    {
+      std::lock_guard<std::mutex> lk(srv->mu);
+      fam = srv->fam;
+    }
+    if (fam != 0 && fam != srv->graph_fam) ENG_TRY(capture_graph(srv, fam));  // new family
     ENG_TRY(cudaGraphLaunch(srv->exec, srv->s));
     ENG_TRY(cudaMemcpyAsync(srv->st_h, srv->st_d, sizeof(SlotState) * (size_t)S,
                             cudaMemcpyDeviceToHost, srv->s));
@@ -787,30 +890,10 @@ int ainv_server_create(ainv_server **out, int max_slots, size_t hbm_bytes, int i
     e = cudaMemcpy(srv->st_d, srv->st_h, sizeof(SlotState) * (size_t)max_slots,
                    cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return fail(e, "initial table");
-  // settle every kernel once on the empty table, then capture the graph:
-  // the init kernel and `iters` batched iterations
-  k_srv_init<<<srv->grid, kBlock, 0, srv->s>>>(srv->tab_d, srv->st_d);
-  e = enqueue_iteration(srv->tab_d, srv->st_d, srv->grid, srv->s);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(srv->s);
-  if (e != cudaSuccess) return fail(e, "first launch");
-  e = cudaStreamBeginCapture(srv->s, cudaStreamCaptureModeThreadLocal);
-  if (e != cudaSuccess) return fail(e, "capture");
-  k_srv_init<<<srv->grid, kBlock, 0, srv->s>>>(srv->tab_d, srv->st_d);
-  cudaError_t ce = cudaGetLastError();
-  for (int k = 0; k < srv->iters && ce == cudaSuccess; k++)
-    ce = enqueue_iteration(srv->tab_d, srv->st_d, srv->grid, srv->s);
-  cudaGraph_t g = nullptr;
-  e = cudaStreamEndCapture(srv->s, &g);
-  if (ce != cudaSuccess || e != cudaSuccess) {
-    if (g) cudaGraphDestroy(g);
-    return fail(ce != cudaSuccess ? ce : e, "capture");
-  }
-  e = cudaGraphInstantiate(&srv->exec, g, 0);
-  cudaGraphDestroy(g);
-  if (e != cudaSuccess) {
-    srv->exec = nullptr;
-    return fail(e, "graph instantiate");
-  }
+  if ((e = cudaMalloc(&srv->tab_empty_d, sizeof(Table))) != cudaSuccess) return fail(e, "table");
+  e = cudaMemcpy(srv->tab_empty_d, srv->tab_h, sizeof(Table), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return fail(e, "empty table");
+  if ((e = capture_graph(srv, kFamStd)) != cudaSuccess) return fail(e, "graph capture");
   srv->running = true;
   srv->engine = std::thread(engine_loop, srv);
   *out = srv;
@@ -828,6 +911,7 @@ int ainv_server_add_operator(ainv_server *srv, const ainv_csr *a, const ainv_han
     return AINV_ERR_ARG;
   }
   std::lock_guard<std::mutex> lk(srv->mu);
+  srv->fam |= ainv::srv::acc64_prec(h->prec) ? ainv::srv::kFamAcc64 : ainv::srv::kFamStd;
   srv->ops.push_back(ainv::srv::Operator{a, h});
   *op = (int)srv->ops.size() - 1;
   return AINV_SUCCESS;
@@ -935,7 +1019,8 @@ int ainv_server_stats(ainv_server *srv, ainv_server_info *out) {
   out->completed = srv->completed;
   out->graph_launches = srv->launches;
   out->kernel_launches = srv->launches *
-      (1 + (long long)srv->iters * ainv::srv::kLaunchesPerIteration);
+      (1 + (long long)srv->iters *
+               (ainv::srv::kLaunchesPerIteration + (srv->graph_fam == 3 ? 4 : 0)));
   out->active = srv->active;
   out->queued = (int)srv->queue.size();
   out->peak_active = srv->peak_active;
@@ -964,6 +1049,7 @@ int ainv_server_destroy(ainv_server *srv) {
   if (srv->exec) cudaGraphExecDestroy(srv->exec);
   if (srv->arena_d) cudaFree(srv->arena_d);
   if (srv->tab_d) cudaFree(srv->tab_d);
+  if (srv->tab_empty_d) cudaFree(srv->tab_empty_d);
   if (srv->tab_h) cudaFreeHost(srv->tab_h);
   if (srv->st_d) cudaFree(srv->st_d);
   if (srv->st_h) cudaFreeHost(srv->st_h);

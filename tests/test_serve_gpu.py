@@ -172,3 +172,18 @@ def test_many_requests_stream_through_few_slots():
     assert all(r.converged for r in res) and st["peak_active"] <= 3
     for j in range(4):
         assert np.array_equal(xs[j], x_alone[j]) and res[j].iter == r_alone[j].iter
+
+
+def test_both_precision_families_in_one_server():
+    """FP32 and FP32_ACC64 operators side by side: the server re-captures its
+    graph with both kernel families, and each result still equals its solo
+    run bit for bit."""
+    ops = _operators("FP32")[:2] + _operators("FP32_ACC64")[2:]
+    reqs = _requests(ops, 8)
+    x1, r1, _ = _run(ops, reqs, max_slots=1, iters=4, alone=True)
+    x2, r2, st = _run(ops, reqs, max_slots=8, iters=4, order=list(reversed(range(8))))
+    assert st["peak_active"] > 1
+    for j, (k, b) in enumerate(reqs):
+        assert r1[j].converged and r2[j].converged
+        assert r1[j].iter == r2[j].iter and np.array_equal(x1[j], x2[j]), j
+        assert _true_relres(ops[k]["csr"], x2[j], b) <= 1.05 * EPS
