@@ -105,7 +105,10 @@ int ainv_gpu_apply(ainv_handle *h, char trans, double alpha, const double *x_dev
  * t left by the last stage 1 on this handle (x is ignored in stage 2). */
 int ainv_gpu_apply_stage(ainv_handle *h, char trans, int stage, double alpha,
                          const double *x_dev, double beta, double *y_dev, void *stream);
-/* Same on host arrays: copies x in and y out (pinned staging owned by h). */
+/* Same on host arrays: copies x (and y when beta != 0) in, y out, and
+ * returns when y is written.  Device staging is owned by h.  With page-locked
+ * x and y (cudaHostAlloc / cudaHostRegister) the copies run chunk by chunk on
+ * streams of h and overlap the sweeps; pageable arrays are copied whole. */
 int ainv_gpu_apply_host(ainv_handle *h, char trans, double alpha, const double *x,
                         double beta, double *y);
 int ainv_gpu_destroy(ainv_handle *h);

@@ -30,6 +30,16 @@ def _stream(s):
     return C.c_void_p(getattr(s, "cuda_stream", s))
 
 
+def _torch():
+    import torch
+    return torch
+
+
+def _is_cpu_tensor(a) -> bool:
+    t = type(a)
+    return t.__module__.startswith("torch") and t.__name__ == "Tensor" and a.device.type == "cpu"
+
+
 class DeviceFactors:
     """W^T (lower CSR), Z (upper CSR) and D^-1 uploaded to the device layout."""
 
@@ -79,7 +89,22 @@ class DeviceFactors:
         check(lib().ainv_gpu_update_a(self._h, dptr(x), dptr(d_out) if d_out is not None else None,
                                       _stream(stream)))
 
-    def apply_host(self, x, alpha=1.0, beta=0.0, y=None, trans="N") -> np.ndarray:
+    def apply_host(self, x, alpha=1.0, beta=0.0, y=None, trans="N"):
+        """y = alpha*op(M) x + beta*y on host arrays (the array form of the
+        apply).  x and y are numpy arrays (a new y is returned) or contiguous
+        float64 CPU torch tensors (y written in place and returned).  With
+        page-locked tensors (``tensor.pin_memory()``) the copies overlap the
+        sweeps chunk by chunk."""
+        if _is_cpu_tensor(x):
+            if y is None or not _is_cpu_tensor(y):
+                raise ValueError("apply_host: y must be a CPU tensor when x is one")
+            for v in (x, y):
+                if v.dtype != _torch().float64 or not v.is_contiguous() or v.numel() != self.n:
+                    raise ValueError("apply_host: tensors must be contiguous float64 of n entries")
+            check(lib().ainv_gpu_apply_host(self._h, trans.encode()[:1], alpha,
+                                            C.c_void_p(x.data_ptr()), beta,
+                                            C.c_void_p(y.data_ptr())))
+            return y
         x = _np(x, np.float64)
         y = np.zeros_like(x) if y is None else _np(y, np.float64).copy()
         check(lib().ainv_gpu_apply_host(self._h, trans.encode()[:1], alpha,

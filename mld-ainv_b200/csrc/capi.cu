@@ -2,8 +2,11 @@
 // device operator A.  The Krylov loop lives in krylov.cu.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <new>
+#include <vector>
 
 #include "internal.h"
 
@@ -27,7 +30,180 @@ void destroy_handle(ainv_handle *h) {
   if (h->xs) cudaFree(h->xs);
   if (h->ys) cudaFree(h->ys);
   if (h->status) cudaFree(h->status);
+  for (cudaStream_t st : h->hs)
+    if (st) cudaStreamDestroy(st);
+  for (cudaEvent_t e : h->hev) cudaEventDestroy(e);
   delete h;
+}
+
+// ---- host-array apply, pipelined over row chunks ----------------------------
+// With page-locked x and y the copies run on their own streams and overlap
+// the sweeps: chunk j of x is copied in while earlier chunks are swept, and
+// rows of y are copied out as soon as their second sweep is done.  PCIe
+// carries both directions at once, so a large apply costs about one copy of
+// x instead of two copies plus the sweeps.  Sweep 1 over chunk c waits for
+// the input chunks up to the one holding the largest column its rows read
+// (W^T and Z^T are lower triangular: chunk c itself).  Sweep 2 (Z or W,
+// upper triangular) is split per chunk into the rows whose columns stay in
+// the chunk, finished as soon as the chunk is in, and the remaining rows
+// (the band reaching into later chunks).  Chunks ramp up from 1/8 of the
+// nominal size at the start and back down at the end, which shortens the
+// wait before the first copy out and the tail after the last copy in.  The
+// arithmetic per row is that of the whole-vector sweeps.
+
+// Nominal slices per chunk: about n/16 rows and at least 128K rows (1 MB per
+// copy), a multiple of 4 slices.  AINV_HOST_CHUNK_ROWS sets the rows instead.
+int host_chunk_slices(int n) {
+  long long rows = std::max<long long>(131072, ((long long)n + 15) / 16);
+  if (const char *e = std::getenv("AINV_HOST_CHUNK_ROWS")) {
+    const long long v = std::atoll(e);
+    if (v > 0) rows = v;
+  }
+  const long long sl = ((rows + ainv::kSlice - 1) / ainv::kSlice + 3) / 4 * 4;
+  return (int)std::min<long long>(sl, 1 << 28);
+}
+
+bool page_locked(const void *p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+// Chunk bounds over ns slices: ramp cs/8, cs/4, cs/2, then chunks of about
+// cs, then the ramp reversed; plain chunks of about cs when ns is too small.
+std::vector<int> chunk_bounds(int ns, int cs) {
+  auto r4 = [](long long v) { return (int)std::max<long long>(4, v / 4 * 4); };
+  std::vector<int> ramp;
+  for (int r = cs / 8; r < cs && r >= 4; r *= 2) ramp.push_back(r4(r));
+  long long rs = 0;
+  for (int r : ramp) rs += 2LL * r;
+  if (ns < rs + 2LL * cs) {
+    ramp.clear();
+    rs = 0;
+  }
+  // sizes over ns rounded up to 4 slices, so every bound but the last one is
+  // a multiple of 4; the last chunk ends at ns
+  std::vector<int> sizes(ramp.begin(), ramp.end());
+  const long long mid = (ns + 3LL) / 4 * 4 - rs;
+  const long long cm = std::max<long long>(1, (mid + cs - 1) / cs);
+  const int each = r4((mid + cm - 1) / cm + 3);
+  for (long long left = mid; left > 0;) {
+    const int sz = (int)std::min<long long>(each, left);
+    sizes.push_back(sz);
+    left -= sz;
+  }
+  sizes.insert(sizes.end(), ramp.rbegin(), ramp.rend());
+  std::vector<int> bound(1, 0);
+  for (int sz : sizes) bound.push_back(bound.back() + sz);
+  bound.back() = ns;
+  return bound;
+}
+
+// Chunk holding slice s.
+int chunk_of(const std::vector<int> &bound, int s) {
+  return (int)(std::upper_bound(bound.begin(), bound.end(), s) - bound.begin()) - 1;
+}
+
+// Last input chunk read by the rows of slices [s0, s1) of m (-1: none).
+int needs(const DevSell &m, const std::vector<int> &bound, int s0, int s1) {
+  int mc = -1;
+  for (int s = s0; s < s1; s++) mc = std::max(mc, m.slice_maxcol[(size_t)s]);
+  return mc < 0 ? -1 : chunk_of(bound, mc / ainv::kSlice);
+}
+
+void make_plan(const DevSell &m1, const DevSell &m2, int cs, ainv::HostPlan &p) {
+  p = ainv::HostPlan{};
+  p.cs = cs;
+  p.bound = chunk_bounds(m1.nslices, cs);
+  const int C = (int)p.bound.size() - 1;
+  for (int c = 0; c < C; c++) {
+    const int b0 = p.bound[(size_t)c], b1 = p.bound[(size_t)c + 1];
+    p.need1.push_back(needs(m1, p.bound, b0, b1));
+    // leading slices (a multiple of 4) whose rows read t of chunks <= c only
+    const long long end_row = (long long)b1 * ainv::kSlice;
+    int q = b0;
+    while (q < b1 && m2.slice_maxcol[(size_t)q] < end_row) q++;
+    q = std::max(b0, q / 4 * 4);
+    for (int part = 0; part < 2; part++) {
+      const int lo = part == 0 ? b0 : q, hi = part == 0 ? q : b1;
+      if (lo == hi) continue;
+      p.u0.push_back(lo);
+      p.u1.push_back(hi);
+      p.need2.push_back(needs(m2, p.bound, lo, hi));
+    }
+  }
+}
+
+int apply_host_chunked(ainv_handle *h, bool tr, int cs, double alpha, const double *x,
+                       double beta, double *y) {
+  const DevSell &m1 = tr ? h->zt : h->wt, &m2 = tr ? h->w : h->z;
+  ainv::HostPlan &p = h->hplan[tr];
+  if (p.cs != cs) make_plan(m1, m2, cs, p);
+  const int C = (int)p.bound.size() - 1, U = (int)p.u0.size();
+  for (cudaStream_t &st : h->hs)
+    if (!st) AINV_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  while ((int)h->hev.size() < 1 + C + U) {
+    cudaEvent_t e;
+    AINV_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    h->hev.push_back(e);
+  }
+  cudaStream_t si = h->hs[0], sc = h->hs[1], so = h->hs[2];
+  cudaEvent_t e0 = h->hev[0], *ein = &h->hev[1], *eout = &h->hev[1 + (size_t)C];
+  const size_t n = (size_t)h->n;
+  auto span = [&](int s0, int s1, size_t &r0, size_t &nb) {
+    r0 = (size_t)s0 * ainv::kSlice;
+    nb = sizeof(double) * (std::min(n, (size_t)s1 * ainv::kSlice) - r0);
+  };
+  int rc = AINV_SUCCESS;
+  auto cuda = [&](cudaError_t e, const char *what) {
+    if (rc == AINV_SUCCESS && e != cudaSuccess) {
+      ainv::set_error("host apply: %s failed: %s", what, cudaGetErrorString(e));
+      rc = AINV_ERR_CUDA;
+    }
+    return rc == AINV_SUCCESS;
+  };
+  // ordered after earlier work on the legacy stream, as the serial form is
+  bool ok = cuda(cudaEventRecord(e0, 0), "event record") &&
+            cuda(cudaStreamWaitEvent(si, e0, 0), "stream wait") &&
+            cuda(cudaStreamWaitEvent(sc, e0, 0), "stream wait") &&
+            cuda(cudaStreamWaitEvent(so, e0, 0), "stream wait");
+  for (int c = 0; ok && c < C; c++) {
+    size_t r0, nb;
+    span(p.bound[(size_t)c], p.bound[(size_t)c + 1], r0, nb);
+    ok = cuda(cudaMemcpyAsync(h->xs + r0, x + r0, nb, cudaMemcpyHostToDevice, si), "copy in");
+    if (ok && beta != 0.0)
+      ok = cuda(cudaMemcpyAsync(h->ys + r0, y + r0, nb, cudaMemcpyHostToDevice, si), "copy in");
+    ok = ok && cuda(cudaEventRecord(ein[c], si), "event record");
+  }
+  for (int i = 0, u = 0; ok && i < C; i++) {
+    const int need = p.need1[(size_t)i];
+    if (need >= 0) ok = cuda(cudaStreamWaitEvent(sc, ein[need], 0), "stream wait");
+    if (ok) {
+      rc = ainv::launch_sweep_dscale_slices(m1, h->d, h->xs, h->t, p.bound[(size_t)i],
+                                            p.bound[(size_t)i + 1], sc);
+      ok = rc == AINV_SUCCESS;
+    }
+    for (; ok && u < U && p.need2[(size_t)u] <= i; u++) {
+      const int a = p.u0[(size_t)u], b = p.u1[(size_t)u];
+      // the y rows of a unit (inside one chunk) came in with that chunk
+      if (beta != 0.0) ok = cuda(cudaStreamWaitEvent(sc, ein[chunk_of(p.bound, a)], 0), "stream wait");
+      if (ok) {
+        rc = ainv::launch_sweep_axpby_slices(m2, h->t, alpha, beta, h->ys, a, b, sc);
+        ok = rc == AINV_SUCCESS;
+      }
+      size_t r0, nb;
+      span(a, b, r0, nb);
+      ok = ok && cuda(cudaEventRecord(eout[u], sc), "event record") &&
+           cuda(cudaStreamWaitEvent(so, eout[u], 0), "stream wait") &&
+           cuda(cudaMemcpyAsync(y + r0, h->ys + r0, nb, cudaMemcpyDeviceToHost, so), "copy out");
+    }
+  }
+  // every copy touching the caller's arrays is done before returning
+  for (cudaStream_t st : {si, sc, so}) cuda(cudaStreamSynchronize(st), "synchronize");
+  return rc;
 }
 
 int check_unit_triangle(const HostCsr &m, bool lower, const char *what) {
@@ -141,6 +317,11 @@ int ainv_gpu_apply_host(ainv_handle *h, char trans, double alpha, const double *
     AINV_CUDA_TRY(cudaMalloc(&h->xs, bytes));
     AINV_CUDA_TRY(cudaMalloc(&h->ys, bytes));
   }
+  const bool tr = (trans == 'T' || trans == 't' || trans == 'C' || trans == 'c');
+  const int cs = host_chunk_slices(h->n);
+  if ((tr || trans == 'N' || trans == 'n') && h->wt.nslices > cs && page_locked(x) &&
+      page_locked(y))
+    return apply_host_chunked(h, tr, cs, alpha, x, beta, y);
   AINV_CUDA_TRY(cudaMemcpyAsync(h->xs, x, bytes, cudaMemcpyHostToDevice, 0));
   if (beta != 0.0) AINV_CUDA_TRY(cudaMemcpyAsync(h->ys, y, bytes, cudaMemcpyHostToDevice, 0));
   AINV_TRY(ainv_gpu_apply(h, trans, alpha, h->xs, beta, h->ys, nullptr));

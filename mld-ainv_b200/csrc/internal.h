@@ -106,6 +106,9 @@ struct DevSell {
   int stage_slices = 0;
   int stage_vmax = 0, stage_imax = 0, stage_noff_max = 0;
   StageDesc *stages = nullptr;
+  // host copy: the largest column each slice reads (-1 for an empty slice);
+  // a sweep over rows of a slice range needs its input only up to there
+  std::vector<int> slice_maxcol;
   size_t bytes() const;
 };
 
@@ -127,6 +130,17 @@ void destroy_mws(MrhsWs *w);
 unsigned long long next_serial();
 }  // namespace ainv
 
+namespace ainv {
+// Schedule of the host-array apply pipeline for one trans.  Chunk c of the
+// vectors is slices [bound[c], bound[c+1]); sweep 1 of chunk c reads input
+// chunks up to need1[c].  Sweep 2 and the copy out run in units: unit u is
+// slices [u0[u], u1[u]) and reads t up to chunk need2[u].
+struct HostPlan {
+  int cs = 0;  // nominal slices per chunk the plan was made for
+  std::vector<int> bound, need1, u0, u1, need2;
+};
+}  // namespace ainv
+
 // ------------------------------------------------------------- handles --
 struct ainv_handle {
   unsigned long long serial = 0;
@@ -141,6 +155,11 @@ struct ainv_handle {
   double *xs = nullptr;   // device staging for the host-array apply
   double *ys = nullptr;
   int *status = nullptr;  // device word: nonzero after a streaming wait timed out
+  // host-array apply pipeline: copy-in, sweep and copy-out streams, events,
+  // and the schedule for 'N' and 'T'
+  cudaStream_t hs[3] = {nullptr, nullptr, nullptr};
+  std::vector<cudaEvent_t> hev;
+  ainv::HostPlan hplan[2];
 };
 
 struct ainv_csr {
@@ -161,6 +180,12 @@ int launch_sweep_dscale(const DevSell &m, const void *d, const double *x, void *
 int launch_sweep_axpby(const DevSell &m, const void *t, double alpha, double beta,
                        double *y, cudaStream_t s, const int *stop = nullptr,
                        int *status = nullptr);
+// The same two sweeps over the rows of slices [s0, s1) only (register path;
+// s0 a multiple of 4).  Rows outside the range are neither read nor written.
+int launch_sweep_dscale_slices(const DevSell &m, const void *d, const double *x, void *t,
+                               int s0, int s1, cudaStream_t s);
+int launch_sweep_axpby_slices(const DevSell &m, const void *t, double alpha, double beta,
+                              double *y, int s0, int s1, cudaStream_t s);
 // y = alpha * A x + beta * y with an FP64 operator.
 int launch_spmv(const DevSell &a, double alpha, const double *x, double beta,
                 double *y, cudaStream_t s, int *status = nullptr);

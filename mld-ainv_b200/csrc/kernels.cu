@@ -48,6 +48,28 @@ __global__ void __launch_bounds__(kBlock)
   });
 }
 
+// Slice-range forms: groups [g0, g1) of S slices (the host-array pipeline).
+template <class V, class T, int S, int P>
+__global__ void __launch_bounds__(kBlock)
+    k_sweep_dscale_range(SellView<V> m, const double *__restrict__ x, const V *__restrict__ d,
+                         T *__restrict__ t, int g0, int g1) {
+  for_each_row<S, P>(
+      m, x, [&](int row, auto acc) { t[row] = (T)(ldd(d + row) * acc); }, g0, g1);
+}
+
+template <class V, class T, int S, int P>
+__global__ void __launch_bounds__(kBlock)
+    k_sweep_axpby_range(SellView<V> m, const T *__restrict__ t, double alpha, double beta,
+                        double *__restrict__ y, int g0, int g1) {
+  for_each_row<S, P>(
+      m, t,
+      [&](int row, auto acc) {
+        const double r = alpha * (double)acc;
+        y[row] = (beta == 0.0) ? r : r + beta * y[row];
+      },
+      g0, g1);
+}
+
 // ---- streaming variants (stream.cuh) ----------------------------------------
 template <class V>
 __device__ __forceinline__ typename Acc<V>::type to_acc(V v) { return v; }
@@ -270,6 +292,38 @@ struct AxpbyLaunch {
   }
 };
 
+template <class V, class T>
+struct DscaleRangeLaunch {
+  const DevSell &m;
+  const void *d;
+  const double *x;
+  void *t;
+  int s0, s1;
+  cudaStream_t s;
+  template <int S, int P>
+  void run() const {
+    const int g0 = s0 / S, g1 = (s1 + S - 1) / S;
+    k_sweep_dscale_range<V, T, S, P><<<grid_for(g1 - g0), kBlock, 0, s>>>(
+        view<V>(m), x, (const V *)d, (T *)t, g0, g1);
+  }
+};
+
+template <class V, class T>
+struct AxpbyRangeLaunch {
+  const DevSell &m;
+  const void *t;
+  double alpha, beta;
+  double *y;
+  int s0, s1;
+  cudaStream_t s;
+  template <int S, int P>
+  void run() const {
+    const int g0 = s0 / S, g1 = (s1 + S - 1) / S;
+    k_sweep_axpby_range<V, T, S, P><<<grid_for(g1 - g0), kBlock, 0, s>>>(
+        view<V>(m), (const T *)t, alpha, beta, y, g0, g1);
+  }
+};
+
 // The epilogue's row vectors as seen from the host (same rule as row_vecs()).
 template <class V, class T>
 RowVecs host_row_vecs(const EpiDscale<V, T> &e) {
@@ -367,6 +421,62 @@ int launch_sweep_axpby(const DevSell &m, const void *t, double alpha, double bet
       return AINV_ERR_ARG;
   }
   return check_launch("sweep_axpby");
+}
+
+namespace {
+// Storage type V and intermediate type T of a precision, as a tag.
+template <class V_, class T_>
+struct Types {
+  using V = V_;
+  using T = T_;
+};
+template <class F>
+int by_prec(int prec, F &&f) {
+  switch (prec) {
+    case AINV_PREC_FP64: f(Types<double, double>()); break;
+    case AINV_PREC_FP32: f(Types<float, float>()); break;
+    case AINV_PREC_BF16: f(Types<__nv_bfloat16, float>()); break;
+    case AINV_PREC_FP32_ACC64: f(Types<f32w, double>()); break;
+    case AINV_PREC_BF16_ACC64: f(Types<b16w, double>()); break;
+    default:
+      set_error("unknown precision %d", prec);
+      return AINV_ERR_ARG;
+  }
+  return AINV_SUCCESS;
+}
+
+int check_range(const DevSell &m, int s0, int s1) {
+  if (s0 < 0 || s1 > m.nslices || s0 > s1 || (s0 & 3) != 0) {
+    set_error("slice range [%d, %d) invalid for %d slices", s0, s1, m.nslices);
+    return AINV_ERR_ARG;
+  }
+  return AINV_SUCCESS;
+}
+}  // namespace
+
+int launch_sweep_dscale_slices(const DevSell &m, const void *d, const double *x, void *t,
+                               int s0, int s1, cudaStream_t s) {
+  AINV_TRY(check_range(m, s0, s1));
+  if (s0 == s1) return AINV_SUCCESS;
+  AINV_TRY(by_prec(m.prec, [&](auto ty) {
+    using V = typename decltype(ty)::V;
+    using T = typename decltype(ty)::T;
+    with_group_pack<V>(group_size(m.prec), m.pack, DscaleRangeLaunch<V, T>{m, d, x, t, s0, s1, s});
+  }));
+  return check_launch("sweep_dscale (slices)");
+}
+
+int launch_sweep_axpby_slices(const DevSell &m, const void *t, double alpha, double beta,
+                              double *y, int s0, int s1, cudaStream_t s) {
+  AINV_TRY(check_range(m, s0, s1));
+  if (s0 == s1) return AINV_SUCCESS;
+  AINV_TRY(by_prec(m.prec, [&](auto ty) {
+    using V = typename decltype(ty)::V;
+    using T = typename decltype(ty)::T;
+    with_group_pack<V>(group_size(m.prec), m.pack,
+                       AxpbyRangeLaunch<V, T>{m, t, alpha, beta, y, s0, s1, s});
+  }));
+  return check_launch("sweep_axpby (slices)");
 }
 
 int launch_spmv(const DevSell &a, double alpha, const double *x, double beta, double *y,

@@ -139,6 +139,7 @@ int upload_sell_t(const HostCsr &a, int prec, DevSell &out) {
   std::vector<int> offs_ptr((size_t)ns + 1, 0);
   std::vector<int> offs_all;
   std::vector<int> offs;
+  std::vector<int> maxcol((size_t)ns, -1);
   long long base_slots = 0;
   for (int s = 0; s < ns; s++) {
     const int r0 = s * kSlice, r1 = std::min(n, r0 + kSlice);
@@ -146,7 +147,10 @@ int upload_sell_t(const HostCsr &a, int prec, DevSell &out) {
     offs.clear();
     for (int r = r0; r < r1; r++) {
       w = std::max(w, a.irp[r + 1] - a.irp[r]);
-      for (int k = a.irp[r]; k < a.irp[r + 1]; k++) offs.push_back(a.ja[k] - r);
+      for (int k = a.irp[r]; k < a.irp[r + 1]; k++) {
+        offs.push_back(a.ja[k] - r);
+        maxcol[(size_t)s] = std::max(maxcol[(size_t)s], a.ja[k]);
+      }
     }
     std::sort(offs.begin(), offs.end());
     offs.erase(std::unique(offs.begin(), offs.end()), offs.end());
@@ -233,6 +237,7 @@ int upload_sell_t(const HostCsr &a, int prec, DevSell &out) {
   m.offset_slices = offset_slices;
   m.pack = P;
   m.prec = prec;
+  m.slice_maxcol = std::move(maxcol);
   // streaming stages: kConsumerSlices warps, each with 8/sizeof(V) slices,
   // so a warp's share of a stage is about 1 KB of values at every precision
   std::vector<StageDesc> stages;

@@ -377,13 +377,14 @@ __device__ __forceinline__ void group_dot(const SellView<V> &m, const GroupCtx<S
 }
 
 // Visit every row of M: epi(row, acc) for rows < n, S slices per warp step,
-// warps striding over the grid.
+// warps striding over the grid.  [g0, g1) restricts the walk to those groups
+// of S slices (rows stay absolute).
 template <int S, int P, int K = 4, class V, class X, class Epi>
 __device__ __forceinline__ void for_each_row(const SellView<V> &m, const X *__restrict__ x,
-                                             Epi &&epi) {
-  const int ngroups = (m.nslices + S - 1) / S;
+                                             Epi &&epi, int g0 = 0, int g1 = 0x7fffffff) {
+  const int ngroups = min((m.nslices + S - 1) / S, g1);
   const int lane = threadIdx.x & 31;
-  for (int g = first_slice(); g < ngroups; g += slice_stride()) {
+  for (int g = g0 + first_slice(); g < ngroups; g += slice_stride()) {
     GroupCtx<S> c;
     group_ctx(m, g, c);
     typename Acc<V>::type acc[S];

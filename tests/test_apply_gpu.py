@@ -249,3 +249,69 @@ def test_stencil_factors_use_offset_mode():
         assert lay["offset_slices"] == lay["nslices"]
         assert lay["nidx"] <= 8 * lay["nslices"]          # a few offsets per slice
         assert lay["slots"] <= 1.02 * 4 * 64000 + 32 * 4   # ~4 slots per row
+
+
+def _scattered_factors(n, per_row=5, seed=11):
+    """Unit triangular W^T (lower) and Z (upper) whose off-diagonal entries sit
+    anywhere in their triangle: every chunk of the host-array pipeline then
+    depends on far-away chunks."""
+    rng = np.random.default_rng(seed)
+
+    def tri(lower):
+        irp, ja, va = [0], [], []
+        for i in range(n):
+            lo, hi = (0, i) if lower else (i + 1, n)
+            cols = rng.integers(lo, hi, per_row) if hi > lo else np.zeros(0, np.int64)
+            cols = np.unique(np.append(cols, i))
+            ja.extend(cols.tolist())
+            va.extend(np.where(cols == i, 1.0, rng.uniform(-0.3, 0.3, len(cols))).tolist())
+            irp.append(len(ja))
+        return np.array(irp, np.int32), np.array(ja, np.int32), np.array(va)
+
+    wt, z = tri(True), tri(False)
+    return dict(wt_irp=wt[0], wt_ja=wt[1], wt_val=wt[2], z_irp=z[0], z_ja=z[1], z_val=z[2],
+                d=rng.uniform(0.5, 2.0, n))
+
+
+@pytest.mark.parametrize("kind", ["stencil", "scattered"])
+def test_pipelined_host_apply_equals_device_form(kind, monkeypatch):
+    """Page-locked host arrays go through the chunked pipeline (copies on their
+    own streams, sweeps over slice ranges); FP64 results are bit-identical to
+    the device-array apply for both trans and beta = 0 / != 0."""
+    if kind == "stencil":
+        irp, ja, val = ainv.pde.gen_pde3d(22, "convdiff", (4.0, -5.0, 6.0))
+        f = build_factors(irp, ja, val)
+    else:
+        f = _scattered_factors(9000)
+    n = len(f["d"])
+    df = device_factors(f)
+    x, y0 = ainv.pde.rand_uniform(17, n), ainv.pde.rand_uniform(18, n)
+    # nominal chunks of 512 rows (ramped: 29 chunks at 22^3), 1024 and 4000 rows
+    for rows in ("512", "1024", "4000"):
+        monkeypatch.setenv("AINV_HOST_CHUNK_ROWS", rows)
+        for trans in "NT":
+            for alpha, beta in ((1.0, 0.0), (2.0, -0.75)):
+                xp = torch.from_numpy(x.copy()).pin_memory()
+                yp = torch.from_numpy(y0.copy()).pin_memory()
+                df.apply_host(xp, alpha, beta, yp, trans)
+                yd = _gpu_apply(df, x, alpha, beta, y0, trans)
+                np.testing.assert_array_equal(yp.numpy(), yd, err_msg=f"{rows} {trans} {beta}")
+                # the pageable form takes the serial path: same numbers
+                np.testing.assert_array_equal(df.apply_host(x, alpha, beta, y0, trans), yd)
+
+
+@pytest.mark.parametrize("prec", ["FP32", "BF16", "FP32_ACC64", "BF16_ACC64"])
+def test_pipelined_host_apply_reduced_precision(prec, monkeypatch):
+    irp, ja, val = ainv.pde.gen_pde3d(20, "convdiff", (1.0, 2.0, 3.0))
+    f = build_factors(irp, ja, val)
+    n = len(f["d"])
+    df = device_factors(f, prec)
+    x, y0 = ainv.pde.rand_uniform(21, n), ainv.pde.rand_uniform(22, n)
+    monkeypatch.setenv("AINV_HOST_CHUNK_ROWS", "640")
+    tol = {"FP32": 5e-6, "BF16": 3e-2, "FP32_ACC64": 5e-6, "BF16_ACC64": 3e-2}[prec]
+    for trans in "NT":
+        xp = torch.from_numpy(x.copy()).pin_memory()
+        yp = torch.from_numpy(y0.copy()).pin_memory()
+        df.apply_host(xp, 1.5, 0.5, yp, trans)
+        ref = O.ainv_apply(oracle_factors(f), x, 1.5, 0.5, y0, trans)
+        assert relerr(yp.numpy(), ref) <= tol, (prec, trans)
