@@ -30,6 +30,7 @@ void destroy_handle(ainv_handle *h) {
   if (h->xs) cudaFree(h->xs);
   if (h->ys) cudaFree(h->ys);
   if (h->status) cudaFree(h->status);
+  ainv::destroy_host_pipe(h->pipe);
   for (cudaStream_t st : h->hs)
     if (st) cudaStreamDestroy(st);
   for (cudaEvent_t e : h->hev) cudaEventDestroy(e);
@@ -37,24 +38,36 @@ void destroy_handle(ainv_handle *h) {
 }
 
 // ---- host-array apply, pipelined over row chunks ----------------------------
-// With page-locked x and y the copies run on their own streams and overlap
-// the sweeps: chunk j of x is copied in while earlier chunks are swept, and
-// rows of y are copied out as soon as their second sweep is done.  PCIe
-// carries both directions at once, so a large apply costs about one copy of
-// x instead of two copies plus the sweeps.  Sweep 1 over chunk c waits for
-// the input chunks up to the one holding the largest column its rows read
-// (W^T and Z^T are lower triangular: chunk c itself).  Sweep 2 (Z or W,
-// upper triangular) is split per chunk into the rows whose columns stay in
-// the chunk, finished as soon as the chunk is in, and the remaining rows
-// (the band reaching into later chunks).  Chunks ramp up from 1/8 of the
-// nominal size at the start and back down at the end, which shortens the
-// wait before the first copy out and the tail after the last copy in.  The
-// arithmetic per row is that of the whole-vector sweeps.
+// With page-locked x and y the copies overlap the sweeps chunk by chunk:
+// chunk j of x is copied in while earlier chunks are swept, and rows of y
+// go out as soon as their second sweep is done.  PCIe carries both
+// directions at once, so a large apply costs little more than one transfer
+// of x.  Sweep 1 over chunk c needs the input chunks up to the one holding
+// the largest column its rows read (W^T and Z^T are lower triangular: chunk
+// c itself).  Sweep 2 (Z or W, upper triangular) is split per chunk into the
+// rows whose columns stay in the chunk, finished as soon as the chunk is in,
+// and the remaining rows (the band reaching into later chunks).  Chunks ramp
+// up from 1/8 of the nominal size at the start and back down at the end,
+// which shortens the wait before the first rows of y and the tail after the
+// last chunk of x.  Two forms run this schedule:
+//  * fused (hostpipe.cu): copies of x plus one persistent kernel that polls
+//    per-chunk flags and writes y straight into the caller's array;
+//  * streams (below, when the two sweeps differ in pack width or y is not
+//    device-mapped): per-chunk kernels and copies on three streams linked by
+//    events.  Under PCIe load each event wait takes tens of microseconds to
+//    resolve, which makes this form slower.
+// The arithmetic per row is that of the whole-vector sweeps.
 
-// Nominal slices per chunk: about n/16 rows and at least 128K rows (1 MB per
+// Events of the stream pipeline: [0] orders it after the legacy stream; then
+// one per chunk copied in and one per unit swept.
+constexpr int kPipeEvents = 1;
+
+// Nominal slices per chunk: about n/8 rows and at least 128K rows (1 MB per
 // copy), a multiple of 4 slices.  AINV_HOST_CHUNK_ROWS sets the rows instead.
+// (At n = 8M: 13 chunks after the ramps.  Each chunk costs about 20-30 us
+// of PCIe time under bidirectional load; n/16 and n/4 measured slower.)
 int host_chunk_slices(int n) {
-  long long rows = std::max<long long>(131072, ((long long)n + 15) / 16);
+  long long rows = std::max<long long>(131072, ((long long)n + 7) / 8);
   if (const char *e = std::getenv("AINV_HOST_CHUNK_ROWS")) {
     const long long v = std::atoll(e);
     if (v > 0) rows = v;
@@ -137,21 +150,15 @@ void make_plan(const DevSell &m1, const DevSell &m2, int cs, ainv::HostPlan &p) 
   }
 }
 
-int apply_host_chunked(ainv_handle *h, bool tr, int cs, double alpha, const double *x,
-                       double beta, double *y) {
+// Enqueue the pipeline on si (copies in), sc (sweeps) and so (copies out);
+// the three streams must already be ordered after whatever comes before.
+int enqueue_pipeline(ainv_handle *h, bool tr, double alpha, const double *x, double beta,
+                     double *y) {
   const DevSell &m1 = tr ? h->zt : h->wt, &m2 = tr ? h->w : h->z;
-  ainv::HostPlan &p = h->hplan[tr];
-  if (p.cs != cs) make_plan(m1, m2, cs, p);
+  const ainv::HostPlan &p = h->hplan[tr];
   const int C = (int)p.bound.size() - 1, U = (int)p.u0.size();
-  for (cudaStream_t &st : h->hs)
-    if (!st) AINV_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-  while ((int)h->hev.size() < 1 + C + U) {
-    cudaEvent_t e;
-    AINV_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    h->hev.push_back(e);
-  }
   cudaStream_t si = h->hs[0], sc = h->hs[1], so = h->hs[2];
-  cudaEvent_t e0 = h->hev[0], *ein = &h->hev[1], *eout = &h->hev[1 + (size_t)C];
+  cudaEvent_t *ein = &h->hev[kPipeEvents], *eout = ein + C;
   const size_t n = (size_t)h->n;
   auto span = [&](int s0, int s1, size_t &r0, size_t &nb) {
     r0 = (size_t)s0 * ainv::kSlice;
@@ -165,11 +172,7 @@ int apply_host_chunked(ainv_handle *h, bool tr, int cs, double alpha, const doub
     }
     return rc == AINV_SUCCESS;
   };
-  // ordered after earlier work on the legacy stream, as the serial form is
-  bool ok = cuda(cudaEventRecord(e0, 0), "event record") &&
-            cuda(cudaStreamWaitEvent(si, e0, 0), "stream wait") &&
-            cuda(cudaStreamWaitEvent(sc, e0, 0), "stream wait") &&
-            cuda(cudaStreamWaitEvent(so, e0, 0), "stream wait");
+  bool ok = true;
   for (int c = 0; ok && c < C; c++) {
     size_t r0, nb;
     span(p.bound[(size_t)c], p.bound[(size_t)c + 1], r0, nb);
@@ -201,8 +204,37 @@ int apply_host_chunked(ainv_handle *h, bool tr, int cs, double alpha, const doub
            cuda(cudaMemcpyAsync(y + r0, h->ys + r0, nb, cudaMemcpyDeviceToHost, so), "copy out");
     }
   }
+  return rc;
+}
+
+int apply_host_chunked(ainv_handle *h, bool tr, int cs, double alpha, const double *x,
+                       double beta, double *y) {
+  ainv::HostPlan &p = h->hplan[tr];
+  if (p.cs != cs) make_plan(tr ? h->zt : h->wt, tr ? h->w : h->z, cs, p);
+  for (cudaStream_t &st : h->hs)
+    if (!st) AINV_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  const int C = (int)p.bound.size() - 1, U = (int)p.u0.size();
+  while ((int)h->hev.size() < kPipeEvents + C + U) {
+    cudaEvent_t e;
+    AINV_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    h->hev.push_back(e);
+  }
+  cudaEvent_t e0 = h->hev[0];
+  // ordered after earlier work on the legacy stream, as the serial form is
+  AINV_CUDA_TRY(cudaEventRecord(e0, 0));
+  for (cudaStream_t st : h->hs) AINV_CUDA_TRY(cudaStreamWaitEvent(st, e0, 0));
+  const bool fused = ainv::host_pipe_usable(h, tr, y);
+  int rc = fused ? ainv::host_pipe_apply(h, tr, p, alpha, x, beta, y, h->hs[0], h->hs[1])
+                 : enqueue_pipeline(h, tr, alpha, x, beta, y);
   // every copy touching the caller's arrays is done before returning
-  for (cudaStream_t st : {si, sc, so}) cuda(cudaStreamSynchronize(st), "synchronize");
+  for (cudaStream_t st : h->hs) {
+    const cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess && rc == AINV_SUCCESS) {
+      ainv::set_error("host apply: synchronize failed: %s", cudaGetErrorString(e));
+      rc = AINV_ERR_CUDA;
+    }
+  }
+  if (rc == AINV_SUCCESS && fused) rc = ainv::host_pipe_status(h);
   return rc;
 }
 

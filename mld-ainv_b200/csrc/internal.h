@@ -135,6 +135,7 @@ namespace ainv {
 // vectors is slices [bound[c], bound[c+1]); sweep 1 of chunk c reads input
 // chunks up to need1[c].  Sweep 2 and the copy out run in units: unit u is
 // slices [u0[u], u1[u]) and reads t up to chunk need2[u].
+struct HostPipe;
 struct HostPlan {
   int cs = 0;  // nominal slices per chunk the plan was made for
   std::vector<int> bound, need1, u0, u1, need2;
@@ -160,7 +161,21 @@ struct ainv_handle {
   cudaStream_t hs[3] = {nullptr, nullptr, nullptr};
   std::vector<cudaEvent_t> hev;
   ainv::HostPlan hplan[2];
+  ainv::HostPipe *pipe = nullptr;  // the persistent-kernel form of the pipeline
 };
+
+namespace ainv {
+// The host-array apply as copies of x plus one persistent kernel
+// (hostpipe.cu).  usable: the two sweeps share a pack width and y is
+// device-mapped page-locked memory.  apply enqueues on si (copies) and sc
+// (the kernel), ordered after whatever precedes them there; status reports
+// a timed-out wait of the last call, after the streams are synchronised.
+bool host_pipe_usable(const ainv_handle *h, bool tr, const double *y);
+int host_pipe_apply(ainv_handle *h, bool tr, const HostPlan &p, double alpha, const double *x,
+                    double beta, double *y, cudaStream_t si, cudaStream_t sc);
+int host_pipe_status(const ainv_handle *h);
+void destroy_host_pipe(HostPipe *hp);
+}  // namespace ainv
 
 struct ainv_csr {
   int n = 0;

@@ -277,7 +277,7 @@ struct Step { static constexpr int kPacks = P >= K ? 1 : K / P; };
 // predicated per pack (w is a multiple of P), so all value / index loads of
 // the step are in flight before the first dependent gather; the FMAs then
 // run in slot order, which is the row's column order.
-template <bool OM, int P, int K, class V, class X, int S>
+template <bool OM, int P, int K, bool NC = true, class V, class X, int S>
 __device__ __forceinline__ void group_slots(const SellView<V> &m, const GroupCtx<S> &c,
                                             const int (&row)[S], int k0,
                                             const X *__restrict__ x,
@@ -320,7 +320,7 @@ __device__ __forceinline__ void group_slots(const SellView<V> &m, const GroupCtx
 #pragma unroll
       for (int e = 0; e < P; e++)
         xv[q][j][e] = (vv[q][j][e] != A(0) && (unsigned)col[q][j][e] < (unsigned)m.n)
-                          ? (A)__ldg(x + col[q][j][e])
+                          ? (A)(NC ? __ldg(x + col[q][j][e]) : __ldcg(x + col[q][j][e]))
                           : A(0);
 #pragma unroll
   for (int q = 0; q < S; q++)
@@ -333,7 +333,7 @@ __device__ __forceinline__ void group_slots(const SellView<V> &m, const GroupCtx
 // acc[q] = row (g*S+q)*32+lane of M dotted with x.  The encoding test is
 // warp-uniform and sits outside the slot loop; a group mixing both
 // encodings is walked one slice at a time.
-template <int P, int K = 4, class V, class X, int S>
+template <int P, int K = 4, bool NC = true, class V, class X, int S>
 __device__ __forceinline__ void group_dot(const SellView<V> &m, const GroupCtx<S> &c, int g,
                                           const X *__restrict__ x,
                                           typename Acc<V>::type (&acc)[S]) {
@@ -352,9 +352,9 @@ __device__ __forceinline__ void group_dot(const SellView<V> &m, const GroupCtx<S
     }
   }
   if (all_om) {
-    for (int k0 = 0; k0 < c.maxw; k0 += KS) group_slots<true, P, K>(m, c, row, k0, x, acc);
+    for (int k0 = 0; k0 < c.maxw; k0 += KS) group_slots<true, P, K, NC>(m, c, row, k0, x, acc);
   } else if (all_col) {
-    for (int k0 = 0; k0 < c.maxw; k0 += KS) group_slots<false, P, K>(m, c, row, k0, x, acc);
+    for (int k0 = 0; k0 < c.maxw; k0 += KS) group_slots<false, P, K, NC>(m, c, row, k0, x, acc);
   } else {
 #pragma unroll
     for (int q = 0; q < S; q++) {
@@ -367,9 +367,9 @@ __device__ __forceinline__ void group_dot(const SellView<V> &m, const GroupCtx<S
       const int r1[1] = {row[q]};
       A a1[1] = {A(0)};
       if (c.om[q]) {
-        for (int k0 = 0; k0 < c1.maxw; k0 += KS) group_slots<true, P, K>(m, c1, r1, k0, x, a1);
+        for (int k0 = 0; k0 < c1.maxw; k0 += KS) group_slots<true, P, K, NC>(m, c1, r1, k0, x, a1);
       } else {
-        for (int k0 = 0; k0 < c1.maxw; k0 += KS) group_slots<false, P, K>(m, c1, r1, k0, x, a1);
+        for (int k0 = 0; k0 < c1.maxw; k0 += KS) group_slots<false, P, K, NC>(m, c1, r1, k0, x, a1);
       }
       acc[q] = a1[0];
     }

@@ -273,11 +273,14 @@ def _scattered_factors(n, per_row=5, seed=11):
                 d=rng.uniform(0.5, 2.0, n))
 
 
+@pytest.mark.parametrize("fused", ["1", "0"])
 @pytest.mark.parametrize("kind", ["stencil", "scattered"])
-def test_pipelined_host_apply_equals_device_form(kind, monkeypatch):
-    """Page-locked host arrays go through the chunked pipeline (copies on their
-    own streams, sweeps over slice ranges); FP64 results are bit-identical to
-    the device-array apply for both trans and beta = 0 / != 0."""
+def test_pipelined_host_apply_equals_device_form(kind, fused, monkeypatch):
+    """Page-locked host arrays go through the chunked pipeline: copies of x
+    with one persistent sweep kernel writing y to the host (fused), or the
+    event-driven stream form; FP64 results are bit-identical to the
+    device-array apply for both trans and beta = 0 / != 0."""
+    monkeypatch.setenv("AINV_HOST_FUSED", fused)
     if kind == "stencil":
         irp, ja, val = ainv.pde.gen_pde3d(22, "convdiff", (4.0, -5.0, 6.0))
         f = build_factors(irp, ja, val)
@@ -315,3 +318,26 @@ def test_pipelined_host_apply_reduced_precision(prec, monkeypatch):
         df.apply_host(xp, 1.5, 0.5, yp, trans)
         ref = O.ainv_apply(oracle_factors(f), x, 1.5, 0.5, y0, trans)
         assert relerr(yp.numpy(), ref) <= tol, (prec, trans)
+
+
+def test_repeated_host_apply_on_the_same_arrays(monkeypatch):
+    """The same page-locked arrays on repeated calls (the fused pipeline's
+    chunk flags carry a new epoch per call): every call reads the arrays'
+    current contents, with scalars and trans changing between calls."""
+    irp, ja, val = ainv.pde.gen_pde3d(21, "convdiff", (3.0, 1.0, -2.0))
+    f = build_factors(irp, ja, val)
+    n = len(f["d"])
+    df = device_factors(f)
+    monkeypatch.setenv("AINV_HOST_CHUNK_ROWS", "1024")
+    xp = torch.zeros(n, dtype=torch.float64).pin_memory()
+    yp = torch.zeros(n, dtype=torch.float64).pin_memory()
+    y0 = ainv.pde.rand_uniform(40, n)
+    calls = [("N", 1.0, 0.0)] * 4 + [("N", 0.5, 0.0)] * 3 + [("T", 1.0, 0.25)] * 3 + \
+            [("N", 1.0, 0.0)] * 3
+    for k, (trans, alpha, beta) in enumerate(calls):
+        x = ainv.pde.rand_uniform(100 + k, n)
+        xp.copy_(torch.from_numpy(x))
+        yp.copy_(torch.from_numpy(y0))
+        df.apply_host(xp, alpha, beta, yp, trans)
+        np.testing.assert_array_equal(yp.numpy(), _gpu_apply(df, x, alpha, beta, y0, trans),
+                                      err_msg=f"call {k}")
