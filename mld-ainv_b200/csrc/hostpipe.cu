@@ -304,8 +304,22 @@ int host_pipe_apply(ainv_handle *h, bool tr, const HostPlan &p, double alpha, co
   *hp.epoch_h = hp.epoch;
   *(volatile int *)hp.status_h = 0;
   const size_t n = (size_t)h->n;
-  // sc: reset the counters, then the kernel
+  // The copies are enqueued before the kernel: a tool that runs each kernel
+  // to completion before the host goes on (a profiler) then still finds
+  // every chunk on its way instead of a kernel waiting for copies that are
+  // not enqueued yet.
   AINV_CUDA_TRY(cudaMemsetAsync(hp.ctr, 0, sizeof(int) * (size_t)(C + 2), sc));
+  // si: the chunks of x (and y), each followed by its flag
+  for (int c = 0; c < C; c++) {
+    const size_t r0 = (size_t)p.bound[(size_t)c] * kSlice;
+    const size_t nb = sizeof(double) * (std::min(n, (size_t)p.bound[(size_t)c + 1] * kSlice) - r0);
+    AINV_CUDA_TRY(cudaMemcpyAsync(h->xs + r0, x + r0, nb, cudaMemcpyHostToDevice, si));
+    if (beta != 0.0)
+      AINV_CUDA_TRY(cudaMemcpyAsync(h->ys + r0, y + r0, nb, cudaMemcpyHostToDevice, si));
+    AINV_CUDA_TRY(cudaMemcpyAsync(hp.flags + c, hp.epoch_h, sizeof(unsigned),
+                                  cudaMemcpyHostToDevice, si));
+  }
+  // sc: the kernel, after the counters are reset
   int dev = 0, sms = 0;
   AINV_CUDA_TRY(cudaGetDevice(&dev));
   AINV_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -320,16 +334,6 @@ int host_pipe_apply(ainv_handle *h, bool tr, const HostPlan &p, double alpha, co
   });
   if (rc != AINV_SUCCESS) return rc;
   AINV_CUDA_TRY(cudaGetLastError());
-  // si: the chunks of x (and y), each followed by its flag
-  for (int c = 0; c < C; c++) {
-    const size_t r0 = (size_t)p.bound[(size_t)c] * kSlice;
-    const size_t nb = sizeof(double) * (std::min(n, (size_t)p.bound[(size_t)c + 1] * kSlice) - r0);
-    AINV_CUDA_TRY(cudaMemcpyAsync(h->xs + r0, x + r0, nb, cudaMemcpyHostToDevice, si));
-    if (beta != 0.0)
-      AINV_CUDA_TRY(cudaMemcpyAsync(h->ys + r0, y + r0, nb, cudaMemcpyHostToDevice, si));
-    AINV_CUDA_TRY(cudaMemcpyAsync(hp.flags + c, hp.epoch_h, sizeof(unsigned),
-                                  cudaMemcpyHostToDevice, si));
-  }
   return AINV_SUCCESS;
 }
 
