@@ -4,13 +4,16 @@
 // Algorithm: mld_d_ainv_bld (src/impl/mld_d_ainv_bld.F90:35-194) with the
 // maxval scaling the solver always requests (src/impl/mld_d_ainv_solver_bld.f90:68-69),
 // the left-looking biconjugation of src/impl/mld_dsparse_biconjg_llk.F90:35-366
-// (plus the SYM-LLK and no-alpha-test variants), and the column
+// (plus the SYM-LLK, no-alpha-test and stabilised STAB-LLK variants), and the column
 // sparsification of src/impl/mld_d_sparsify.f90:35-149.  Floating-point
 // operations happen in the reference's order with one rounding per
 // operation, so the factors are bit-identical to the reference algorithm.
+// (STAB-LLK also multiplies A by sparse columns of Z and W through PSBLAS
+// routines outside the reference tree; their accumulation order here is
+// documented at SparseProduct.)
 //
-// The Z and W halves of the biconjugation only share read-only data (A and
-// its transpose), so they run on two threads.
+// In LLK the Z and W halves only share read-only data (A and its
+// transpose), so they run on two threads.  STAB-LLK interleaves them.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -92,7 +95,20 @@ class HalfBuilder {
 
   // piv receives the pivots; out gets the factor as CSC columns.
   void run(double piv0, std::vector<double> &piv, HostCsr &out) {
+    start(out);
     piv.assign((size_t)n_, 0.0);
+    piv[0] = piv0;
+    for (int i = 1; i < n_; i++) {
+      update(i, piv, out, [&](int j) { return dot_with(j); });
+      double p = dot_with(i);
+      if (std::fabs(p) < kEpsTol) p = kTinyPivot;
+      piv[i] = p;
+      keep_column(i, out);
+    }
+  }
+
+  // Column 0 of the factor (e_0) and empty work state.
+  void start(HostCsr &out) {
     out.n = n_;
     out.irp.assign((size_t)n_ + 1, 0);
     out.ja.clear();
@@ -102,72 +118,65 @@ class HalfBuilder {
     work_.assign((size_t)n_, 0.0);
     in_col_.assign((size_t)n_, 0);
     queued_.assign((size_t)n_, 0);
-
-    piv[0] = piv0;
     out.ja.push_back(0);
     out.val.push_back(1.0);
     out.irp[1] = 1;
+  }
 
-    for (int i = 1; i < n_; i++) {
-      std::vector<int> nz;  // positions set in work_, in insertion order
-      work_[i] = 1.0;
-      in_col_[i] = 1;
-      nz.push_back(i);
-      MinQueue steps;
-      for (int k = touch_.irp[i]; k < touch_.irp[i + 1]; k++) {
-        const int j = touch_.ja[k];
-        if (j < i) {
-          steps.push(j);
-          queued_[j] = 1;
-        }
+  // Work column i = e_i updated by the earlier columns j < i of out whose
+  // coefficient -dot(j)/piv[j] passes the alpha test; dot(j) sees the work
+  // column through work().
+  template <class Dot>
+  void update(int i, const std::vector<double> &piv, const HostCsr &out, Dot &&dot) {
+    nz_.clear();
+    work_[i] = 1.0;
+    in_col_[i] = 1;
+    nz_.push_back(i);
+    MinQueue steps;
+    for (int k = touch_.irp[i]; k < touch_.irp[i + 1]; k++) {
+      const int j = touch_.ja[k];
+      if (j < i) {
+        steps.push(j);
+        queued_[j] = 1;
       }
-      int lastj = -1;
-      while (!steps.empty()) {
-        const int j = steps.top();
-        steps.pop();
-        if (j <= lastj) continue;  // repeated entry
-        lastj = j;
-        queued_[j] = 0;
-        if (j >= i) continue;
-        const double alpha = -dot_with(j) / piv[j];
-        if (alpha_test_ && !(std::fabs(alpha) > thresh_)) continue;
-        for (int k = out.irp[j]; k < out.irp[j + 1]; k++) {
-          const int kr = out.ja[k];
-          work_[kr] = work_[kr] + alpha * out.val[k];
-          if (!in_col_[kr]) {
-            in_col_[kr] = 1;
-            nz.push_back(kr);
-            for (int kc = touch_.irp[kr]; kc < touch_.irp[kr + 1]; kc++) {
-              const int nj = touch_.ja[kc];
-              if (!queued_[nj] && nj > j && nj < i) {
-                steps.push(nj);
-                queued_[nj] = 1;
-              }
+    }
+    int lastj = -1;
+    while (!steps.empty()) {
+      const int j = steps.top();
+      steps.pop();
+      if (j <= lastj) continue;  // repeated entry
+      lastj = j;
+      queued_[j] = 0;
+      if (j >= i) continue;
+      const double alpha = -dot(j) / piv[j];
+      if (alpha_test_ && !(std::fabs(alpha) > thresh_)) continue;
+      for (int k = out.irp[j]; k < out.irp[j + 1]; k++) {
+        const int kr = out.ja[k];
+        work_[kr] = work_[kr] + alpha * out.val[k];
+        if (!in_col_[kr]) {
+          in_col_[kr] = 1;
+          nz_.push_back(kr);
+          for (int kc = touch_.irp[kr]; kc < touch_.irp[kr + 1]; kc++) {
+            const int nj = touch_.ja[kc];
+            if (!queued_[nj] && nj > j && nj < i) {
+              steps.push(nj);
+              queued_[nj] = 1;
             }
           }
         }
       }
-      double p = dot_with(i);
-      if (std::fabs(p) < kEpsTol) p = kTinyPivot;
-      piv[i] = p;
-      keep_column(i, nz, out);
     }
   }
 
- private:
-  double dot_with(int j) const {
-    double s = 0.0;
-    for (int k = dots_.irp[j]; k < dots_.irp[j + 1]; k++) s = s + work_[dots_.ja[k]] * dots_.val[k];
-    return s;
-  }
+  const std::vector<double> &work() const { return work_; }
 
   // Diagonal plus at most cap-1 entries of largest magnitude >= thresh,
   // offered to the heap in ascending index order; survivors sorted by index.
-  void keep_column(int i, std::vector<int> &nz, HostCsr &out) {
-    std::sort(nz.begin(), nz.end());
+  void keep_column(int i, HostCsr &out) {
+    std::sort(nz_.begin(), nz_.end());
     heap_.clear();
     double diag = 0.0;
-    for (int r : nz) {
+    for (int r : nz_) {
       if (r == i)
         diag = work_[r];
       else if (std::fabs(work_[r]) >= thresh_)
@@ -194,6 +203,13 @@ class HalfBuilder {
     out.irp[(size_t)i + 1] = (int)out.ja.size();
   }
 
+ private:
+  double dot_with(int j) const {
+    double s = 0.0;
+    for (int k = dots_.irp[j]; k < dots_.irp[j + 1]; k++) s = s + work_[dots_.ja[k]] * dots_.val[k];
+    return s;
+  }
+
   const HostCsr &dots_;
   const HostCsr &touch_;
   const int n_, cap_;
@@ -201,9 +217,109 @@ class HalfBuilder {
   const bool alpha_test_;
   std::vector<double> work_;
   std::vector<char> in_col_, queued_;
+  std::vector<int> nz_;  // positions set in work_, in insertion order
   MagnitudeHeap heap_;
   std::vector<std::pair<int, double>> kept_;
 };
+
+// y = x^T M for a sparse x (an index-sorted column of Z or W) and M in CSR:
+// x's entries in order, each adding x_k * M(k, :) into a dense accumulator;
+// the result comes back sorted by index.  With M = A this is PSBLAS
+// psb_d_spvspm(done, a, x, dzero, y); with M = A^T (A's CSC arrays) it is
+// psb_d_spmspv(done, ac, x, dzero, y) = A x.  PSBLAS is not part of the
+// reference tree; this accumulation order is the restatement's own.
+class SparseProduct {
+ public:
+  explicit SparseProduct(int n) : acc_((size_t)n, 0.0), seen_((size_t)n, 0) {}
+  void run(const HostCsr &x, int col, const HostCsr &m) {
+    idx_.clear();
+    for (int k = x.irp[col]; k < x.irp[col + 1]; k++) {
+      const int r = x.ja[k];
+      const double xv = x.val[k];
+      for (int e = m.irp[r]; e < m.irp[r + 1]; e++) {
+        const int c = m.ja[e];
+        if (!seen_[c]) {
+          seen_[c] = 1;
+          acc_[c] = 0.0;
+          idx_.push_back(c);
+        }
+        acc_[c] = acc_[c] + xv * m.val[e];
+      }
+    }
+    std::sort(idx_.begin(), idx_.end());
+    val_.resize(idx_.size());
+    for (size_t m2 = 0; m2 < idx_.size(); m2++) {
+      val_[m2] = acc_[idx_[m2]];
+      seen_[idx_[m2]] = 0;
+    }
+  }
+  // psb_spge_dot: sum of y_k * w[idx_k] in index order, from zero
+  double dot_dense(const std::vector<double> &w) const {
+    double s = 0.0;
+    for (size_t m = 0; m < idx_.size(); m++) s = s + val_[m] * w[(size_t)idx_[m]];
+    return s;
+  }
+  // psb_spdot_srtd: merge with an index-sorted column of f
+  double dot_sorted(const HostCsr &f, int col) const {
+    double s = 0.0;
+    size_t a = 0;
+    int b = f.irp[col];
+    while (a < idx_.size() && b < f.irp[col + 1]) {
+      if (idx_[a] < f.ja[b]) {
+        a++;
+      } else if (idx_[a] > f.ja[b]) {
+        b++;
+      } else {
+        s = s + val_[a] * f.val[b];
+        a++;
+        b++;
+      }
+    }
+    return s;
+  }
+
+ private:
+  std::vector<double> acc_;
+  std::vector<char> seen_;
+  std::vector<int> idx_;
+  std::vector<double> val_;
+};
+
+// Stabilised left-looking biconjugation (STAB-LLK,
+// src/impl/mld_dsparse_biconjg_s_ft_llk.F90:35-414).  For each i, column i
+// of Z and then column i of W: the Z step j uses p_i = (w_j^T A) . z
+// (:164-169), the W step j uses q_i = (A z_j) . w (:297-304), both divided by
+// the common pivot of column j; the pivot of column i is then
+// (A z_i) . w_i over the kept entries (:381-389) with the 1e-3 guard
+// (:402-406).  Candidate steps come from A's columns (Z) and rows (W) as in
+// LLK.  The halves depend on each other column by column, so they run in
+// turn on one thread.
+void stab_llk(const HostCsr &a, const HostCsr &at, int cap, double thresh, double piv0,
+              std::vector<double> &piv, HostCsr &zc, HostCsr &wc) {
+  const int n = a.n;
+  HalfBuilder zb(a, at, cap, thresh, true), wb(at, a, cap, thresh, true);
+  zb.start(zc);
+  wb.start(wc);
+  piv.assign((size_t)n, 0.0);
+  piv[0] = piv0;
+  SparseProduct y(n);
+  for (int i = 1; i < n; i++) {
+    zb.update(i, piv, zc, [&](int j) {
+      y.run(wc, j, a);  // w_j^T A
+      return y.dot_dense(zb.work());
+    });
+    zb.keep_column(i, zc);
+    wb.update(i, piv, wc, [&](int j) {
+      y.run(zc, j, at);  // A z_j
+      return y.dot_dense(wb.work());
+    });
+    wb.keep_column(i, wc);
+    y.run(zc, i, at);  // A z_i
+    double q = y.dot_sorted(wc, i);
+    if (std::fabs(q) < kEpsTol) q = kTinyPivot;
+    piv[(size_t)i] = q;
+  }
+}
 
 }  // namespace
 
@@ -213,7 +329,7 @@ int ainv_biconjg_build(const HostCsr &a_in, int alg, int fill_in, double thresh,
     set_error("AINV build: fill_in must be >= 1 (got %d)", fill_in);
     return AINV_ERR_ARG;
   }
-  if (alg != kAlgLLK && alg != kAlgSymLLK && alg != kAlgLLKNoth) {
+  if (alg != kAlgLLK && alg != kAlgSymLLK && alg != kAlgLLKNoth && alg != kAlgStabLLK) {
     set_error("AINV build: Invalid alg %d", alg);
     return AINV_ERR_ARG;
   }
@@ -255,6 +371,8 @@ int ainv_biconjg_build(const HostCsr &a_in, int alg, int fill_in, double thresh,
   if (alg == kAlgSymLLK) {
     zb.run(a11, p, zc);
     wc = zc;  // W = Z (src/impl/mld_dsparse_biconjg_s_llk.F90:246)
+  } else if (alg == kAlgStabLLK) {
+    stab_llk(a, at, fill_in, thresh, a11, p, zc, wc);
   } else {
     HalfBuilder wb(at, a, fill_in, thresh, alpha_test);  // dots: columns of A
     std::thread th([&] { wb.run(a11, q, wc); });

@@ -224,7 +224,7 @@ int mld_d_solver_build(mld_d_solver *sv, int n, const int *irp, const int *ja,
   clear_data(sv);
   int rc;
   if (sv->kind == kAinv) {
-    if (sv->alg == ainv::kAlgStabLLK || sv->alg == ainv::kAlgMLK) {
+    if (sv->alg == ainv::kAlgMLK) {
       ainv::set_error("AINV build: algorithm '%s' is not built into this library",
                       alg_name(sv->alg));
       return AINV_ERR_UNSUPPORTED;

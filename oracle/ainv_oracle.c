@@ -18,6 +18,10 @@
  *     fixes which equal-magnitude entries survive the fill cap.
  *   - psb_spge_dot: sequential sum of x(i)*y(iv(i)) from zero.
  *   - psb_d_csr_maxval: max |a_ij|.
+ *   - psb_d_spvspm / psb_d_spmspv (x^T A and A x for a sparse x, used by
+ *     STAB-LLK): accumulated in x's entry order, result sorted by index;
+ *     psb_spdot_srtd: merge of two index-sorted sparse vectors.  These
+ *     orders are this restatement's choice (unpinned).
  */
 #include "ainv_oracle.h"
 
@@ -293,6 +297,139 @@ static int biconjg_half(int n, int noth, const int *dp, const int *di,
   return 0;
 }
 
+/* y = x^T M for a sparse x (nx entries xi/xv) and M in CSR (mp/mi/mv): the
+ * entries of x in stored order, each adding x_k * M(k, :) into a dense
+ * accumulator; the touched indices come back sorted with their sums.  With M
+ * = A this is psb_d_spvspm(done, a, x, dzero, y); with M the CSR of A^T
+ * (A's CSC arrays) it is psb_d_spmspv(done, ac, x, dzero, y) = A x.  PSBLAS
+ * is not in the reference tree: the accumulation order (x's order) and the
+ * sorted output are this restatement's choice, so bits at this boundary are
+ * unpinned. */
+static int cmp_int(const void *a, const void *b) {
+  int x = *(const int *)a, y = *(const int *)b;
+  return (x > y) - (x < y);
+}
+static int sp_x_mat(int nx, const int *xi, const double *xv, const int *mp, const int *mi,
+                    const double *mv, double *acc, char *flag, int *yi, double *yv) {
+  int ny = 0;
+  for (int k = 0; k < nx; k++) {
+    int r = xi[k];
+    for (int e = mp[r]; e < mp[r + 1]; e++) {
+      int c = mi[e];
+      if (!flag[c]) { flag[c] = 1; acc[c] = 0.0; yi[ny++] = c; }
+      acc[c] = acc[c] + xv[k] * mv[e];
+    }
+  }
+  qsort(yi, (size_t)ny, sizeof(int), cmp_int);
+  for (int m = 0; m < ny; m++) { yv[m] = acc[yi[m]]; flag[yi[m]] = 0; }
+  return ny;
+}
+
+/* Stabilised left-looking biconjugation, mld_dsparse_biconjg_s_ft_llk
+ * (src/impl/mld_dsparse_biconjg_s_ft_llk.F90:35-414).  Column i of Z, then
+ * column i of W, sharing one work vector and heaps:
+ *  - Z step j: p_i = (w_j^T A) . zval (psb_d_spvspm, :164-169), alpha = -p_i/p_j;
+ *  - W step j: q_i = (A z_j) . wval (psb_d_spmspv, :297-304), alpha = -q_i/q_j;
+ *  - then q_i = (A z_i) . w_i over the kept entries (psb_spdot_srtd, :381-389),
+ *    the 1e-3 guard, and p_i = q_i (:402-406).
+ * Candidate steps come from A's columns (Z) and rows (W) as in LLK; the
+ * heap only ever holds j < i, so the loop's exit at j >= i (:159,:282) acts
+ * like LLK's skip.  Z and W come back as CSC arrays. */
+static int biconjg_s_ft_llk(int n, const int *ap, const int *aj, const double *av,
+                            const int *acp, const int *ari, const double *acv,
+                            int nzrmax, double thresh, double a11, double *p,
+                            int *zcp, int *zri, double *zv, int *wcp, int *wri, double *wv) {
+  double *zval = (double *)calloc((size_t)n, sizeof(double));
+  int *izkr = (int *)calloc((size_t)n, sizeof(int));
+  int *izcr = (int *)calloc((size_t)n, sizeof(int));
+  double *acc = (double *)calloc((size_t)n, sizeof(double));
+  char *flag = (char *)calloc((size_t)n, 1);
+  int *yi = (int *)malloc(sizeof(int) * (size_t)n);
+  double *yv = (double *)malloc(sizeof(double) * (size_t)n);
+  double *xw = (double *)malloc(sizeof(double) * (size_t)(nzrmax + 1));
+  int *xwid = (int *)malloc(sizeof(int) * (size_t)(nzrmax + 1));
+  iheap heap = {0}, rheap = {0};
+  dheap dh = {0};
+  if (!zval || !izkr || !izcr || !acc || !flag || !yi || !yv || !xw || !xwid) return -1;
+
+  p[0] = a11;
+  zcp[0] = 0; zcp[1] = 1; zri[0] = 0; zv[0] = 1.0;
+  wcp[0] = 0; wcp[1] = 1; wri[0] = 0; wv[0] = 1.0;
+  long nzz = 1, nzw = 1;
+
+  for (int i = 1; i < n; i++) {
+    for (int half = 0; half < 2; half++) {
+      /* half 0: Z (candidates from A's column i / columns kr; dot source W);
+       * half 1: W (candidates from A's row i / rows kr; dot source Z) */
+      const int *cp = half == 0 ? acp : ap, *ci = half == 0 ? ari : aj;
+      int *fcp = half == 0 ? zcp : wcp, *fri = half == 0 ? zri : wri;
+      double *fv = half == 0 ? zv : wv;
+      const int *ocp = half == 0 ? wcp : zcp, *ori = half == 0 ? wri : zri;
+      const double *ov = half == 0 ? wv : zv;
+      const int *mp = half == 0 ? ap : acp, *mi = half == 0 ? aj : ari;
+      const double *mv = half == 0 ? av : acv;
+      zval[i] = 1.0;
+      izkr[i] = 1;
+      heap.n = 0;
+      ih_push(&heap, i);
+      rheap.n = 0;
+      for (int k = cp[i]; k < cp[i + 1]; k++)
+        if (ci[k] < i) { ih_push(&rheap, ci[k]); izcr[ci[k]] = 1; }
+      int lastj = -1;
+      for (;;) {
+        int j, got = 0;
+        while (ih_pop(&rheap, &j) == 0)
+          if (j > lastj) { lastj = j; got = 1; break; }
+        if (!got) break;
+        izcr[j] = 0;
+        if (j >= i) break;
+        int ny = sp_x_mat(ocp[j + 1] - ocp[j], ori + ocp[j], ov + ocp[j], mp, mi, mv, acc, flag,
+                          yi, yv);
+        double s = 0.0;
+        for (int m = 0; m < ny; m++) s = s + yv[m] * zval[yi[m]];
+        double alpha = -s / p[j];
+        if (fabs(alpha) > thresh) {
+          for (long k = fcp[j]; k < fcp[j + 1]; k++) {
+            int kr = fri[k];
+            zval[kr] = zval[kr] + alpha * fv[k];
+            if (izkr[kr] == 0) {
+              ih_push(&heap, kr);
+              izkr[kr] = 1;
+              for (int kc = cp[kr]; kc < cp[kr + 1]; kc++) {
+                int nextj = ci[kc];
+                if (izcr[nextj] == 0 && nextj > j && nextj < i) {
+                  ih_push(&rheap, nextj);
+                  izcr[nextj] = 1;
+                }
+              }
+            }
+          }
+        }
+      }
+      long *nzf = half == 0 ? &nzz : &nzw;
+      int nz = sparsify(i, nzrmax, thresh, zval, &heap, izkr, &dh, xw, xwid, fri + *nzf,
+                        fv + *nzf);
+      *nzf += nz;
+      fcp[i + 1] = (int)*nzf;
+    }
+    /* q_i = (A z_i) . w_i, both index-sorted */
+    int ny = sp_x_mat(zcp[i + 1] - zcp[i], zri + zcp[i], zv + zcp[i], acp, ari, acv, acc, flag,
+                      yi, yv);
+    double s = 0.0;
+    int a = 0, b = wcp[i];
+    while (a < ny && b < wcp[i + 1]) {
+      if (yi[a] < wri[b]) a++;
+      else if (yi[a] > wri[b]) b++;
+      else { s = s + yv[a] * wv[b]; a++; b++; }
+    }
+    if (fabs(s) < ORC_EPSTOL) s = 1.0e-3;
+    p[i] = s;
+  }
+  free(zval); free(izkr); free(izcr); free(acc); free(flag); free(yi); free(yv);
+  free(xw); free(xwid); free(heap.v); free(rheap.v); free(dh.key); free(dh.idx);
+  return 0;
+}
+
 /* CSR -> CSC (equivalently CSR of the transpose); indices come out sorted
  * because rows are scanned in ascending order. */
 static void csr_transpose(int n, const int *irp, const int *ja, const double *val,
@@ -353,9 +490,16 @@ int orc_ainv_build(int alg, int n, const int *irp, const int *ja,
   double *p = (double *)malloc(sizeof(double) * (size_t)n);
   double *q = (double *)malloc(sizeof(double) * (size_t)n);
   int noth = (alg == ORC_ALG_LLK_NOTH);
-  int rc = biconjg_half(n, noth, cirp, cja, cval, acp, ari, fill_in, thresh, a11,
-                        p, zcp, zri, zv);
-  if (rc == 0) {
+  int rc;
+  if (alg == ORC_ALG_S_FT_LLK) {
+    /* W's CSC arrays go straight into the CSR arrays of Wt */
+    rc = biconjg_s_ft_llk(n, cirp, cja, cval, acp, ari, acv, fill_in, thresh, a11, p,
+                          zcp, zri, zv, wt_irp, wt_ja, wt_val);
+  } else {
+    rc = biconjg_half(n, noth, cirp, cja, cval, acp, ari, fill_in, thresh, a11,
+                      p, zcp, zri, zv);
+  }
+  if (rc == 0 && alg != ORC_ALG_S_FT_LLK) {
     if (alg == ORC_ALG_S_LLK) {
       /* W = Z (src/impl/mld_dsparse_biconjg_s_llk.F90:246) */
       memcpy(wt_irp, zcp, sizeof(int) * (size_t)(n + 1));

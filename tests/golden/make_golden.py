@@ -9,6 +9,7 @@ separately from the C oracle and following the Fortran line by line:
   - left-looking biconjugation        src/impl/mld_dsparse_biconjg_llk.F90:35-366
   - SYM-LLK (W = Z)                   src/impl/mld_dsparse_biconjg_s_llk.F90:246
   - LLK without the alpha test        src/impl/mld_dsparse_biconjg_llk_noth.F90
+  - STAB-LLK (stabilised pivots)      src/impl/mld_dsparse_biconjg_s_ft_llk.F90
   - sparsify (diag + nzrmax-1 largest, PSBLAS magnitude-heap tie order)
                                       src/impl/mld_d_sparsify.f90:35-149
   - Z CSC->CSR, W CSC->transpose      src/mld_d_biconjg_mod.F90:131-135
@@ -196,6 +197,83 @@ def biconjg_half(n, dot_rows, cand_rows, nzrmax, thresh, piv0, noth):
     return piv, cols
 
 
+def sp_x_mat(xi, xv, mrows):
+    """y = x^T M for a sparse index-sorted x and M given by rows: x's entries
+    in order, each adding x_k * M(k, :); the result sorted by index.  With M
+    = A this is PSBLAS psb_d_spvspm; with M = A^T (A's columns) it is
+    psb_d_spmspv, y = A x (an order of accumulation chosen here: PSBLAS is
+    outside the reference tree)."""
+    acc = {}
+    for k, xk in zip(xi, xv):
+        for c, a in mrows[k]:
+            acc[c] = acc.get(c, 0.0) + xk * a
+    idx = sorted(acc)
+    return idx, [acc[c] for c in idx]
+
+
+def stab_llk(n, srows, scols, col_idx, row_idx, nzrmax, thresh, piv0):
+    """mld_dsparse_biconjg_s_ft_llk (src/impl/mld_dsparse_biconjg_s_ft_llk.F90):
+    for each i, column i of Z (step j: (w_j^T A) . z) and then of W (step j:
+    (A z_j) . w), both divided by the common pivot of column j; the pivot of
+    column i is (A z_i) . w_i over the kept entries, with the 1e-3 guard."""
+    piv = [0.0] * n
+    piv[0] = piv0
+    zcols, wcols = [([0], [1.0])], [([0], [1.0])]
+    zw = [0.0] * n
+    for i in range(1, n):
+        for half in (0, 1):
+            cand = col_idx if half == 0 else row_idx
+            own = zcols if half == 0 else wcols
+            other = wcols if half == 0 else zcols
+            mrows = srows if half == 0 else scols
+            zw[i] = 1.0
+            nzset = {i}
+            rh = []
+            flagged = set()
+            for j in cand[i]:
+                if j < i:
+                    heapq.heappush(rh, j)
+                    flagged.add(j)
+            lastj = -1
+            while True:
+                j = None
+                while rh:
+                    c = heapq.heappop(rh)
+                    if c > lastj:
+                        lastj = c
+                        j = c
+                        break
+                if j is None or j >= i:
+                    break
+                flagged.discard(j)
+                yi, yv = sp_x_mat(*other[j], mrows)
+                s = 0.0
+                for k, y in zip(yi, yv):
+                    s = s + y * zw[k]
+                alpha = -s / piv[j]
+                if abs(alpha) > thresh:
+                    ci, cv = own[j]
+                    for kr, v in zip(ci, cv):
+                        zw[kr] = zw[kr] + alpha * v
+                        if kr not in nzset:
+                            nzset.add(kr)
+                            for nj in cand[kr]:
+                                if nj not in flagged and j < nj < i:
+                                    heapq.heappush(rh, nj)
+                                    flagged.add(nj)
+            own.append(sparsify(i, nzrmax, thresh, zw, nzset))
+        yi, yv = sp_x_mat(*zcols[i], scols)
+        w = dict(zip(*wcols[i]))
+        s = 0.0
+        for k, y in zip(yi, yv):
+            if k in w:
+                s = s + y * w[k]
+        if abs(s) < EPSTOL:
+            s = 1.0e-3
+        piv[i] = s
+    return piv, zcols, wcols
+
+
 def ainv_build(rows, alg, nzrmax, thresh):
     n = len(rows)
     mx = max(abs(v) for e in rows for _, v in e)
@@ -215,10 +293,13 @@ def ainv_build(rows, alg, nzrmax, thresh):
     col_idx = [[r for r, _ in e] for e in scols]
     row_idx = [[c for c, _ in e] for e in srows]
     noth = alg == "LLK-NOTH"
-    p, zcols = biconjg_half(n, srows, col_idx, nzrmax, thresh, a11, noth)
+    if alg == "STAB-LLK":
+        p, zcols, wcols = stab_llk(n, srows, scols, col_idx, row_idx, nzrmax, thresh, a11)
+    else:
+        p, zcols = biconjg_half(n, srows, col_idx, nzrmax, thresh, a11, noth)
     if alg == "SYM-LLK":
         wcols = zcols
-    else:
+    elif alg != "STAB-LLK":
         _, wcols = biconjg_half(n, scols, row_idx, nzrmax, thresh, a11, noth)
     d = np.array([(1.0 if abs(v) < EPSTOL else 1.0 / v) * w for v in p])
     # Wt CSR: row i = column w_i
@@ -519,6 +600,8 @@ CASES = [
     ("convdiff6_cap4", 6, "convdiff", (40.0, -25.0, 10.0), "LLK", 4, 0.02),
     ("convdiff5_noth", 5, "convdiff", (30.0, 30.0, 30.0), "LLK-NOTH", 6, 0.05),
     ("convdiff5_sym", 5, "convdiff", (5.0, 5.0, 5.0), "SYM-LLK", 8, 0.05),
+    ("convdiff6_stab", 6, "convdiff", (40.0, -25.0, 10.0), "STAB-LLK", 8, 0.05),
+    ("convdiff4_stab_exact", 4, "convdiff", (20.0, 5.0, -15.0), "STAB-LLK", 64, 0.0),
 ]
 
 HAND_4x4 = [  # small nonsymmetric case worked by hand in the test

@@ -82,20 +82,58 @@ def test_host_build_matches_golden(path):
         np.testing.assert_array_equal(f[k], g[k], err_msg=k)
 
 
+@pytest.mark.parametrize("alg", ["LLK", "STAB-LLK"])
 @pytest.mark.parametrize("idim,kind,beta,fill,thr", [
     (14, "convdiff", (10 / np.sqrt(3),) * 3, 20, 0.1),
     (11, "convdiff", (80.0, -30.0, 15.0), 6, 0.02),
     (12, "poisson", (0, 0, 0), 3, 0.01),
     (10, "convdiff", (-50.0, 20.0, -70.0), 20, 0.0),
 ])
-def test_host_build_matches_oracle(idim, kind, beta, fill, thr):
+def test_host_build_matches_oracle(idim, kind, beta, fill, thr, alg):
     irp, ja, val = ainv.pde.gen_pde3d(idim, kind, beta)
     sv = ainv.mld_d_ainv_solver_type()
+    assert sv.csetc("AINV_ALG", alg) == 0
     sv.cseti("SUB_FILLIN", fill)
     sv.csetr("SUB_ILUTHRS", thr)
     assert sv.build(irp, ja, val) == 0
-    of = O.ainv_build(O.CSR(len(irp) - 1, irp, ja, val), "LLK", fill, thr)
+    of = O.ainv_build(O.CSR(len(irp) - 1, irp, ja, val), alg, fill, thr)
     _factors_equal(sv.factors(), of)
+
+
+def _dense(irp, ja, val, n):
+    m = np.zeros((n, n))
+    for r in range(n):
+        for k in range(irp[r], irp[r + 1]):
+            m[r, ja[k]] += val[k]
+    return m
+
+
+@pytest.mark.parametrize("kind,beta", [("convdiff", (25.0, -10.0, 5.0)), ("poisson", (0, 0, 0))])
+def test_stab_llk_known_answers(kind, beta):
+    """STAB-LLK without dropping is an exact biconjugation, Z D^-1 W^T = A^-1;
+    on a symmetric A its W equals Z; with dropping its pivots differ from
+    LLK's (they come from w_i^T A z_i)."""
+    irp, ja, val = ainv.pde.gen_pde3d(5, kind, beta)
+    n = len(irp) - 1
+    sv = ainv.mld_d_ainv_solver_type()
+    assert sv.csetc("AINV_ALG", "STAB-LLK") == 0
+    sv.cseti("SUB_FILLIN", n)
+    sv.csetr("SUB_ILUTHRS", 0.0)
+    assert sv.build(irp, ja, val) == 0
+    f = sv.factors()
+    wt = _dense(f["wt_irp"], f["wt_ja"], f["wt_val"], n)
+    z = _dense(f["z_irp"], f["z_ja"], f["z_val"], n)
+    m = z @ np.diag(f["d"]) @ wt
+    assert np.abs(m @ _dense(irp, ja, val, n) - np.eye(n)).max() < 1e-12
+    if kind == "poisson":
+        np.testing.assert_array_equal(wt.T, z)
+    llk, stab = ainv.mld_d_ainv_solver_type(), ainv.mld_d_ainv_solver_type()
+    assert stab.csetc("AINV_ALG", "STAB-LLK") == 0
+    for s in (llk, stab):
+        s.cseti("SUB_FILLIN", 8)
+        s.csetr("SUB_ILUTHRS", 0.05)
+        assert s.build(irp, ja, val) == 0
+    assert not np.array_equal(llk.factors()["d"], stab.factors()["d"])
 
 
 def test_generators_match_oracle():
