@@ -8,9 +8,8 @@
 // sparsification of src/impl/mld_d_sparsify.f90:35-149.  Floating-point
 // operations happen in the reference's order with one rounding per
 // operation, so the factors are bit-identical to the reference algorithm.
-// (STAB-LLK also multiplies A by sparse columns of Z and W through PSBLAS
-// routines outside the reference tree; their accumulation order here is
-// documented at SparseProduct.)
+// (STAB-LLK also multiplies A by sparse columns of Z and W; the order of
+// those sums is documented at SparseProduct.)
 //
 // In LLK the Z and W halves only share read-only data (A and its
 // transpose), so they run on two threads.  STAB-LLK interleaves them.
@@ -33,8 +32,9 @@ constexpr double kTinyPivot = 1.0e-3;
 // Magnitude-ordered heap with the exact pop order of PSBLAS psb_d_idx_heap
 // in psb_asort_down_ mode: 1-based binary heap; an inserted key rises while
 // strictly larger in magnitude than its parent; the root's replacement sinks
-// toward the larger child (left child on ties, or when it is the last
-// element) while strictly smaller than it.  This order decides which
+// toward the larger child (the left one only when strictly larger or when
+// it is the last element, so the right one on ties) while strictly smaller
+// than it.  This order decides which
 // equal-magnitude entries survive the fill cap.
 class MagnitudeHeap {
  public:
@@ -223,11 +223,11 @@ class HalfBuilder {
 };
 
 // y = x^T M for a sparse x (an index-sorted column of Z or W) and M in CSR:
-// x's entries in order, each adding x_k * M(k, :) into a dense accumulator;
-// the result comes back sorted by index.  With M = A this is PSBLAS
-// psb_d_spvspm(done, a, x, dzero, y); with M = A^T (A's CSC arrays) it is
-// psb_d_spmspv(done, ac, x, dzero, y) = A x.  PSBLAS is not part of the
-// reference tree; this accumulation order is the restatement's own.
+// psb_d_spvspm (M = A) and psb_d_spmspv (M = A^T, i.e. A's CSC arrays, giving
+// A x) of src/mld_d_biconjg_mod.F90:145-296.  Those take x's entries in
+// order and merge (1*x_k) * M(k, :) into the running result with PSBLAS's
+// sorted sparse axpby psb_nspaxpby (y_c = x_k*m + y_c, two roundings), so
+// the result is index-sorted and each sum runs in x's order, as here.
 class SparseProduct {
  public:
   explicit SparseProduct(int n) : acc_((size_t)n, 0.0), seen_((size_t)n, 0) {}
@@ -291,7 +291,8 @@ class SparseProduct {
 // (:164-169), the W step j uses q_i = (A z_j) . w (:297-304), both divided by
 // the common pivot of column j; the pivot of column i is then
 // (A z_i) . w_i over the kept entries (:381-389) with the 1e-3 guard
-// (:402-406).  Candidate steps come from A's columns (Z) and rows (W) as in
+// (:402-406), psb_spdot_srtd being a merge of two index-sorted sparse
+// vectors.  Candidate steps come from A's columns (Z) and rows (W) as in
 // LLK.  The halves depend on each other column by column, so they run in
 // turn on one thread.
 void stab_llk(const HostCsr &a, const HostCsr &at, int cap, double thresh, double piv0,

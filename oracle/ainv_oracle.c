@@ -18,10 +18,9 @@
  *     fixes which equal-magnitude entries survive the fill cap.
  *   - psb_spge_dot: sequential sum of x(i)*y(iv(i)) from zero.
  *   - psb_d_csr_maxval: max |a_ij|.
- *   - psb_d_spvspm / psb_d_spmspv (x^T A and A x for a sparse x, used by
- *     STAB-LLK): accumulated in x's entry order, result sorted by index;
- *     psb_spdot_srtd: merge of two index-sorted sparse vectors.  These
- *     orders are this restatement's choice (unpinned).
+ *   - psb_nspaxpby (sorted sparse axpby, used by the in-tree
+ *     psb_d_spvspm / psb_d_spmspv for STAB-LLK) and psb_spdot_srtd (merge
+ *     of two index-sorted sparse vectors).
  */
 #include "ainv_oracle.h"
 
@@ -297,14 +296,13 @@ static int biconjg_half(int n, int noth, const int *dp, const int *di,
   return 0;
 }
 
-/* y = x^T M for a sparse x (nx entries xi/xv) and M in CSR (mp/mi/mv): the
- * entries of x in stored order, each adding x_k * M(k, :) into a dense
- * accumulator; the touched indices come back sorted with their sums.  With M
- * = A this is psb_d_spvspm(done, a, x, dzero, y); with M the CSR of A^T
- * (A's CSC arrays) it is psb_d_spmspv(done, ac, x, dzero, y) = A x.  PSBLAS
- * is not in the reference tree: the accumulation order (x's order) and the
- * sorted output are this restatement's choice, so bits at this boundary are
- * unpinned. */
+/* y = x^T M for a sparse x (nx entries xi/xv) and M in CSR (mp/mi/mv):
+ * psb_d_spvspm (M = A) and psb_d_spmspv (M = the CSR of A^T, i.e. A's CSC
+ * arrays, giving A x), src/mld_d_biconjg_mod.F90:145-296.  They take x's
+ * entries in order and merge (1*x_k) * M(k, :) into the running result with
+ * PSBLAS's sorted sparse axpby psb_nspaxpby: y_c = x_k*m + y_c with two
+ * roundings, result index-sorted.  Here: a dense accumulator summed in x's
+ * order, indices sorted at the end -- the same numbers. */
 static int cmp_int(const void *a, const void *b) {
   int x = *(const int *)a, y = *(const int *)b;
   return (x > y) - (x < y);

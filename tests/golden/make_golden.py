@@ -199,10 +199,9 @@ def biconjg_half(n, dot_rows, cand_rows, nzrmax, thresh, piv0, noth):
 
 def sp_x_mat(xi, xv, mrows):
     """y = x^T M for a sparse index-sorted x and M given by rows: x's entries
-    in order, each adding x_k * M(k, :); the result sorted by index.  With M
-    = A this is PSBLAS psb_d_spvspm; with M = A^T (A's columns) it is
-    psb_d_spmspv, y = A x (an order of accumulation chosen here: PSBLAS is
-    outside the reference tree)."""
+    in order, each merged as x_k * M(k, :) into the sorted result (psb_d_spvspm
+    with M = A, psb_d_spmspv with M = A's columns giving A x;
+    src/mld_d_biconjg_mod.F90:145-296, through PSBLAS psb_nspaxpby)."""
     acc = {}
     for k, xk in zip(xi, xv):
         for c, a in mrows[k]:
