@@ -4,7 +4,8 @@
 // Algorithm: mld_d_ainv_bld (src/impl/mld_d_ainv_bld.F90:35-194) with the
 // maxval scaling the solver always requests (src/impl/mld_d_ainv_solver_bld.f90:68-69),
 // the left-looking biconjugation of src/impl/mld_dsparse_biconjg_llk.F90:35-366
-// (plus the SYM-LLK, no-alpha-test and stabilised STAB-LLK variants), and the column
+// (plus the SYM-LLK, no-alpha-test, stabilised STAB-LLK and list-based MLK
+// variants), and the column
 // sparsification of src/impl/mld_d_sparsify.f90:35-149.  Floating-point
 // operations happen in the reference's order with one rounding per
 // operation, so the factors are bit-identical to the reference algorithm.
@@ -79,6 +80,52 @@ class MagnitudeHeap {
   std::vector<int> idx_{0};
 };
 
+// PSBLAS psb_hsort(x, ix, dir=psb_asort_down_) on m entries: a heap with
+// the smallest magnitude at the root (1-based; an inserted key rises while
+// strictly smaller in magnitude than its parent; the root's replacement
+// sinks toward the smaller child -- the left one only when strictly smaller
+// or when it is the last element -- while strictly larger than it) takes
+// the entries in order; then the root is taken out m-1 times and stored
+// from the last position backwards, and the first position keeps the last
+// root.  The result is descending in magnitude; this fixes the order of
+// equal magnitudes.
+void hsort_abs_down(double *x, int *ix, int m) {
+  std::vector<double> k(1);
+  std::vector<int> v(1);
+  for (int j = 0; j < m; j++) {
+    k.push_back(x[j]);
+    v.push_back(ix[j]);
+    size_t c = k.size() - 1;
+    while (c > 1 && std::fabs(k[c]) < std::fabs(k[c / 2])) {
+      std::swap(k[c], k[c / 2]);
+      std::swap(v[c], v[c / 2]);
+      c /= 2;
+    }
+  }
+  for (int j = m - 1; j >= 1; j--) {
+    x[j] = k[1];
+    ix[j] = v[1];
+    k[1] = k.back();
+    v[1] = v.back();
+    k.pop_back();
+    v.pop_back();
+    const size_t last = k.size() - 1;
+    size_t c = 1;
+    while (c <= last / 2) {
+      const size_t l = 2 * c;
+      const size_t ch = (l == last || std::fabs(k[l]) < std::fabs(k[l + 1])) ? l : l + 1;
+      if (!(std::fabs(k[c]) > std::fabs(k[ch]))) break;
+      std::swap(k[c], k[ch]);
+      std::swap(v[c], v[ch]);
+      c = ch;
+    }
+  }
+  if (m > 0) {
+    x[0] = k[1];
+    ix[0] = v[1];
+  }
+}
+
 using MinQueue = std::priority_queue<int, std::vector<int>, std::greater<int>>;
 
 // Column-by-column builder of one unit upper triangular factor (Z, or W).
@@ -88,10 +135,11 @@ using MinQueue = std::priority_queue<int, std::vector<int>, std::greater<int>>;
 // nonzero at kr (columns of A for Z, rows of A for W).
 class HalfBuilder {
  public:
+  // list_sparsify: MLK's mld_d_sparsify_list instead of mld_d_sparsify.
   HalfBuilder(const HostCsr &dots, const HostCsr &touch, int cap, double thresh,
-              bool alpha_test)
+              bool alpha_test, bool list_sparsify = false)
       : dots_(dots), touch_(touch), n_(dots.n), cap_(cap), thresh_(thresh),
-        alpha_test_(alpha_test) {}
+        alpha_test_(alpha_test), list_sparsify_(list_sparsify) {}
 
   // piv receives the pivots; out gets the factor as CSC columns.
   void run(double piv0, std::vector<double> &piv, HostCsr &out) {
@@ -170,9 +218,50 @@ class HalfBuilder {
 
   const std::vector<double> &work() const { return work_; }
 
+  // mld_d_sparsify_list (src/impl/mld_d_sparsify.f90:152-230): the column's
+  // entries in index order, the diagonal swapped into the first slot (the
+  // entry it displaces takes the diagonal's place); the rest sorted by
+  // descending magnitude (psb_hsort); cut at the first entry below thresh
+  // and at cap entries; survivors sorted by index.
+  void keep_column_list(int i, HostCsr &out) {
+    std::sort(nz_.begin(), nz_.end());
+    lw_.clear();
+    li_.clear();
+    for (int r : nz_) {
+      lw_.push_back(work_[r]);
+      li_.push_back(r);
+      if (r == i) {
+        std::swap(lw_.front(), lw_.back());
+        std::swap(li_.front(), li_.back());
+      }
+      work_[r] = 0.0;
+      in_col_[r] = 0;
+    }
+    const int m = (int)lw_.size();
+    if (m > 2) hsort_abs_down(lw_.data() + 1, li_.data() + 1, m - 1);
+    int k = 1;
+    while (k < m && !(std::fabs(lw_[k]) < thresh_)) k++;
+    const int keep = std::max(1, std::min(k, cap_));
+    kept_.clear();
+    for (int e = 0; e < keep; e++) kept_.push_back({li_[e], lw_[e]});
+    std::sort(kept_.begin(), kept_.end(),
+              [](const std::pair<int, double> &a, const std::pair<int, double> &b) {
+                return a.first < b.first;
+              });
+    for (const auto &e : kept_) {
+      out.ja.push_back(e.first);
+      out.val.push_back(e.second);
+    }
+    out.irp[(size_t)i + 1] = (int)out.ja.size();
+  }
+
   // Diagonal plus at most cap-1 entries of largest magnitude >= thresh,
   // offered to the heap in ascending index order; survivors sorted by index.
   void keep_column(int i, HostCsr &out) {
+    if (list_sparsify_) {
+      keep_column_list(i, out);
+      return;
+    }
     std::sort(nz_.begin(), nz_.end());
     heap_.clear();
     double diag = 0.0;
@@ -214,8 +303,9 @@ class HalfBuilder {
   const HostCsr &touch_;
   const int n_, cap_;
   const double thresh_;
-  const bool alpha_test_;
-  std::vector<double> work_;
+  const bool alpha_test_, list_sparsify_;
+  std::vector<double> work_, lw_;
+  std::vector<int> li_;
   std::vector<char> in_col_, queued_;
   std::vector<int> nz_;  // positions set in work_, in insertion order
   MagnitudeHeap heap_;
@@ -330,7 +420,8 @@ int ainv_biconjg_build(const HostCsr &a_in, int alg, int fill_in, double thresh,
     set_error("AINV build: fill_in must be >= 1 (got %d)", fill_in);
     return AINV_ERR_ARG;
   }
-  if (alg != kAlgLLK && alg != kAlgSymLLK && alg != kAlgLLKNoth && alg != kAlgStabLLK) {
+  if (alg != kAlgLLK && alg != kAlgSymLLK && alg != kAlgLLKNoth && alg != kAlgStabLLK &&
+      alg != kAlgMLK) {
     set_error("AINV build: Invalid alg %d", alg);
     return AINV_ERR_ARG;
   }
@@ -368,14 +459,19 @@ int ainv_biconjg_build(const HostCsr &a_in, int alg, int fill_in, double thresh,
   const bool alpha_test = alg != kAlgLLKNoth;
   std::vector<double> p, q;
   HostCsr zc, wc;
-  HalfBuilder zb(a, at, fill_in, thresh, alpha_test);   // dots: rows of A
+  // MLK (src/impl/mld_dsparse_biconjg_mlk.F90) keeps its candidate steps and
+  // nonzero positions in sorted linked lists merged by hlmerge (:444-487)
+  // instead of heaps.  Those visit the same steps in the same ascending order
+  // as LLK's heaps, so only its list form of sparsify differs.
+  const bool mlk = alg == kAlgMLK;
+  HalfBuilder zb(a, at, fill_in, thresh, alpha_test, mlk);   // dots: rows of A
   if (alg == kAlgSymLLK) {
     zb.run(a11, p, zc);
     wc = zc;  // W = Z (src/impl/mld_dsparse_biconjg_s_llk.F90:246)
   } else if (alg == kAlgStabLLK) {
     stab_llk(a, at, fill_in, thresh, a11, p, zc, wc);
   } else {
-    HalfBuilder wb(at, a, fill_in, thresh, alpha_test);  // dots: columns of A
+    HalfBuilder wb(at, a, fill_in, thresh, alpha_test, mlk);  // dots: columns of A
     std::thread th([&] { wb.run(a11, q, wc); });
     zb.run(a11, p, zc);
     th.join();

@@ -224,11 +224,6 @@ int mld_d_solver_build(mld_d_solver *sv, int n, const int *irp, const int *ja,
   clear_data(sv);
   int rc;
   if (sv->kind == kAinv) {
-    if (sv->alg == ainv::kAlgMLK) {
-      ainv::set_error("AINV build: algorithm '%s' is not built into this library",
-                      alg_name(sv->alg));
-      return AINV_ERR_UNSUPPORTED;
-    }
     rc = ainv::ainv_biconjg_build(a, sv->alg, sv->fill_in, sv->thresh, sv->wt, sv->z, sv->d);
   } else if (sv->kind == kInvk) {
     // src/impl/mld_d_invk_solver_bld.f90:68-69: (fill_in, inv_fill) -> (w, d, z)

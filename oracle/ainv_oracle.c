@@ -428,6 +428,186 @@ static int biconjg_s_ft_llk(int n, const int *ap, const int *aj, const double *a
   return 0;
 }
 
+/* ---------------------------------------------------------------- MLK */
+/* psb_hsort(x, ix, dir=psb_asort_down_) on m entries, in place: the entries
+ * are inserted one by one into a 1-based heap with the smallest |x| at the
+ * root (rise while strictly smaller than the parent); then for j = m..2 the
+ * root is taken out (the last heap entry sinks from the root toward the
+ * smaller child -- left only when strictly smaller or the last one -- while
+ * strictly larger) and stored at position j.  Descending |x|. */
+static void o_hsort_abs_down(double *x, int *ix, int m) {
+  for (int i = 1; i <= m; i++) {
+    int c = i;
+    double key = x[c - 1];
+    int id = ix[c - 1];
+    while (c > 1 && fabs(key) < fabs(x[c / 2 - 1])) {
+      x[c - 1] = x[c / 2 - 1];
+      ix[c - 1] = ix[c / 2 - 1];
+      c /= 2;
+    }
+    x[c - 1] = key;
+    ix[c - 1] = id;
+  }
+  for (int j = m; j >= 2; j--) {
+    double top = x[0], lk = x[j - 1];
+    int tid = ix[0], lid = ix[j - 1];
+    int size = j - 1, c = 1;
+    while (2 * c <= size) {
+      int l = 2 * c;
+      int ch = (l == size || fabs(x[l - 1]) < fabs(x[l])) ? l : l + 1;
+      if (!(fabs(lk) > fabs(x[ch - 1]))) break;
+      x[c - 1] = x[ch - 1];
+      ix[c - 1] = ix[ch - 1];
+      c = ch;
+    }
+    x[c - 1] = lk;
+    ix[c - 1] = lid;
+    x[j - 1] = top;
+    ix[j - 1] = tid;
+  }
+}
+
+/* hlmerge (src/impl/mld_dsparse_biconjg_mlk.F90:444-487): merge the sorted
+ * vals[0..nv) into the sorted linked list at *head (listv[k]: next index,
+ * -1 at the end; *head = -1 for an empty list), skipping duplicates. */
+static void hlmerge(int *head, int *listv, const int *vals, int nv) {
+  int lv = 0;
+  if (*head < 0 && nv > 0) {
+    *head = vals[0];
+    lv = 1;
+  } else if (*head >= 0 && nv > 0 && *head > vals[0]) {
+    listv[vals[0]] = *head;
+    *head = vals[0];
+    lv = 1;
+  }
+  int lh = *head, ph = lh;
+  while (lh >= 0 && lv < nv) {
+    if (lh == vals[lv]) {
+      lv++;
+    } else if (lh > vals[lv]) {
+      listv[vals[lv]] = lh;
+      listv[ph] = vals[lv];
+      lh = vals[lv];
+      lv++;
+    } else {
+      ph = lh;
+      lh = listv[lh];
+    }
+  }
+  lh = ph;
+  while (lv < nv) {
+    listv[lh] = vals[lv];
+    lh = listv[lh];
+    lv++;
+  }
+}
+
+/* mld_d_sparsify_list (src/impl/mld_d_sparsify.f90:152-230): walk the list
+ * (ascending), swapping the diagonal into slot 0; sort slots 1.. by
+ * descending |value|; keep up to the first value below thresh and at most
+ * nzrmax entries; sort the survivors by index.  Clears zw, ikr and the list. */
+static int sparsify_list(int idiag, int nzrmax, double thresh, double *zw, int *lhead,
+                         int *listv, int *ikr, double *xw, int *xwid, int *oz, double *ov) {
+  int cur = *lhead, m = 0;
+  *lhead = -1;
+  while (cur >= 0) {
+    xw[m] = zw[cur];
+    xwid[m] = cur;
+    if (cur == idiag) {
+      double t = xw[0]; xw[0] = xw[m]; xw[m] = t;
+      int ti = xwid[0]; xwid[0] = xwid[m]; xwid[m] = ti;
+    }
+    m++;
+    zw[cur] = 0.0;
+    ikr[cur] = 0;
+    int next = listv[cur];
+    listv[cur] = -1;
+    cur = next;
+  }
+  if (m > 2) o_hsort_abs_down(xw + 1, xwid + 1, m - 1);
+  int k = 1;
+  while (k < m && !(fabs(xw[k]) < thresh)) k++;
+  int nz = k < nzrmax ? k : nzrmax;
+  if (nz < 1) nz = 1;
+  for (int a = 1; a < nz; a++) {
+    int ki = xwid[a];
+    double kv = xw[a];
+    int b = a - 1;
+    while (b >= 0 && xwid[b] > ki) { xwid[b + 1] = xwid[b]; xw[b + 1] = xw[b]; b--; }
+    xwid[b + 1] = ki;
+    xw[b + 1] = kv;
+  }
+  for (int a = 0; a < nz; a++) { oz[a] = xwid[a]; ov[a] = xw[a]; }
+  return nz;
+}
+
+/* One half of mld_dsparse_biconjg_mlk (src/impl/mld_dsparse_biconjg_mlk.F90:
+ * Z :116-287, W :288-438), with its linked lists: candidate steps in hlist,
+ * the column's nonzero positions in rwlist.  Arguments as biconjg_half. */
+static int biconjg_half_mlk(int n, const int *dp, const int *di, const double *dx,
+                            const int *np_, const int *ni, int nzrmax, double thresh,
+                            double piv0, double *piv, int *fcp, int *fri, double *fv) {
+  double *zval = (double *)calloc((size_t)n, sizeof(double));
+  int *izkr = (int *)calloc((size_t)n, sizeof(int));
+  int *hlist = (int *)malloc(sizeof(int) * (size_t)n);
+  int *rwlist = (int *)malloc(sizeof(int) * (size_t)n);
+  double *xw = (double *)malloc(sizeof(double) * (size_t)n);
+  int *xwid = (int *)malloc(sizeof(int) * (size_t)n);
+  if (!zval || !izkr || !hlist || !rwlist || !xw || !xwid) return -1;
+  for (int k = 0; k < n; k++) { hlist[k] = -1; rwlist[k] = -1; }
+
+  piv[0] = piv0;
+  fcp[0] = 0; fcp[1] = 1; fri[0] = 0; fv[0] = 1.0;
+  long nzz = 1;
+  for (int i = 1; i < n; i++) {
+    zval[i] = 1.0;
+    izkr[i] = 1;
+    int rwhead = i, hlhead = -1;
+    /* candidates: the entries of touch row i below i (:136-155) */
+    int ifrst = np_[i], ilst = np_[i] - 1;
+    for (int j = np_[i + 1] - 1; j >= np_[i]; j--)
+      if (ni[j] < i) { ilst = j; break; }
+    if (ilst >= ifrst) hlmerge(&hlhead, hlist, ni + ifrst, ilst - ifrst + 1);
+    for (;;) {
+      int j = hlhead;
+      if (j < 0) break;
+      hlhead = hlist[j];
+      hlist[j] = -1;
+      if (j >= i) continue;
+      double s = 0.0;
+      for (int k = dp[j]; k < dp[j + 1]; k++) s = s + zval[di[k]] * dx[k];
+      double alpha = -s / piv[j];
+      if (fabs(alpha) > thresh) {
+        hlmerge(&rwhead, rwlist, fri + fcp[j], fcp[j + 1] - fcp[j]);
+        for (long k = fcp[j]; k < fcp[j + 1]; k++) {
+          int kr = fri[k];
+          zval[kr] = zval[kr] + alpha * fv[k];
+          if (izkr[kr] == 0) {
+            izkr[kr] = 1;
+            int f = np_[kr + 1], l = np_[kr] - 1;
+            for (int kc = np_[kr]; kc < np_[kr + 1]; kc++)
+              if (ni[kc] < i && ni[kc] > j) {
+                if (kc < f) f = kc;
+                if (kc > l) l = kc;
+              }
+            if (l >= f) hlmerge(&hlhead, hlist, ni + f, l - f + 1);
+          }
+        }
+      }
+    }
+    double s = 0.0;
+    for (int k = dp[i]; k < dp[i + 1]; k++) s = s + zval[di[k]] * dx[k];
+    if (fabs(s) < ORC_EPSTOL) s = 1.0e-3;
+    piv[i] = s;
+    int nz = sparsify_list(i, nzrmax, thresh, zval, &rwhead, rwlist, izkr, xw, xwid,
+                           fri + nzz, fv + nzz);
+    nzz += nz;
+    fcp[i + 1] = (int)nzz;
+  }
+  free(zval); free(izkr); free(hlist); free(rwlist); free(xw); free(xwid);
+  return 0;
+}
+
 /* CSR -> CSC (equivalently CSR of the transpose); indices come out sorted
  * because rows are scanned in ascending order. */
 static void csr_transpose(int n, const int *irp, const int *ja, const double *val,
@@ -493,11 +673,16 @@ int orc_ainv_build(int alg, int n, const int *irp, const int *ja,
     /* W's CSC arrays go straight into the CSR arrays of Wt */
     rc = biconjg_s_ft_llk(n, cirp, cja, cval, acp, ari, acv, fill_in, thresh, a11, p,
                           zcp, zri, zv, wt_irp, wt_ja, wt_val);
+  } else if (alg == ORC_ALG_MLK) {
+    rc = biconjg_half_mlk(n, cirp, cja, cval, acp, ari, fill_in, thresh, a11, p, zcp, zri, zv);
+    if (rc == 0)
+      rc = biconjg_half_mlk(n, acp, ari, acv, cirp, cja, fill_in, thresh, a11, q, wt_irp,
+                            wt_ja, wt_val);
   } else {
     rc = biconjg_half(n, noth, cirp, cja, cval, acp, ari, fill_in, thresh, a11,
                       p, zcp, zri, zv);
   }
-  if (rc == 0 && alg != ORC_ALG_S_FT_LLK) {
+  if (rc == 0 && alg != ORC_ALG_S_FT_LLK && alg != ORC_ALG_MLK) {
     if (alg == ORC_ALG_S_LLK) {
       /* W = Z (src/impl/mld_dsparse_biconjg_s_llk.F90:246) */
       memcpy(wt_irp, zcp, sizeof(int) * (size_t)(n + 1));

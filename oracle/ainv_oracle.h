@@ -26,7 +26,7 @@ extern "C" {
 #endif
 
 /* Biconjugation variants (src/mld_base_ainv_mod.F90:50-56). */
-enum { ORC_ALG_LLK = 0, ORC_ALG_S_LLK = 1, ORC_ALG_LLK_NOTH = 2, ORC_ALG_S_FT_LLK = 3 };
+enum { ORC_ALG_LLK = 0, ORC_ALG_S_LLK = 1, ORC_ALG_LLK_NOTH = 2, ORC_ALG_S_FT_LLK = 3, ORC_ALG_MLK = 4 };
 
 /* PSBLAS d_epstol (unit roundoff guard used by the pivot checks). */
 #define ORC_EPSTOL 1.1e-16

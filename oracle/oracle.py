@@ -18,7 +18,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "libainv_oracle.so")
 _lib = None
 
-ALG = {"LLK": 0, "SYM-LLK": 1, "LLK-NOTH": 2, "STAB-LLK": 3}
+ALG = {"LLK": 0, "SYM-LLK": 1, "LLK-NOTH": 2, "STAB-LLK": 3, "MLK": 4}
 
 _i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")

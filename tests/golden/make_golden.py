@@ -10,6 +10,8 @@ separately from the C oracle and following the Fortran line by line:
   - SYM-LLK (W = Z)                   src/impl/mld_dsparse_biconjg_s_llk.F90:246
   - LLK without the alpha test        src/impl/mld_dsparse_biconjg_llk_noth.F90
   - STAB-LLK (stabilised pivots)      src/impl/mld_dsparse_biconjg_s_ft_llk.F90
+  - MLK (sparsify_list, psb_hsort)    src/impl/mld_dsparse_biconjg_mlk.F90,
+                                      src/impl/mld_d_sparsify.f90:152-230
   - sparsify (diag + nzrmax-1 largest, PSBLAS magnitude-heap tie order)
                                       src/impl/mld_d_sparsify.f90:35-149
   - Z CSC->CSR, W CSC->transpose      src/mld_d_biconjg_mod.F90:131-135
@@ -141,8 +143,69 @@ def sparsify(idiag, nzrmax, thresh, zw, nzset):
     return [xwid[t] for t in order], [xw[t] for t in order]
 
 
+def hsort_abs_down(x, ix):
+    """PSBLAS psb_hsort(dir=psb_asort_down_): the entries inserted in order
+    into a 1-based heap with the smallest |x| at the root (rise while
+    strictly smaller than the parent); the root taken out len-1 times into
+    the last free position (the last entry sinks toward the smaller child --
+    left only when strictly smaller or the last one -- while strictly
+    larger); the first position keeps the last root."""
+    hk, hv = [None], [None]
+    for key, idx in zip(x, ix):
+        hk.append(key)
+        hv.append(idx)
+        c = len(hk) - 1
+        while c > 1 and abs(hk[c]) < abs(hk[c // 2]):
+            hk[c], hk[c // 2] = hk[c // 2], hk[c]
+            hv[c], hv[c // 2] = hv[c // 2], hv[c]
+            c //= 2
+    m = len(x)
+    ox, oi = [None] * m, [None] * m
+    for j in range(m - 1, 0, -1):
+        ox[j], oi[j] = hk[1], hv[1]
+        hk[1], hv[1] = hk[-1], hv[-1]
+        hk.pop()
+        hv.pop()
+        last, c = len(hk) - 1, 1
+        while 2 * c <= last:
+            l = 2 * c
+            ch = l if (l == last or abs(hk[l]) < abs(hk[l + 1])) else l + 1
+            if not abs(hk[c]) > abs(hk[ch]):
+                break
+            hk[c], hk[ch] = hk[ch], hk[c]
+            hv[c], hv[ch] = hv[ch], hv[c]
+            c = ch
+    if m:
+        ox[0], oi[0] = hk[1], hv[1]
+    return ox, oi
+
+
+def sparsify_list(idiag, nzrmax, thresh, zw, nzset):
+    """mld_d_sparsify_list (src/impl/mld_d_sparsify.f90:152-230), used by MLK:
+    entries in index order with the diagonal swapped into slot 0, the rest
+    by descending magnitude (psb_hsort), cut at the first value below
+    thresh and at nzrmax entries, survivors sorted by index."""
+    xw, xi = [], []
+    for r in sorted(nzset):
+        xw.append(zw[r])
+        xi.append(r)
+        if r == idiag:
+            xw[0], xw[-1] = xw[-1], xw[0]
+            xi[0], xi[-1] = xi[-1], xi[0]
+        zw[r] = 0.0
+    m = len(xw)
+    if m > 2:
+        xw[1:], xi[1:] = hsort_abs_down(xw[1:], xi[1:])
+    k = 1
+    while k < m and not abs(xw[k]) < thresh:
+        k += 1
+    nz = max(1, min(k, nzrmax))
+    order = sorted(range(nz), key=lambda t: xi[t])
+    return [xi[t] for t in order], [xw[t] for t in order]
+
+
 # --------------------------------------------------------- biconjugation --
-def biconjg_half(n, dot_rows, cand_rows, nzrmax, thresh, piv0, noth):
+def biconjg_half(n, dot_rows, cand_rows, nzrmax, thresh, piv0, noth, keep=sparsify):
     """dot_rows[j]: list of (k, a) giving the dot vector j; cand_rows[kr]:
     indices j whose dot vector touches position kr; the starting candidates
     for column i are cand_rows[i] filtered to j < i."""
@@ -193,7 +256,7 @@ def biconjg_half(n, dot_rows, cand_rows, nzrmax, thresh, piv0, noth):
         if abs(s) < EPSTOL:
             s = 1.0e-3
         piv[i] = s
-        cols.append(sparsify(i, nzrmax, thresh, zw, nzset))
+        cols.append(keep(i, nzrmax, thresh, zw, nzset))
     return piv, cols
 
 
@@ -292,14 +355,17 @@ def ainv_build(rows, alg, nzrmax, thresh):
     col_idx = [[r for r, _ in e] for e in scols]
     row_idx = [[c for c, _ in e] for e in srows]
     noth = alg == "LLK-NOTH"
+    # MLK (src/impl/mld_dsparse_biconjg_mlk.F90) visits the same steps as LLK
+    # through sorted linked lists; only its list form of sparsify differs
+    keep = sparsify_list if alg == "MLK" else sparsify
     if alg == "STAB-LLK":
         p, zcols, wcols = stab_llk(n, srows, scols, col_idx, row_idx, nzrmax, thresh, a11)
     else:
-        p, zcols = biconjg_half(n, srows, col_idx, nzrmax, thresh, a11, noth)
+        p, zcols = biconjg_half(n, srows, col_idx, nzrmax, thresh, a11, noth, keep)
     if alg == "SYM-LLK":
         wcols = zcols
     elif alg != "STAB-LLK":
-        _, wcols = biconjg_half(n, scols, row_idx, nzrmax, thresh, a11, noth)
+        _, wcols = biconjg_half(n, scols, row_idx, nzrmax, thresh, a11, noth, keep)
     d = np.array([(1.0 if abs(v) < EPSTOL else 1.0 / v) * w for v in p])
     # Wt CSR: row i = column w_i
     wt = rows_to_csr([list(zip(ci, cv)) for ci, cv in wcols])
@@ -601,6 +667,7 @@ CASES = [
     ("convdiff5_sym", 5, "convdiff", (5.0, 5.0, 5.0), "SYM-LLK", 8, 0.05),
     ("convdiff6_stab", 6, "convdiff", (40.0, -25.0, 10.0), "STAB-LLK", 8, 0.05),
     ("convdiff4_stab_exact", 4, "convdiff", (20.0, 5.0, -15.0), "STAB-LLK", 64, 0.0),
+    ("convdiff6_mlk", 6, "convdiff", (40.0, -25.0, 10.0), "MLK", 4, 0.02),
 ]
 
 HAND_4x4 = [  # small nonsymmetric case worked by hand in the test
@@ -640,6 +707,31 @@ def rand_rows(seed, n, density):
         rows.append(e)
     return rows
 
+
+def tie_rows(seed, n, density):
+    """Nonsymmetric matrix whose values come from {-1, 1, -0.5, 0.5} (diagonal
+    4): equal magnitudes meet at the fill cap, where MLK's list sparsify
+    (psb_hsort) and LLK's magnitude heap keep different entries."""
+    u = splitmix_uniform(seed, n * n, 0.0, 1.0)
+    v = splitmix_uniform(seed + 1000, n * n, 0.0, 1.0)
+    vals = (-1.0, 1.0, -0.5, 0.5)
+    rows = []
+    for i in range(n):
+        e = []
+        for j in range(n):
+            if i == j:
+                e.append((j, 4.0))
+            elif u[i * n + j] < density:
+                e.append((j, vals[min(3, int(v[i * n + j] * 4))]))
+        rows.append(e)
+    return rows
+
+
+# name, seed, n, density, alg, fill_in, thresh
+TIE_CASES = [
+    ("mlk_ties20", 1, 20, 0.25, "MLK", 2, 0.0),
+    ("llk_ties20", 1, 20, 0.25, "LLK", 2, 0.0),
+]
 
 RAND_CASES = [
     # name, seed, n, density, solver, params
@@ -682,8 +774,20 @@ def main_inverse():
             solver=np.array(solver), params=np.array(p, np.float64)))
 
 
+def main_ties():
+    for name, seed, n, dens, alg, fill, thr in TIE_CASES:
+        rows = tie_rows(seed, n, dens)
+        a = rows_to_csr(rows)
+        wt, z, d = ainv_build(rows, alg, fill, thr)
+        save(name, rows, a, wt, z, d, dict(
+            meta=np.array([seed, 4, fill], np.int64), beta=np.zeros(3),
+            kind=np.array("ties"), density=np.array(dens), alg=np.array(alg),
+            thresh=np.array(thr)))
+
+
 def main():
     main_inverse()
+    main_ties()
     cases = [(c[0], pde3d(c[1], c[2], c[3]), c) for c in CASES]
     cases.append(("hand4", HAND_4x4, ("hand4", 0, "hand", (0, 0, 0), "LLK", 4, 0.0)))
     for name, rows, c in cases:

@@ -82,7 +82,7 @@ def test_host_build_matches_golden(path):
         np.testing.assert_array_equal(f[k], g[k], err_msg=k)
 
 
-@pytest.mark.parametrize("alg", ["LLK", "STAB-LLK"])
+@pytest.mark.parametrize("alg", ["LLK", "STAB-LLK", "MLK"])
 @pytest.mark.parametrize("idim,kind,beta,fill,thr", [
     (14, "convdiff", (10 / np.sqrt(3),) * 3, 20, 0.1),
     (11, "convdiff", (80.0, -30.0, 15.0), 6, 0.02),
@@ -251,3 +251,53 @@ def test_dump_writes_matrix_market(tmp_path):
     np.testing.assert_array_equal(W.indptr, f["wt_irp"])
     np.testing.assert_array_equal(Z.data, f["z_val"])
     np.testing.assert_array_equal(D, f["d"])
+
+
+def _tie_matrix(seed, n, density=0.25):
+    rng = np.random.default_rng(seed)
+    m = np.where(rng.random((n, n)) < density, rng.choice([-1.0, 1.0, -0.5, 0.5], (n, n)), 0.0)
+    np.fill_diagonal(m, 4.0)
+    irp, ja, val = [0], [], []
+    for r in range(n):
+        c = np.nonzero(m[r])[0]
+        ja += c.tolist()
+        val += m[r, c].tolist()
+        irp.append(len(ja))
+    return np.array(irp, np.int32), np.array(ja, np.int32), np.array(val)
+
+
+def test_mlk_differs_from_llk_only_at_ties():
+    """MLK (src/impl/mld_dsparse_biconjg_mlk.F90) walks the same steps as LLK
+    through sorted linked lists; only its sparsify (mld_d_sparsify_list with
+    psb_hsort) orders equal magnitudes differently.  On the PDE grid the two
+    agree; on matrices built from {+-1, +-0.5} they differ, and the product's
+    MLK still equals the oracle's literal linked-list restatement."""
+    irp, ja, val = ainv.pde.gen_pde3d(10, "convdiff", (-50.0, 20.0, -70.0))
+    f = {}
+    for alg in ("LLK", "MLK"):
+        sv = ainv.mld_d_ainv_solver_type()
+        assert sv.csetc("AINV_ALG", alg) == 0
+        sv.cseti("SUB_FILLIN", 20)
+        sv.csetr("SUB_ILUTHRS", 0.1)
+        assert sv.build(irp, ja, val) == 0
+        f[alg] = sv.factors()
+    for k in f["LLK"]:
+        np.testing.assert_array_equal(f["LLK"][k], f["MLK"][k], err_msg=k)
+    gm = np.load(os.path.join(GOLD, "mlk_ties20.npz"))
+    gl = np.load(os.path.join(GOLD, "llk_ties20.npz"))
+    assert not np.array_equal(gm["z_ja"], gl["z_ja"])
+    differ = 0
+    for seed in (1, 3, 4, 5, 6):
+        irp, ja, val = _tie_matrix(seed, 14 + seed)
+        n = len(irp) - 1
+        for fill, thr in ((2, 0.0), (3, 0.01)):
+            sv = ainv.mld_d_ainv_solver_type()
+            assert sv.csetc("AINV_ALG", "MLK") == 0
+            sv.cseti("SUB_FILLIN", fill)
+            sv.csetr("SUB_ILUTHRS", thr)
+            assert sv.build(irp, ja, val) == 0
+            om = O.ainv_build(O.CSR(n, irp, ja, val), "MLK", fill, thr)
+            ol = O.ainv_build(O.CSR(n, irp, ja, val), "LLK", fill, thr)
+            _factors_equal(sv.factors(), om)
+            differ += not np.array_equal(om.z.ja, ol.z.ja) or not np.array_equal(om.wt.ja, ol.wt.ja)
+    assert differ > 0
