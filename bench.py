@@ -161,13 +161,13 @@ def build_workload(idim=IDIM):
     return (irp, ja, val), sv
 
 
-def cpu_baseline_apply(f, n, budget_s=10.0, max_reps=200):
-    """Oracle apply ('N') on all host cores for a bounded sample."""
+def cpu_baseline_apply(f, n, budget_s=10.0, max_reps=200, threads=None):
+    """Oracle apply ('N') on all host cores (or `threads`) for a bounded sample."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     of = O.Factors(O.CSR(n, f["wt_irp"], f["wt_ja"], f["wt_val"]),
                    O.CSR(n, f["z_irp"], f["z_ja"], f["z_val"]), f["d"])
-    cores = os.cpu_count() or 1
+    cores = threads or os.cpu_count() or 1
     O.set_threads(cores)
     x = np.ascontiguousarray(np.random.default_rng(0).uniform(-1, 1, n))
     O.ainv_apply(of, x)  # warm
@@ -387,9 +387,13 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         dt, reps, cores = cpu_baseline_apply(f, n)
+        dt1, reps1, _ = cpu_baseline_apply(f, n, budget_s=5.0, max_reps=50, threads=1)
         cpu = {"value": round(B_csr / dt / 1e9, 3), "unit": "GB/s", "cores": cores, "kind": "port",
                "sample": f"{reps} full 200^3 applies ({dt * 1e3:.1f} ms each) of the CPU "
-                         "restatement of the reference apply, OpenMP over rows"}
+                         "restatement of the reference apply, OpenMP over rows",
+               "nproc": os.cpu_count(),
+               "one_thread": {"value": round(B_csr / dt1 / 1e9, 3), "unit": "GB/s",
+                              "ms_per_apply": round(dt1 * 1e3, 2), "applies": reps1}}
 
     if rank == 0:
         out = {"metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world,
