@@ -341,7 +341,12 @@ def main():
     torch.cuda.synchronize()
     st_ms = {s: sum(a.elapsed_time(b) for a, b in st[s]) / K2 for s in st}
     dom = max((1, 2), key=lambda s: st_ms[s])
-    dom_name = {1: "k_sweep_dscale", 2: "k_sweep_axpby"}[dom]
+    # FP64 sweep 1 runs the streaming kernel unless AINV_STREAM=0 forces the
+    # register family (AINV_STREAM=1 streams sweep 2 as well)
+    forced = os.environ.get("AINV_STREAM")
+    names = {1: "k_sweep_dscale" if forced == "0" else "k_stream_dscale",
+             2: "k_stream_axpby" if forced == "1" else "k_sweep_axpby"}
+    dom_name = names[dom]
     peak, peak_kind = measured_peaks()
     achieved = sb[dom - 1] / (st_ms[dom] * 1e-3) / 1e9
     traffic = recorded_traffic(dom_name)
@@ -418,8 +423,8 @@ def main():
                             "traffic": traffic, "algorithmic_bytes": sb[dom - 1],
                             "layout_bytes": lb[dom - 1],
                             "layout_frac": round(lb[dom - 1] / (st_ms[dom] * 1e-3) / 1e9 / peak, 4),
-                            "stage_ms": {"k_sweep_dscale": round(st_ms[1], 5),
-                                         "k_sweep_axpby": round(st_ms[2], 5)}},
+                            "stage_ms": {names[1]: round(st_ms[1], 5),
+                                         names[2]: round(st_ms[2], 5)}},
                "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
                "gpu_launches": 2 * K}
         out.update(extras)

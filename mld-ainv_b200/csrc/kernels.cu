@@ -149,15 +149,28 @@ int group_size(int prec) {
 }
 
 // Streaming (stream.cuh) is the default where it measured faster on B200 --
-// FP32 and BF16 factors; FP64 factors and the FP64 operator A use the
-// register kernels.  AINV_STREAM=0 / 1 forces one choice for every matrix.
-bool stream_enabled(int prec) {
+// FP32 and BF16 factors, and sweep 1 (the D^-1 epilogue) of FP64 factors
+// (0.095 vs 0.102 ms at 200^3); FP64 sweep 2 (0.141 vs 0.087 ms) and the FP64
+// operator A use the register kernels.  Both families sum the same products
+// in the same slot order.  AINV_STREAM=0 / 1 forces one choice for every
+// matrix.
+namespace {
+int stream_forced() {
   static const int forced = [] {
     const char *e = std::getenv("AINV_STREAM");
     return e ? (std::atoi(e) != 0 ? 1 : 0) : -1;
   }();
-  if (forced >= 0) return forced == 1;
+  return forced;
+}
+}  // namespace
+bool stream_enabled(int prec) {
+  if (stream_forced() >= 0) return stream_forced() == 1;
   return prec != AINV_PREC_FP64;
+}
+bool stream_enabled_sweep1(int prec) {
+  if (stream_forced() >= 0) return stream_forced() == 1;
+  (void)prec;
+  return true;
 }
 
 int sm_count() {
@@ -361,8 +374,9 @@ struct StreamLaunch {
 // Streaming launch when the layout allows it (returns false otherwise).
 template <class V, class X, class Epi>
 bool try_stream(const DevSell &m, const X *x, const Epi &epi, int *status, cudaStream_t s,
-                const int *stop) {
-  if (!status || !stream_enabled(m.prec)) return false;
+                const int *stop, bool sweep1 = false) {
+  if (!status || !(sweep1 ? stream_enabled_sweep1(m.prec) : stream_enabled(m.prec)))
+    return false;
   if ((reinterpret_cast<uintptr_t>(x) & 15u) != 0) return false;  // bulk copies need 16 B
   const RowVecs rv = host_row_vecs(epi);
   for (int i = 0; i < kMaxRowVecs; i++)
@@ -380,7 +394,7 @@ bool try_stream(const DevSell &m, const X *x, const Epi &epi, int *status, cudaS
 template <class V, class T>
 void sweep_dscale(const DevSell &m, const void *d, const double *x, void *t, cudaStream_t s,
                   const int *stop, int *status) {
-  if (try_stream<V>(m, x, EpiDscale<V, T>{(const V *)d, (T *)t}, status, s, stop)) return;
+  if (try_stream<V>(m, x, EpiDscale<V, T>{(const V *)d, (T *)t}, status, s, stop, true)) return;
   with_group_pack<V>(group_size(m.prec), m.pack, DscaleLaunch<V, T>{m, d, x, t, s, stop});
 }
 

@@ -564,6 +564,7 @@ int stream_plan(const DevSell &m, int xs, int nrv, StreamLayout &L, size_t &smem
 template <class V>
 constexpr int stream_rmax() { return sizeof(V) >= 8 ? 1 : (int)(8 / sizeof(V)); }
 bool stream_enabled(int prec);
+bool stream_enabled_sweep1(int prec);  // sweep 1 (t = D^-1 M x) of the apply
 int sm_count();
 // Allow `bytes` of dynamic shared memory for kernel; false if refused.
 bool set_smem_attr(const void *kernel, size_t bytes);
