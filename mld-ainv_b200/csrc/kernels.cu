@@ -20,6 +20,7 @@
 #include <cstdlib>
 #include <mutex>
 #include <map>
+#include <tuple>
 #include <utility>
 
 #include "stream.cuh"
@@ -150,7 +151,7 @@ int group_size(int prec) {
 
 // Streaming (stream.cuh) is the default where it measured faster on B200 --
 // FP32 and BF16 factors, and sweep 1 (the D^-1 epilogue) of FP64 factors
-// (0.095 vs 0.102 ms at 200^3); FP64 sweep 2 (0.141 vs 0.087 ms) and the FP64
+// (0.095 vs 0.102 ms at 200^3); FP64 sweep 2 (0.102 vs 0.086 ms) and the FP64
 // operator A use the register kernels.  Both families sum the same products
 // in the same slot order.  AINV_STREAM=0 / 1 forces one choice for every
 // matrix.
@@ -184,6 +185,32 @@ int sm_count() {
     sms[d] = v;
   }
   return sms[d];
+}
+
+int occupancy_grid(const void *kernel, int threads, size_t smem, int grid) {
+  // blocks of this kernel that fit on an SM at once (registers and shared
+  // memory), cached per kernel, shared memory size and device
+  static std::mutex mu;
+  static std::map<std::tuple<const void *, size_t, int>, int> cache;
+  int d = 0;
+  if (cudaGetDevice(&d) != cudaSuccess) d = 0;
+  int per_sm = 0;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find({kernel, smem, d});
+    if (it != cache.end()) per_sm = it->second;
+  }
+  if (per_sm == 0) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) !=
+            cudaSuccess ||
+        per_sm < 1) {
+      cudaGetLastError();
+      per_sm = 1;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    cache[{kernel, smem, d}] = per_sm;
+  }
+  return std::max(1, std::min(grid, per_sm * sm_count()));
 }
 
 bool set_smem_attr(const void *kernel, size_t bytes) {
@@ -365,7 +392,8 @@ struct StreamLaunch {
   void run() const {
     auto kern = k_stream<V, X, P, Epi>;
     if (!set_smem_attr((const void *)kern, smem)) return;
-    kern<<<grid, kStreamThreads, smem, s>>>(view<V>(m), m.stages, m.nstages, x, L, epi, status,
+    const int g = occupancy_grid((const void *)kern, kStreamThreads, smem, grid);
+    kern<<<g, kStreamThreads, smem, s>>>(view<V>(m), m.stages, m.nstages, x, L, epi, status,
                                             stop);
     *launched = true;
   }

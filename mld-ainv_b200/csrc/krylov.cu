@@ -352,7 +352,8 @@ struct StreamCgSweep2Launch {
   void run() const {
     auto kern = k_stream_cg_sweep2<V, T, P>;
     if (!set_smem_attr((const void *)kern, smem)) return;
-    kern<<<grid, kStreamThreads, smem, s>>>(view<V>(m), m.stages, m.nstages, L, (const T *)t, r,
+    const int g = occupancy_grid((const void *)kern, kStreamThreads, smem, grid);
+    kern<<<g, kStreamThreads, smem, s>>>(view<V>(m), m.stages, m.nstages, L, (const T *)t, r,
                                             z, st, partials);
     *launched = true;
   }
@@ -414,7 +415,8 @@ struct StreamDotsLaunch {
   void run() const {
     auto kern = k_stream_dots<MODE, P>;
     if (!set_smem_attr((const void *)kern, smem)) return;
-    kern<<<grid, kStreamThreads, smem, s>>>(view<double>(m), m.stages, m.nstages, L, x, y, w1,
+    const int g = occupancy_grid((const void *)kern, kStreamThreads, smem, grid);
+    kern<<<g, kStreamThreads, smem, s>>>(view<double>(m), m.stages, m.nstages, L, x, y, w1,
                                             w2, w3, st, pp);
     *launched = true;
   }

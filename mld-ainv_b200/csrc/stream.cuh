@@ -566,6 +566,10 @@ constexpr int stream_rmax() { return sizeof(V) >= 8 ? 1 : (int)(8 / sizeof(V)); 
 bool stream_enabled(int prec);
 bool stream_enabled_sweep1(int prec);  // sweep 1 (t = D^-1 M x) of the apply
 int sm_count();
+// A persistent grid of at most `grid` blocks, capped at the blocks of
+// `kernel` that can be resident at once (registers and shared memory), so
+// a kernel that needs more registers never runs a second partial wave.
+int occupancy_grid(const void *kernel, int threads, size_t smem, int grid);
 // Allow `bytes` of dynamic shared memory for kernel; false if refused.
 bool set_smem_attr(const void *kernel, size_t bytes);
 
