@@ -108,7 +108,8 @@ int ainv_gpu_apply_stage(ainv_handle *h, char trans, int stage, double alpha,
 /* Same on host arrays: copies x (and y when beta != 0) in, y out, and
  * returns when y is written.  Device staging is owned by h.  With page-locked
  * x and y (cudaHostAlloc / cudaHostRegister) the copies run chunk by chunk on
- * streams of h and overlap the sweeps; pageable arrays are copied whole. */
+ * streams of h and overlap the sweeps; pageable arrays, and x and y that
+ * overlap (x == y included), are copied whole. */
 int ainv_gpu_apply_host(ainv_handle *h, char trans, double alpha, const double *x,
                         double beta, double *y);
 int ainv_gpu_destroy(ainv_handle *h);

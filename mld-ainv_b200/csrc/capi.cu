@@ -351,8 +351,11 @@ int ainv_gpu_apply_host(ainv_handle *h, char trans, double alpha, const double *
   }
   const bool tr = (trans == 'T' || trans == 't' || trans == 'C' || trans == 'c');
   const int cs = host_chunk_slices(h->n);
-  if ((tr || trans == 'N' || trans == 'n') && h->wt.nslices > cs && page_locked(x) &&
-      page_locked(y))
+  // The pipelined forms write y while later chunks of x are still being read,
+  // so arrays that overlap take the serial form (copy all of x first).
+  const bool overlap = x < y + h->n && y < x + h->n;
+  if ((tr || trans == 'N' || trans == 'n') && h->wt.nslices > cs && !overlap &&
+      page_locked(x) && page_locked(y))
     return apply_host_chunked(h, tr, cs, alpha, x, beta, y);
   AINV_CUDA_TRY(cudaMemcpyAsync(h->xs, x, bytes, cudaMemcpyHostToDevice, 0));
   if (beta != 0.0) AINV_CUDA_TRY(cudaMemcpyAsync(h->ys, y, bytes, cudaMemcpyHostToDevice, 0));

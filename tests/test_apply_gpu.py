@@ -341,3 +341,19 @@ def test_repeated_host_apply_on_the_same_arrays(monkeypatch):
         df.apply_host(xp, alpha, beta, yp, trans)
         np.testing.assert_array_equal(yp.numpy(), _gpu_apply(df, x, alpha, beta, y0, trans),
                                       err_msg=f"call {k}")
+
+
+def test_host_apply_in_place(monkeypatch):
+    """x and y the same page-locked array (y = op(M) y): the call copies all
+    of x before writing y, so the result equals the out-of-place apply."""
+    irp, ja, val = ainv.pde.gen_pde3d(20, "convdiff", (2.0, -1.0, 3.0))
+    f = build_factors(irp, ja, val)
+    n = len(f["d"])
+    df = device_factors(f)
+    monkeypatch.setenv("AINV_HOST_CHUNK_ROWS", "512")
+    x = ainv.pde.rand_uniform(31, n)
+    for trans in "NT":
+        ref = _gpu_apply(df, x, 1.25, 0.0, np.zeros(n), trans)
+        buf = torch.from_numpy(x.copy()).pin_memory()
+        df.apply_host(buf, 1.25, 0.0, buf, trans)
+        np.testing.assert_array_equal(buf.numpy(), ref)
