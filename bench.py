@@ -386,6 +386,8 @@ def main():
     if not args.no_extras and world == 1:
         extras = run_extras(ainv, torch, dev, irp, ja, val, f, sv, flush, stream, ms)
         extras["block_cg"] = run_block_cg(ainv, torch, dev)
+        if not args.no_cpu:
+            extras["cpu_solves"] = run_cpu_solves(ainv, torch, dev, irp, ja, val, f, extras)
     if not args.no_serve and world == 1:
         extras["serving"] = run_serving(ainv, torch, args)
 
@@ -585,6 +587,84 @@ def run_variants(ainv, torch, dev, irp, ja, val, A, b, bn, xs, x, y, flush, stre
     return out
 
 
+def run_cpu_solves(ainv, torch, dev, irp, ja, val, f, extras):
+    """The CPU side of the solve configs, on all host cores with the oracle's
+    restated Krylov loop (FP64 factors: the CPU path has no other), next to
+    the GPU figure of the same config:
+      config 1: 40^3 Poisson (6/-1), b = A*1, x0 = 0, AINV drop 0.1 fill 20, CG to 1e-9;
+      config 2: the 200^3 convection-diffusion system of the solve leg, BiCGSTAB to 1e-9;
+      config 4: one of the 32 right-hand sides of the block leg (128^3 Poisson, CG to
+                1e-9); 32 sequential CPU solves are 32 x that time."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+
+    def factors(d):
+        m = len(d["d"])
+        return O.Factors(O.CSR(m, d["wt_irp"], d["wt_ja"], d["wt_val"]),
+                         O.CSR(m, d["z_irp"], d["z_ja"], d["z_val"]), d["d"])
+
+    def cpu(method, a_irp, a_ja, a_val, fd, b):
+        a = O.CSR(len(a_irp) - 1, a_irp, a_ja, a_val)
+        t = time.perf_counter()
+        _, it, err, rc = O.solve(method, a, factors(fd), b, eps=1e-9, itmax=3000)
+        return {"s_per_solve": round(time.perf_counter() - t, 4), "iters": it,
+                "relres": err, "info": rc}
+
+    def build(i, j, v):
+        sv = ainv.mld_d_ainv_solver_type()
+        sv.cseti("SUB_FILLIN", FILL)
+        sv.csetr("SUB_ILUTHRS", THRESH)
+        assert sv.build(i, j, v) == 0, ainv.last_error()
+        return sv.factors()
+
+    out = {"threads": cores, "kind": "port"}
+    # config 1
+    i1, j1, v1 = ainv.pde.gen_pde3d(40, "poisson")
+    f1 = build(i1, j1, v1)
+    n1 = len(i1) - 1
+    b1 = O.spmv(O.CSR(n1, i1, j1, v1), np.ones(n1))
+    A1 = ainv.DeviceOperator(i1, j1, v1)
+    d1 = ainv.DeviceFactors((f1["wt_irp"], f1["wt_ja"], f1["wt_val"]),
+                            (f1["z_irp"], f1["z_ja"], f1["z_val"]), f1["d"])
+    bt = torch.from_numpy(b1).to(dev)
+    gpu_t = []
+    for _ in range(4):
+        xg = torch.zeros(n1, dtype=torch.float64, device=dev)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        r = A1.solve(bt, xg, d1, "CG", 1e-9, 3000)
+        torch.cuda.synchronize()
+        gpu_t.append(time.perf_counter() - t)
+    c1 = cpu("CG", i1, j1, v1, f1, b1)
+    out["config1_poisson40_cg"] = {"cpu": c1, "gpu": {"s_per_solve": round(min(gpu_t[1:]), 5),
+                                                      "iters": r.iter, "relres": r.err},
+                                   "gpu_speedup": round(c1["s_per_solve"] / min(gpu_t[1:]), 2)}
+    d1.close()
+    A1.close()
+    # config 2
+    n = len(irp) - 1
+    xs = ainv.pde.rand_uniform(0, n)
+    b2 = O.spmv(O.CSR(n, irp, ja, val), xs)
+    c2 = cpu("BICGSTAB", irp, ja, val, f, b2)
+    g2 = extras.get("solve", {}).get("FP64", {}).get("s_per_solve")
+    out["config2_convdiff200_bicgstab"] = {"cpu": c2, "gpu_s_per_solve": g2,
+                                           "gpu_speedup": round(c2["s_per_solve"] / g2, 2)
+                                           if g2 else None}
+    # config 4
+    i4, j4, v4 = ainv.pde.gen_pde3d(128, "poisson")
+    f4 = build(i4, j4, v4)
+    b4 = ainv.pde.rand_normal(0, len(i4) - 1)
+    c4 = cpu("CG", i4, j4, v4, f4, b4)
+    gb = extras.get("block_cg", {}).get("s_per_block_solve")
+    out["config4_poisson128_cg_per_rhs"] = {
+        "cpu": c4, "cpu_32_sequential_s": round(32 * c4["s_per_solve"], 2),
+        "gpu_block_s": gb,
+        "gpu_speedup": round(32 * c4["s_per_solve"] / gb, 2) if gb else None}
+    return out
+
+
 def run_block_cg(ainv, torch, dev, idim=128, m=32, itmax=2000, reps=3, single=True):
     """Multi-right-hand-side CG: 3-D Poisson on a 128^3 grid, 32 right-hand
     sides N(0,1) (seed k for column k), AINV drop 0.1 fill 20 with FP32
@@ -685,7 +765,7 @@ def run_serving(ainv, torch, args):
     from ainv import serve, workload
     specs = workload.serving_operators()
     t0 = time.perf_counter()
-    ops = []
+    ops, host = [], []
     for sp in specs:
         irp, ja, val = ainv.pde.gen_pde3d(sp.idim, sp.kind, sp.beta)
         sv = ainv.mld_d_ainv_solver_type()
@@ -697,6 +777,7 @@ def run_serving(ainv, torch, args):
                     ainv.DeviceFactors((f["wt_irp"], f["wt_ja"], f["wt_val"]),
                                        (f["z_irp"], f["z_ja"], f["z_val"]), f["d"],
                                        prec=args.serve_prec), sp.n))
+        host.append((irp, ja, val, f))
     t_build = time.perf_counter() - t0
     nreq = args.serve_requests
     opsel = workload.request_ops(nreq, len(ops))
@@ -741,7 +822,26 @@ def run_serving(ainv, torch, args):
     for a, f, _ in ops:
         f.close()
         a.close()
-    return {"operators": [{"idim": sp.idim, "kind": sp.kind,
+    cpu = None
+    if not args.no_cpu:
+        # the same requests solved one after another on the host cores (the
+        # oracle's restated BiCGSTAB, FP64 factors), for up to 15 s
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        O.set_threads(os.cpu_count() or 1)
+        t, done = time.perf_counter(), 0
+        while done < nreq and time.perf_counter() - t < 15.0:
+            hi, hj, hv, hf = host[opsel[done]]
+            m = len(hi) - 1
+            O.solve("BICGSTAB", O.CSR(m, hi, hj, hv),
+                    O.Factors(O.CSR(m, hf["wt_irp"], hf["wt_ja"], hf["wt_val"]),
+                              O.CSR(m, hf["z_irp"], hf["z_ja"], hf["z_val"]), hf["d"]),
+                    rhs[done].numpy(), eps=1e-8, itmax=2000)
+            done += 1
+        cpu = {"requests": done, "solves_per_s": round(done / (time.perf_counter() - t), 2),
+               "threads": os.cpu_count() or 1, "kind": "port",
+               "sample": "the first requests of the stream, solved one after another"}
+    return {"cpu_sequential": cpu, "operators": [{"idim": sp.idim, "kind": sp.kind,
                            "beta": [round(b, 3) for b in sp.beta]} for sp in specs],
             "factors": f"AINV LLK drop 0.1 fill 20, {args.serve_prec}", "tol": 1e-8,
             "slots": args.serve_slots, "iters_per_launch": args.serve_iters,
