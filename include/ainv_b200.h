@@ -109,7 +109,8 @@ int ainv_gpu_apply_stage(ainv_handle *h, char trans, int stage, double alpha,
  * returns when y is written.  Device staging is owned by h.  With page-locked
  * x and y (cudaHostAlloc / cudaHostRegister) the copies run chunk by chunk on
  * streams of h and overlap the sweeps; pageable arrays, and x and y that
- * overlap (x == y included), are copied whole. */
+ * overlap (x == y included), are copied whole.  y is written by the device:
+ * do not register it with cudaHostRegisterReadOnly. */
 int ainv_gpu_apply_host(ainv_handle *h, char trans, double alpha, const double *x,
                         double beta, double *y);
 int ainv_gpu_destroy(ainv_handle *h);

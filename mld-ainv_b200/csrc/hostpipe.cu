@@ -273,6 +273,15 @@ bool host_pipe_usable(const ainv_handle *h, bool tr, const double *y) {
     cudaGetLastError();
     return false;
   }
+  // the kernel stores into y, so y must not be registered read-only (a
+  // contract of every form, which all write y from the device); where the
+  // runtime reports the flags, such a y is sent to the other forms
+  unsigned flags = 0;
+  if (cudaHostGetFlags(&flags, (void *)y) == cudaSuccess) {
+    if (flags & cudaHostRegisterReadOnly) return false;
+  } else {
+    cudaGetLastError();
+  }
   return true;
 }
 
