@@ -467,6 +467,24 @@ def run_extras(ainv, torch, dev, irp, ja, val, f, sv, flush, stream, fp64_ms):
                               "layout_GBps": round(Bl / (ms * 1e-3) / 1e9, 2),
                               "speedup_vs_fp64": round(fp64_ms / ms, 3)}
         df.close()
+    # the transposed apply y = W D^-1 Z^T x (trans 'T'), FP64 factors: same
+    # algorithmic bytes as 'N' (Z^T has nnz_Z entries, W has nnz_W)
+    df = sv.device
+    for _ in range(5):
+        df.apply(x, y, 1.0, 0.0, "T", stream)
+    evs = []
+    for _ in range(50):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        df.apply(x, y, 1.0, 0.0, "T", stream)
+        b.record(stream)
+        evs.append((a, b))
+    torch.cuda.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in evs) / len(evs)
+    Bt = csr_apply_bytes(n, nnz[1], nnz[0], sv=8, sd=8, st=8)
+    out["trans_T"] = {"ms": round(ms, 5), "GB/s": round(Bt / (ms * 1e-3) / 1e9, 2),
+                      "bytes": Bt, "vs_N": round(fp64_ms / ms, 3)}
     # BiCGSTAB to 1e-9, b = A x*, x* ~ U(-1,1) seed 0
     A = ainv.DeviceOperator(irp, ja, val)
     xs = torch.from_numpy(ainv.pde.rand_uniform(0, n)).to(dev)
