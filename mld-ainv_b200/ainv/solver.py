@@ -17,7 +17,7 @@ import ctypes as C
 import numpy as np
 
 from ._lib import PREC, SUCCESS, lib, last_error
-from .device import DeviceFactors, _stream, dptr
+from .device import DeviceFactors, _is_cpu_tensor, _stream, _torch, dptr
 
 
 class _SolverType:
@@ -97,7 +97,20 @@ class _SolverType:
                                         trans.encode()[:1], _stream(stream))
 
     def apply_a(self, alpha, x, beta, y, trans: str = "N") -> int:
-        """apply_a: host arrays; y (float64, contiguous) is updated in place."""
+        """apply_a: host arrays; y (float64, contiguous) is updated in place.
+        x and y are numpy arrays or CPU torch tensors; with page-locked
+        tensors (``tensor.pin_memory()``) the transfers overlap the sweeps."""
+        if _is_cpu_tensor(y):
+            if not _is_cpu_tensor(x):
+                raise TypeError("x must be a CPU tensor when y is one")
+            for v in (x, y):
+                if v.dtype != _torch().float64 or not v.is_contiguous():
+                    raise TypeError("x and y must be contiguous float64 tensors")
+            if x.numel() != y.numel():
+                raise TypeError("x and y differ in length")
+            return lib().mld_d_solver_apply_host(self._h, float(alpha), C.c_void_p(x.data_ptr()),
+                                                 float(beta), C.c_void_p(y.data_ptr()),
+                                                 trans.encode()[:1])
         x = np.ascontiguousarray(x, np.float64)
         if not (isinstance(y, np.ndarray) and y.dtype == np.float64 and y.flags.c_contiguous):
             raise TypeError("y must be a contiguous float64 numpy array")

@@ -233,6 +233,15 @@ def test_apply_requires_device_factors():
     assert sv.build(irp, ja, val) == 0
     y = np.zeros(64)
     assert sv.apply_a(1.0, np.ones(64), 0.0, y) == ainv._lib.ERR_NOT_BUILT
+    torch = pytest.importorskip("torch")
+    xt, yt = torch.ones(64, dtype=torch.float64), torch.zeros(64, dtype=torch.float64)
+    assert sv.apply_a(1.0, xt, 0.0, yt) == ainv._lib.ERR_NOT_BUILT
+    with pytest.raises(TypeError):
+        sv.apply_a(1.0, np.ones(64), 0.0, yt)               # mixed array kinds
+    with pytest.raises(TypeError):
+        sv.apply_a(1.0, xt.float(), 0.0, yt)                # not float64
+    with pytest.raises(TypeError):
+        sv.apply_a(1.0, xt[:32], 0.0, yt)                   # lengths differ
 
 
 def test_dump_writes_matrix_market(tmp_path):
