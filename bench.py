@@ -606,13 +606,16 @@ def run_variants(ainv, torch, dev, irp, ja, val, A, b, bn, xs, x, y, flush, stre
 
 
 def run_cpu_solves(ainv, torch, dev, irp, ja, val, f, extras):
-    """The CPU side of the solve configs, on all host cores with the oracle's
-    restated Krylov loop (FP64 factors: the CPU path has no other), next to
-    the GPU figure of the same config:
-      config 1: 40^3 Poisson (6/-1), b = A*1, x0 = 0, AINV drop 0.1 fill 20, CG to 1e-9;
-      config 2: the 200^3 convection-diffusion system of the solve leg, BiCGSTAB to 1e-9;
-      config 4: one of the 32 right-hand sides of the block leg (128^3 Poisson, CG to
-                1e-9); 32 sequential CPU solves are 32 x that time."""
+    """The CPU side of the solve workloads, on all host cores with the
+    oracle's restated Krylov loop (FP64 factors: the CPU path has no other),
+    next to the GPU figure of the same workload:
+      poisson40_cg: 40^3 Poisson (6/-1), b = A*1, x0 = 0, AINV drop 0.1 fill 20,
+                    CG to 1e-9;
+      convdiff200_bicgstab: the 200^3 convection-diffusion system of the solve
+                    leg, BiCGSTAB to 1e-9;
+      poisson128_cg_per_rhs: one of the 32 right-hand sides of the block leg
+                    (128^3 Poisson, CG to 1e-9); 32 sequential CPU solves are
+                    32 x that time."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     cores = os.cpu_count() or 1
@@ -638,7 +641,7 @@ def run_cpu_solves(ainv, torch, dev, irp, ja, val, f, extras):
         return sv.factors()
 
     out = {"threads": cores, "kind": "port"}
-    # config 1
+    # 40^3 Poisson, CG
     i1, j1, v1 = ainv.pde.gen_pde3d(40, "poisson")
     f1 = build(i1, j1, v1)
     n1 = len(i1) - 1
@@ -656,27 +659,27 @@ def run_cpu_solves(ainv, torch, dev, irp, ja, val, f, extras):
         torch.cuda.synchronize()
         gpu_t.append(time.perf_counter() - t)
     c1 = cpu("CG", i1, j1, v1, f1, b1)
-    out["config1_poisson40_cg"] = {"cpu": c1, "gpu": {"s_per_solve": round(min(gpu_t[1:]), 5),
+    out["poisson40_cg"] = {"cpu": c1, "gpu": {"s_per_solve": round(min(gpu_t[1:]), 5),
                                                       "iters": r.iter, "relres": r.err},
                                    "gpu_speedup": round(c1["s_per_solve"] / min(gpu_t[1:]), 2)}
     d1.close()
     A1.close()
-    # config 2
+    # 200^3 convection-diffusion, BiCGSTAB
     n = len(irp) - 1
     xs = ainv.pde.rand_uniform(0, n)
     b2 = O.spmv(O.CSR(n, irp, ja, val), xs)
     c2 = cpu("BICGSTAB", irp, ja, val, f, b2)
     g2 = extras.get("solve", {}).get("FP64", {}).get("s_per_solve")
-    out["config2_convdiff200_bicgstab"] = {"cpu": c2, "gpu_s_per_solve": g2,
+    out["convdiff200_bicgstab"] = {"cpu": c2, "gpu_s_per_solve": g2,
                                            "gpu_speedup": round(c2["s_per_solve"] / g2, 2)
                                            if g2 else None}
-    # config 4
+    # 128^3 Poisson, one of the block leg's right-hand sides
     i4, j4, v4 = ainv.pde.gen_pde3d(128, "poisson")
     f4 = build(i4, j4, v4)
     b4 = ainv.pde.rand_normal(0, len(i4) - 1)
     c4 = cpu("CG", i4, j4, v4, f4, b4)
     gb = extras.get("block_cg", {}).get("s_per_block_solve")
-    out["config4_poisson128_cg_per_rhs"] = {
+    out["poisson128_cg_per_rhs"] = {
         "cpu": c4, "cpu_32_sequential_s": round(32 * c4["s_per_solve"], 2),
         "gpu_block_s": gb,
         "gpu_speedup": round(32 * c4["s_per_solve"] / gb, 2) if gb else None}
