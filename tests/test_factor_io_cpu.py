@@ -86,3 +86,22 @@ def test_cache_round_trip_and_checks(tmp_path):
     open(bad, "wb").write(bytes(raw[:100]))
     assert other.restore(bad) == ainv._lib.ERR_ARG
     assert ainv.mld_d_ainv_solver_type().save(path) == ainv._lib.ERR_NOT_BUILT
+
+
+@pytest.mark.parametrize("alg", ["STAB-LLK", "MLK"])
+def test_cache_keeps_the_biconjugation_variant(tmp_path, alg):
+    """AINV factors of the STAB-LLK / MLK variants: the cache restores the
+    factors bit for bit and the variant with them (descr names it)."""
+    irp, ja, val = ainv.pde.gen_pde3d(7, "convdiff", (12.0, -4.0, 3.0))
+    sv = ainv.mld_d_ainv_solver_type()
+    assert sv.csetc("AINV_ALG", alg) == 0
+    sv.cseti("SUB_FILLIN", 6)
+    sv.csetr("SUB_ILUTHRS", 0.05)
+    assert sv.build(irp, ja, val) == 0
+    path = str(tmp_path / "f.bin")
+    assert sv.save(path) == 0
+    other = ainv.mld_d_ainv_solver_type()
+    assert other.restore(path) == 0
+    _same(sv.factors(), other.factors())
+    assert other.descr() == sv.descr()
+    assert {"STAB-LLK": "Stabilized", "MLK": "list merge"}[alg] in other.descr()
