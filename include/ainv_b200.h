@@ -247,9 +247,13 @@ int mld_d_solver_load(mld_d_solver *sv, const char *prefix);
  * the reference; it skips the host build when factors are reused. */
 int mld_d_solver_save(const mld_d_solver *sv, const char *path);
 int mld_d_solver_restore(mld_d_solver *sv, const char *path);
-/* update(x) of the plugin type: the device update_a on the uploaded factors
- * (x: n host doubles), the new d copied back to the host factors. */
-int mld_d_solver_update_a(mld_d_solver *sv, const double *x);
+/* update(x) of the plugin type (src/impl/mld_d_base_ainv_update_a.f90:35-79):
+ * the device update_a on the uploaded factors, x being nx host doubles.
+ * As in the reference (:54-58, info = -1 when size(x) < size(d)), nx < n is
+ * an argument error and nothing is read.  The new d is formed in FP64 from
+ * the host's FP64 d whatever the device precision, stored in the host
+ * factors and uploaded rounded to the device precision. */
+int mld_d_solver_update_a(mld_d_solver *sv, const double *x, int nx);
 /* MatrixMarket dump of W^T, D^-1 and Z as <prefix>_wmat.mtx,
  * <prefix>_diag.mtx, <prefix>_zmat.mtx. */
 int mld_d_solver_dump(const mld_d_solver *sv, const char *prefix);

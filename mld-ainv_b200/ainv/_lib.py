@@ -56,7 +56,7 @@ SIGNATURES = [
     ("ainv_csr_solve_info", _i, [_vp, _ip, _ip]),
     ("ainv_gpu_solve", _i, [_vp, _vp, _vp, _vp, _i, _d, _i, _ip, _dp, _vp]),
     ("ainv_gpu_update_a", _i, [_vp, _vp, _vp, _vp]),
-    ("mld_d_solver_update_a", _i, [_vp, _vp]),
+    ("mld_d_solver_update_a", _i, [_vp, _vp, _i]),
     ("mld_d_solver_load", _i, [_vp, C.c_char_p]),
     ("mld_d_solver_save", _i, [_vp, C.c_char_p]),
     ("mld_d_solver_restore", _i, [_vp, C.c_char_p]),

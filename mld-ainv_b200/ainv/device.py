@@ -17,11 +17,38 @@ def _np(a, dtype):
     return np.ascontiguousarray(a, dtype=dtype)
 
 
-def dptr(t) -> C.c_void_p:
-    """Device address of a CUDA tensor (float64, contiguous)."""
-    if not t.is_cuda or not t.is_contiguous():
-        raise ValueError("expected a contiguous CUDA tensor")
+def dptr(t, n: int, name: str = "vector") -> C.c_void_p:
+    """Device address of `t` once it is known to be a contiguous float64
+    CUDA tensor of at least n entries.  The kernels read or write n entries
+    through the raw address, so a strided or single-precision tensor
+    (TypeError) or a short one (ValueError) is rejected here, before any
+    call reaches the library."""
+    if not (_is_tensor(t) and t.is_cuda):
+        raise TypeError(f"{name}: expected a CUDA tensor")
+    if t.dtype != _torch().float64 or not t.is_contiguous():
+        raise TypeError(f"{name}: expected a contiguous float64 tensor")
+    if t.numel() < n:
+        raise ValueError(f"{name}: {t.numel()} entries, {n} needed")
     return C.c_void_p(t.data_ptr())
+
+
+def hptr(a, n: int, name: str = "array") -> C.c_void_p:
+    """Host address of a numpy array or CPU tensor once it is known to be
+    contiguous float64 with at least n entries (the library reads or writes
+    n entries through it, from the CPU or from a kernel over PCIe)."""
+    if _is_cpu_tensor(a):
+        if a.dtype != _torch().float64 or not a.is_contiguous():
+            raise TypeError(f"{name}: expected a contiguous float64 tensor")
+        size, addr = a.numel(), a.data_ptr()
+    elif isinstance(a, np.ndarray):
+        if a.dtype != np.float64 or not a.flags.c_contiguous:
+            raise TypeError(f"{name}: expected a contiguous float64 array")
+        size, addr = a.size, a.ctypes.data
+    else:
+        raise TypeError(f"{name}: expected a numpy array or a CPU tensor, got {type(a)}")
+    if size < n:
+        raise ValueError(f"{name}: {size} entries, {n} needed")
+    return C.c_void_p(addr)
 
 
 def _stream(s):
@@ -35,9 +62,13 @@ def _torch():
     return torch
 
 
-def _is_cpu_tensor(a) -> bool:
+def _is_tensor(a) -> bool:
     t = type(a)
-    return t.__module__.startswith("torch") and t.__name__ == "Tensor" and a.device.type == "cpu"
+    return t.__module__.startswith("torch") and t.__name__ in ("Tensor", "Parameter")
+
+
+def _is_cpu_tensor(a) -> bool:
+    return _is_tensor(a) and a.device.type == "cpu"
 
 
 class DeviceFactors:
@@ -73,20 +104,25 @@ class DeviceFactors:
 
     def apply(self, x, y, alpha=1.0, beta=0.0, trans="N", stream=None) -> None:
         """y = alpha * Z D^-1 W^T x + beta * y (trans 'N'), device tensors."""
-        check(lib().ainv_gpu_apply(self._h, trans.encode()[:1], alpha, dptr(x), beta, dptr(y),
-                                   _stream(stream)))
+        n = self.n
+        check(lib().ainv_gpu_apply(self._h, trans.encode()[:1], alpha, dptr(x, n, "x"), beta,
+                                   dptr(y, n, "y"), _stream(stream)))
 
     def apply_stage(self, stage, x=None, y=None, alpha=1.0, beta=0.0, trans="N", stream=None):
         """Run sweep 1 (t = D^-1 W^T x) or sweep 2 (y = alpha Z t + beta y) alone."""
+        n = self.n
         check(lib().ainv_gpu_apply_stage(self._h, trans.encode()[:1], int(stage), alpha,
-                                         dptr(x) if x is not None else None, beta,
-                                         dptr(y) if y is not None else None, _stream(stream)))
+                                         dptr(x, n, "x") if x is not None else None, beta,
+                                         dptr(y, n, "y") if y is not None else None,
+                                         _stream(stream)))
 
     def update_a(self, x, d_out=None, stream=None) -> None:
         """update_a on the device: d <- 1/(1/d + diag(W^T diag(x) Z)); x a
         CUDA float64 tensor of n entries, d_out (optional) receives the new d
         in FP64."""
-        check(lib().ainv_gpu_update_a(self._h, dptr(x), dptr(d_out) if d_out is not None else None,
+        n = self.n
+        check(lib().ainv_gpu_update_a(self._h, dptr(x, n, "x"),
+                                      dptr(d_out, n, "d_out") if d_out is not None else None,
                                       _stream(stream)))
 
     def apply_host(self, x, alpha=1.0, beta=0.0, y=None, trans="N"):
@@ -95,20 +131,17 @@ class DeviceFactors:
         float64 CPU torch tensors (y written in place and returned).  With
         page-locked tensors (``tensor.pin_memory()``) the copies overlap the
         sweeps chunk by chunk."""
+        n = self.n
         if _is_cpu_tensor(x):
             if y is None or not _is_cpu_tensor(y):
                 raise ValueError("apply_host: y must be a CPU tensor when x is one")
-            for v in (x, y):
-                if v.dtype != _torch().float64 or not v.is_contiguous() or v.numel() != self.n:
-                    raise ValueError("apply_host: tensors must be contiguous float64 of n entries")
             check(lib().ainv_gpu_apply_host(self._h, trans.encode()[:1], alpha,
-                                            C.c_void_p(x.data_ptr()), beta,
-                                            C.c_void_p(y.data_ptr())))
+                                            hptr(x, n, "x"), beta, hptr(y, n, "y")))
             return y
         x = _np(x, np.float64)
         y = np.zeros_like(x) if y is None else _np(y, np.float64).copy()
-        check(lib().ainv_gpu_apply_host(self._h, trans.encode()[:1], alpha,
-                                        C.c_void_p(x.ctypes.data), beta, C.c_void_p(y.ctypes.data)))
+        check(lib().ainv_gpu_apply_host(self._h, trans.encode()[:1], alpha, hptr(x, n, "x"), beta,
+                                        hptr(y, n, "y")))
         return y
 
     def check(self) -> None:
@@ -190,7 +223,8 @@ class DeviceOperator:
         check(lib().ainv_csr_check(self._h))
 
     def spmv(self, x, y, alpha=1.0, beta=0.0, stream=None) -> None:
-        check(lib().ainv_csr_spmv(self._h, alpha, dptr(x), beta, dptr(y), _stream(stream)))
+        check(lib().ainv_csr_spmv(self._h, alpha, dptr(x, self.n, "x"), beta,
+                                  dptr(y, self.n, "y"), _stream(stream)))
 
     def solve(self, b, x, factors: DeviceFactors | None = None, method="BICGSTAB", eps=1e-9,
               itmax=1000, stream=None) -> SolveResult:
@@ -198,7 +232,8 @@ class DeviceOperator:
         Returns the status instead of raising for NOCONV / breakdown."""
         it, err = C.c_int(0), C.c_double(0.0)
         info = lib().ainv_gpu_solve(factors.handle if factors is not None else None, self._h,
-                                    dptr(b), dptr(x), KRYLOV[method.upper()], eps, itmax,
+                                    dptr(b, self.n, "b"), dptr(x, self.n, "x"),
+                                    KRYLOV[method.upper()], eps, itmax,
                                     C.byref(it), C.byref(err), _stream(stream))
         if info not in (SUCCESS, 4102, 4103, 4104):
             check(info)
@@ -214,12 +249,15 @@ class DeviceOperator:
         solutions.  Statuses are returned per column instead of raised."""
         if B.dim() != 2 or B.shape != X.shape or B.shape[0] != self.n:
             raise ValueError("B and X must both have shape (n, m)")
+        if factors is not None and factors.n != self.n:
+            raise ValueError("block_solve: preconditioner and operator sizes differ")
         m = B.shape[1]
         it = (C.c_int * m)()
         err = (C.c_double * m)()
         st = (C.c_int * m)()
         info = lib().ainv_gpu_block_solve(factors.handle if factors is not None else None,
-                                          self._h, m, dptr(B), m, dptr(X), m, eps, itmax, it,
+                                          self._h, m, dptr(B, self.n * m, "B"), m,
+                                          dptr(X, self.n * m, "X"), m, eps, itmax, it,
                                           err, st, _stream(stream))
         if info not in (SUCCESS, 4102, 4103, 4104):
             check(info)

@@ -15,7 +15,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from ._lib import Result, ServerInfo, check, lib
-from .device import DeviceFactors, DeviceOperator
+from .device import DeviceFactors, DeviceOperator, hptr
 
 
 @dataclass
@@ -60,19 +60,24 @@ class SolveServer:
         self._h = h
         self._keep = []       # operators / factors referenced by the server
         self._buffers = {}    # id -> (b, x) kept alive until wait
+        self._rows = {}       # operator -> rows (length of its b and x)
 
     def add_operator(self, a: DeviceOperator, f: DeviceFactors) -> int:
         op = C.c_int(0)
         check(lib().ainv_server_add_operator(self._h, a.handle, f.handle, C.byref(op)))
         self._keep.append((a, f))
+        self._rows[op.value] = a.n
         return op.value
 
     def submit(self, op: int, b, x, eps: float = 1e-8, itmax: int = 1000) -> int:
         """Queue A_op x = b.  b and x are host float64 buffers (numpy arrays
         or pinned torch tensors) kept alive here until `wait`."""
         rid = C.c_longlong(0)
-        check(lib().ainv_server_submit(self._h, op, C.c_void_p(_host_ptr(b)),
-                                       C.c_void_p(_host_ptr(x)), eps, itmax, C.byref(rid)))
+        n = self._rows.get(op)
+        if n is None:
+            raise ValueError(f"unknown operator {op}")
+        check(lib().ainv_server_submit(self._h, op, hptr(b, n, "b"), hptr(x, n, "x"), eps,
+                                       itmax, C.byref(rid)))
         self._buffers[rid.value] = (b, x)
         return rid.value
 
@@ -110,13 +115,3 @@ class SolveServer:
             pass
 
 
-def _host_ptr(a) -> int:
-    if isinstance(a, np.ndarray):
-        if a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]:
-            raise ValueError("host buffers must be contiguous float64")
-        return a.ctypes.data
-    if hasattr(a, "data_ptr"):
-        if a.is_cuda:
-            raise ValueError("the server takes host buffers")
-        return a.data_ptr()
-    raise TypeError(f"unsupported buffer {type(a)}")

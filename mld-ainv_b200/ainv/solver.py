@@ -17,7 +17,7 @@ import ctypes as C
 import numpy as np
 
 from ._lib import PREC, SUCCESS, lib, last_error
-from .device import DeviceFactors, _is_cpu_tensor, _stream, _torch, dptr
+from .device import DeviceFactors, _is_cpu_tensor, _stream, dptr, hptr
 
 
 class _SolverType:
@@ -87,36 +87,45 @@ class _SolverType:
 
     def update_a(self, x) -> int:
         """update(x) of the plugin type (shifted system A + diag(x)) on the
-        uploaded factors; the host d follows."""
+        uploaded factors; the host d follows.  Like the reference, x shorter
+        than the factors' n is an argument error (info != 0)."""
         x = np.ascontiguousarray(x, np.float64)
-        return lib().mld_d_solver_update_a(self._h, C.c_void_p(x.ctypes.data))
+        return lib().mld_d_solver_update_a(self._h, C.c_void_p(x.ctypes.data), x.size)
+
+    def _n(self) -> int | None:
+        """Rows of the factors: the device copy's, else the host build's,
+        else None (nothing built)."""
+        h = lib().mld_d_solver_handle(self._h)
+        if h:
+            return lib().ainv_gpu_get_n(C.c_void_p(h))
+        n = C.c_int(0)
+        if lib().mld_d_solver_get_factors(self._h, C.byref(n), None, None,
+                                          *([None] * 7)) == SUCCESS:
+            return n.value
+        return None
 
     def apply(self, alpha, x, beta, y, trans: str = "N", stream=None) -> int:
-        """apply_v: y = alpha * M x + beta * y on device tensors."""
-        return lib().mld_d_solver_apply(self._h, float(alpha), dptr(x), float(beta), dptr(y),
-                                        trans.encode()[:1], _stream(stream))
+        """apply_v: y = alpha * M x + beta * y on device tensors (float64,
+        contiguous, at least n entries each)."""
+        n = self._n() or 0
+        return lib().mld_d_solver_apply(self._h, float(alpha), dptr(x, n, "x"), float(beta),
+                                        dptr(y, n, "y"), trans.encode()[:1], _stream(stream))
 
     def apply_a(self, alpha, x, beta, y, trans: str = "N") -> int:
         """apply_a: host arrays; y (float64, contiguous) is updated in place.
-        x and y are numpy arrays or CPU torch tensors; with page-locked
-        tensors (``tensor.pin_memory()``) the transfers overlap the sweeps."""
+        x and y are numpy arrays or CPU torch tensors of at least n entries;
+        with page-locked tensors (``tensor.pin_memory()``) the transfers
+        overlap the sweeps."""
         if _is_cpu_tensor(y):
             if not _is_cpu_tensor(x):
                 raise TypeError("x must be a CPU tensor when y is one")
-            for v in (x, y):
-                if v.dtype != _torch().float64 or not v.is_contiguous():
-                    raise TypeError("x and y must be contiguous float64 tensors")
-            if x.numel() != y.numel():
-                raise TypeError("x and y differ in length")
-            return lib().mld_d_solver_apply_host(self._h, float(alpha), C.c_void_p(x.data_ptr()),
-                                                 float(beta), C.c_void_p(y.data_ptr()),
-                                                 trans.encode()[:1])
-        x = np.ascontiguousarray(x, np.float64)
-        if not (isinstance(y, np.ndarray) and y.dtype == np.float64 and y.flags.c_contiguous):
-            raise TypeError("y must be a contiguous float64 numpy array")
-        return lib().mld_d_solver_apply_host(self._h, float(alpha), C.c_void_p(x.ctypes.data),
-                                             float(beta), C.c_void_p(y.ctypes.data),
-                                             trans.encode()[:1])
+        elif isinstance(y, np.ndarray):
+            x = np.ascontiguousarray(x, np.float64)
+        else:
+            raise TypeError("y must be a numpy array or a CPU tensor")
+        n = self._n() or 0
+        return lib().mld_d_solver_apply_host(self._h, float(alpha), hptr(x, n, "x"), float(beta),
+                                             hptr(y, n, "y"), trans.encode()[:1])
 
     @property
     def device(self) -> DeviceFactors | None:

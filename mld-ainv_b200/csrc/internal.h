@@ -206,6 +206,13 @@ int launch_spmv(const DevSell &a, double alpha, const double *x, double beta,
                 double *y, cudaStream_t s, int *status = nullptr);
 // Both sweeps of the apply for trans 'N' or 'T'/'C'.
 // status: device word for wait timeouts (the handle's own when null).
+// update_a (src/impl/mld_d_base_ainv_update_a.f90:53-79) on stream s:
+// d <- 1/(1/d_old + diag(W^T diag(x) Z)), d_old read from d64_in when given
+// (FP64) else from the handle's device d; the new d is stored in the
+// handle (its precision) and, when d64 is given, in FP64.  d64 may alias
+// d64_in.
+int update_a_async(ainv_handle *h, const double *x, const double *d64_in, double *d64,
+                   cudaStream_t s);
 int ainv_apply_async(const ainv_handle *h, char trans, double alpha, const double *x,
                      double beta, double *y, cudaStream_t s, const int *stop = nullptr,
                      int *status = nullptr);

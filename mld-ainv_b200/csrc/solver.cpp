@@ -286,21 +286,32 @@ int mld_d_solver_apply_host(mld_d_solver *sv, double alpha, const double *x, dou
   return ainv_gpu_apply_host(sv->h, trans, alpha, x, beta, y);
 }
 
-int mld_d_solver_update_a(mld_d_solver *sv, const double *x) {
+int mld_d_solver_update_a(mld_d_solver *sv, const double *x, int nx) {
   if (!sv || !x) return AINV_ERR_ARG;
+  // src/impl/mld_d_base_ainv_update_a.f90:53-79 on the device; sv%d and the
+  // device copy are both replaced.  Wrong size: info = -1 there (:54-58).
+  if (sv->built && nx < (int)sv->d.size()) {
+    ainv::set_error("update_a: x has %d entries, the factors %d", nx, (int)sv->d.size());
+    return AINV_ERR_ARG;
+  }
   if (!sv->h) {
     ainv::set_error("update_a: factors are not on the device (build, then cnv)");
     return AINV_ERR_NOT_BUILT;
   }
-  // src/impl/mld_d_base_ainv_update_a.f90:53-79 on the device; sv%d and the
-  // device copy are both replaced
+  // The old d enters in FP64 from sv%d (the device copy may be rounded to
+  // FP32/BF16), so the host d keeps the reference's FP64 recurrence across
+  // repeated updates; the kernel overwrites dd with the new FP64 d.
   const size_t bytes = sizeof(double) * sv->d.size();
   double *xd = nullptr, *dd = nullptr;
   cudaError_t e = cudaMalloc(&xd, bytes);
   if (e == cudaSuccess) e = cudaMalloc(&dd, bytes);
   if (e == cudaSuccess) e = cudaMemcpy(xd, x, bytes, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dd, sv->d.data(), bytes, cudaMemcpyHostToDevice);
   int rc = AINV_SUCCESS;
-  if (e == cudaSuccess) rc = ainv_gpu_update_a(sv->h, xd, dd, nullptr);
+  if (e == cudaSuccess) {
+    rc = ainv::update_a_async(sv->h, xd, dd, dd, nullptr);
+    if (rc == AINV_SUCCESS) e = cudaStreamSynchronize(nullptr);
+  }
   if (e == cudaSuccess && rc == AINV_SUCCESS)
     e = cudaMemcpy(sv->d.data(), dd, bytes, cudaMemcpyDeviceToHost);
   if (xd) cudaFree(xd);

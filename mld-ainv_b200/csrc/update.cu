@@ -27,10 +27,13 @@ __device__ __forceinline__ void slot_of(const SellView<V> &m, int pack, int s, i
   col = om ? s * kSlice + lane + __ldg(m.idx + ib + k) : __ldg(m.idx + ib + pos);
 }
 
+// d64_in (optional): the old d in FP64, read instead of the device copy d
+// (which is rounded for FP32/BF16 handles); may alias d64 (each thread
+// reads its row before writing it).
 template <class V>
 __global__ void __launch_bounds__(kBlock)
     k_update_a(SellView<V> wt, int wpack, SellView<V> zt, int zpack, const double *__restrict__ x,
-               V *__restrict__ d, double *__restrict__ d64) {
+               V *__restrict__ d, const double *d64_in, double *d64) {
   const int row = blockIdx.x * kBlock + threadIdx.x;
   if (row >= wt.n) return;
   const int s = row / kSlice, lane = row % kSlice;
@@ -61,37 +64,39 @@ __global__ void __launch_bounds__(kBlock)
       }
     }
   }
-  const double dd = __ddiv_rn(1.0, __dadd_rn(__ddiv_rn(1.0, (double)ldd(d + row)), e));
+  const double dold = d64_in ? d64_in[row] : (double)ldd(d + row);
+  const double dd = __ddiv_rn(1.0, __dadd_rn(__ddiv_rn(1.0, dold), e));
   d[row] = (V)dd;
   if (d64) d64[row] = dd;
 }
 
 }  // namespace
 
-int update_a_async(ainv_handle *h, const double *x, double *d64, cudaStream_t s) {
+int update_a_async(ainv_handle *h, const double *x, const double *d64_in, double *d64,
+                   cudaStream_t s) {
   const int G = (h->n + kBlock - 1) / kBlock;
   switch (h->prec) {
     case AINV_PREC_FP64:
       k_update_a<double><<<G, kBlock, 0, s>>>(view<double>(h->wt), h->wt.pack,
                                                view<double>(h->zt), h->zt.pack, x, (double *)h->d,
-                                               d64);
+                                               d64_in, d64);
       break;
     case AINV_PREC_FP32:
       k_update_a<float><<<G, kBlock, 0, s>>>(view<float>(h->wt), h->wt.pack, view<float>(h->zt),
-                                              h->zt.pack, x, (float *)h->d, d64);
+                                              h->zt.pack, x, (float *)h->d, d64_in, d64);
       break;
     case AINV_PREC_FP32_ACC64:
       k_update_a<f32w><<<G, kBlock, 0, s>>>(view<f32w>(h->wt), h->wt.pack, view<f32w>(h->zt),
-                                             h->zt.pack, x, (f32w *)h->d, d64);
+                                             h->zt.pack, x, (f32w *)h->d, d64_in, d64);
       break;
     case AINV_PREC_BF16_ACC64:
       k_update_a<b16w><<<G, kBlock, 0, s>>>(view<b16w>(h->wt), h->wt.pack, view<b16w>(h->zt),
-                                             h->zt.pack, x, (b16w *)h->d, d64);
+                                             h->zt.pack, x, (b16w *)h->d, d64_in, d64);
       break;
     default:
       k_update_a<__nv_bfloat16><<<G, kBlock, 0, s>>>(view<__nv_bfloat16>(h->wt), h->wt.pack,
                                                       view<__nv_bfloat16>(h->zt), h->zt.pack, x,
-                                                      (__nv_bfloat16 *)h->d, d64);
+                                                      (__nv_bfloat16 *)h->d, d64_in, d64);
       break;
   }
   const cudaError_t e = cudaGetLastError();
@@ -110,5 +115,5 @@ extern "C" int ainv_gpu_update_a(ainv_handle *h, const double *x_dev, double *d_
     ainv::set_error("ainv_gpu_update_a: null argument");
     return AINV_ERR_ARG;
   }
-  return ainv::update_a_async(h, x_dev, d_dev_out, (cudaStream_t)stream);
+  return ainv::update_a_async(h, x_dev, nullptr, d_dev_out, (cudaStream_t)stream);
 }

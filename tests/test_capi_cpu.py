@@ -240,8 +240,8 @@ def test_apply_requires_device_factors():
         sv.apply_a(1.0, np.ones(64), 0.0, yt)               # mixed array kinds
     with pytest.raises(TypeError):
         sv.apply_a(1.0, xt.float(), 0.0, yt)                # not float64
-    with pytest.raises(TypeError):
-        sv.apply_a(1.0, xt[:32], 0.0, yt)                   # lengths differ
+    with pytest.raises(ValueError):
+        sv.apply_a(1.0, xt[:32], 0.0, yt)                   # x shorter than n
 
 
 def test_dump_writes_matrix_market(tmp_path):

@@ -77,3 +77,23 @@ def test_solver_type_update_and_shifted_solve():
     res = A.solve(b, x, sv.device, "BICGSTAB", 1e-9, 1000)
     assert res.converged, res
     assert ainv.mld_d_ainv_solver_type().update_a(shift) == ainv._lib.ERR_NOT_BUILT
+
+
+def test_reduced_precision_update_keeps_fp64_host_d():
+    """With FP32 factors on the device the solver type still forms the new
+    d in FP64 from its FP64 host d, so repeated updates track the oracle's
+    FP64 recurrence (only the device factors' rounding enters, through e)."""
+    irp, ja, val = ainv.pde.gen_pde3d(20, "convdiff", (10 / np.sqrt(3),) * 3)
+    n = len(irp) - 1
+    sv = ainv.mld_d_ainv_solver_type()
+    sv.cseti("SUB_FILLIN", 20)
+    sv.csetr("SUB_ILUTHRS", 0.1)
+    assert sv.build(irp, ja, val, amold="FP32") == 0
+    of = oracle_factors(sv.factors())
+    d_ref = of.d
+    for k in range(3):
+        shift = ainv.pde.rand_uniform(60 + k, n, 0.0, 2.0)
+        assert sv.update_a(shift) == 0
+        d_ref = O.update_a(O.Factors(of.wt, of.z, d_ref), shift)
+        assert relerr(sv.factors()["d"], d_ref) <= 1e-6
+    assert sv.update_a(np.zeros(n - 1)) == ainv._lib.ERR_ARG
