@@ -73,6 +73,9 @@ def layout_bytes(n, lay, vsize, tsize):
     return s1, s2
 
 
+PEAK = [6650.0, "fallback"]  # HBM GB/s the fractions use; set from measured_peaks()
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -348,6 +351,7 @@ def main():
              2: "k_stream_axpby" if forced == "1" else "k_sweep_axpby"}
     dom_name = names[dom]
     peak, peak_kind = measured_peaks()
+    PEAK[:] = [peak, peak_kind]
     achieved = sb[dom - 1] / (st_ms[dom] * 1e-3) / 1e9
     traffic = recorded_traffic(dom_name)
 
@@ -465,6 +469,7 @@ def run_extras(ainv, torch, dev, irp, ja, val, f, sv, flush, stream, fp64_ms):
         out["mixed"][prec] = {"ms": round(ms, 5), "GB/s": round(Bm / (ms * 1e-3) / 1e9, 2),
                               "bytes": Bm, "layout_bytes": Bl,
                               "layout_GBps": round(Bl / (ms * 1e-3) / 1e9, 2),
+                              "layout_frac": round(Bl / (ms * 1e-3) / 1e9 / PEAK[0], 4),
                               "speedup_vs_fp64": round(fp64_ms / ms, 3)}
         df.close()
     # the transposed apply y = W D^-1 Z^T x (trans 'T'), FP64 factors: same
@@ -536,7 +541,158 @@ def run_extras(ainv, torch, dev, irp, ja, val, f, sv, flush, stream, fp64_ms):
     out["variants"] = run_variants(ainv, torch, dev, irp, ja, val, A, b, bn, xs, x, y,
                                    flush, stream)
     A.close()
+    out["general_pattern"] = run_general_pattern(ainv, torch, dev, f, x, y, flush, stream)
+    served = run_served_200(ainv, torch, dev, irp, ja, val, sv)
+    # the precision configuration at 200^3: plain (one solve at a time) and
+    # served, each against the plain FP64 solve; residuals are FP64 b - A x
+    fp64 = seeds["FP64"]["solves_per_s"]
+    out["mixed_200"] = {
+        "target": "mixed-precision served solve >= 1.5x the plain FP64 solve's solves/s "
+                  "at FP64 relative residual 1e-9",
+        "plain": {p: {"solves_per_s": seeds[p]["solves_per_s"],
+                      "vs_fp64": round(seeds[p]["solves_per_s"] / fp64, 3),
+                      "iters_3rhs": seeds[p]["iters"],
+                      "true_relres_seed0": out["solve"][p]["true_relres"],
+                      "max_err_vs_xstar_seed0": out["solve"][p]["max_err_vs_xstar"]}
+                  for p in seeds},
+        "served": served}
     return out
+
+
+def run_served_200(ainv, torch, dev, irp, ja, val, sv, requests=16, slots=16, iters=4):
+    """The mixed-precision, served solve on the 200^3 convection-diffusion
+    case against the plain FP64 GPU solve.  `requests` right-hand sides
+    b_k = A x*_k (x*_k ~ U(-1,1), seed k), BiCGSTAB to 1e-9 from x0 = 0:
+      plain_fp64: ainv_gpu_solve with FP64 factors, one system after another;
+      served[mode]: all requests submitted at once to a solve server holding
+        the operator with factors of that precision; the server batches
+        them (requests on one operator share its reads) and confirms each
+        result on the FP64 true residual b - A x.
+    solves/s = requests / (last completion - first submission); latency =
+    submission of the host b -> solution in the host x buffer."""
+    from ainv import serve
+    n = len(irp) - 1
+    A = ainv.DeviceOperator(irp, ja, val)
+    xstar = [ainv.pde.rand_uniform(k, n) for k in range(requests)]
+    bh = []
+    for k in range(requests):
+        bd = torch.zeros(n, dtype=torch.float64, device=dev)
+        A.spmv(torch.from_numpy(xstar[k]).to(dev), bd, 1.0, 0.0)
+        bh.append(bd.cpu().pin_memory())
+    out = {"workload": "convdiff3d_200_upwind_bicgstab_1e-9_ainv_llk_drop0.1_fill20",
+           "requests": requests, "slots": slots, "iters_per_launch": iters}
+    # plain FP64 solves, one after another (device b and x)
+    assert sv.cnv("FP64") == 0, ainv.last_error()
+    its, t_tot = [], 0.0
+    x = torch.zeros(n, dtype=torch.float64, device=dev)
+    A.solve(bh[0].to(dev), x, sv.device, "BICGSTAB", 1e-9, 2000)  # warm-up
+    for k in range(requests):
+        b = bh[k].to(dev)
+        x.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = A.solve(b, x, sv.device, "BICGSTAB", 1e-9, 2000)
+        torch.cuda.synchronize()
+        t_tot += time.perf_counter() - t0
+        its.append(r.iter)
+    plain = requests / t_tot
+    out["plain_fp64"] = {"solves_per_s": round(plain, 3), "iters_mean": round(float(np.mean(its)), 2),
+                         "iters": its}
+    out["served"] = {}
+    for mode in ("FP32_ACC64", "BF16_ACC64", "FP32", "BF16", "FP64"):
+        assert sv.cnv(mode) == 0, ainv.last_error()
+        xh = [torch.zeros(n, dtype=torch.float64).pin_memory() for _ in range(requests)]
+        with serve.SolveServer(max_slots=slots, iters_per_launch=iters) as srv:
+            op = srv.add_operator(A, sv.device)
+            srv.wait(srv.submit(op, bh[0], xh[0], 1e-9, 2000))  # warm-up: graph capture
+            rids = [srv.submit(op, bh[k], xh[k], 1e-9, 2000) for k in range(requests)]
+            res = [srv.wait(q) for q in rids]
+            st = srv.stats()
+        t_first = min(q.t_submit for q in res)
+        t_last = max(q.t_done for q in res)
+        lat = np.array([q.latency for q in res]) * 1e3
+        sps = requests / (t_last - t_first)
+        out["served"][mode] = {
+            "solves_per_s": round(sps, 3), "vs_plain_fp64": round(sps / plain, 3),
+            "converged": int(sum(q.converged for q in res)),
+            "max_final_fp64_relres": float(max(q.err for q in res)),
+            "max_err_vs_xstar": float(max(np.abs(xh[k].numpy() - xstar[k]).max()
+                                          for k in range(requests))),
+            "iters_mean": round(float(np.mean([q.iter for q in res])), 2),
+            "iters_max": int(max(q.iter for q in res)),
+            "p50_ms": round(float(np.percentile(lat, 50)), 2),
+            "p99_ms": round(float(np.percentile(lat, 99)), 2),
+            "peak_active": st["peak_active"]}
+    assert sv.cnv("FP64") == 0, ainv.last_error()
+    A.close()
+    return out
+
+
+def permuted_factors(f, seed=1):
+    """The factors under a seeded random symmetric permutation P: P W^T P^T,
+    P Z P^T and P D^-1 (the apply of P M P^T).  Same entries and work as the
+    stencil factors, but every row's columns scattered: the layout falls
+    back to per-entry columns (no shared offsets)."""
+    import scipy.sparse as sps
+    n = len(f["d"])
+    p = np.random.default_rng(seed).permutation(n)
+    out = {"d": np.ascontiguousarray(f["d"][p])}
+    for k in ("wt", "z"):
+        m = sps.csr_matrix((f[k + "_val"], f[k + "_ja"], f[k + "_irp"]), shape=(n, n))
+        m = m[p][:, p].tocsr()
+        m.sort_indices()
+        out[k + "_irp"] = m.indptr.astype(np.int32)
+        out[k + "_ja"] = m.indices.astype(np.int32)
+        out[k + "_val"] = m.data.astype(np.float64)
+    return out
+
+
+def run_general_pattern(ainv, torch, dev, f, x, y, flush, stream, reps=30):
+    """The apply on factors that are not stencil-shaped: the 200^3 factors
+    under a random symmetric permutation (permuted_factors), FP64, L2
+    flushed between applies."""
+    n = len(f["d"])
+    g = permuted_factors(f)
+    df = ainv.DeviceFactors((g["wt_irp"], g["wt_ja"], g["wt_val"]),
+                            (g["z_irp"], g["z_ja"], g["z_val"]), g["d"])
+    lay = {k: df.layout_info(k) for k in ("wt", "z")}
+    for _ in range(3):
+        df.apply(x, y, 1.0, 0.0, "N", stream)
+    evs = []
+    for _ in range(reps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        df.apply(x, y, 1.0, 0.0, "N", stream)
+        b.record(stream)
+        evs.append((a, b))
+    st = {}
+    for stage in (1, 2):
+        ev2 = []
+        for _ in range(reps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            df.apply_stage(stage, x=x, y=y, alpha=1.0, beta=0.0, trans="N", stream=stream)
+            b.record(stream)
+            ev2.append((a, b))
+        torch.cuda.synchronize()
+        st[stage] = sum(a.elapsed_time(b) for a, b in ev2) / reps
+    torch.cuda.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in evs) / reps
+    B = csr_apply_bytes(n, len(g["wt_ja"]), len(g["z_ja"]))
+    lb = layout_bytes(n, lay, 8, 8)
+    df.close()
+    return {"workload": "convdiff3d_200 AINV factors under a random symmetric permutation "
+                        "(seed 1), FP64 'N' apply",
+            "offset_slices": [lay["wt"]["offset_slices"], lay["z"]["offset_slices"]],
+            "nslices": lay["wt"]["nslices"], "slots": [lay["wt"]["slots"], lay["z"]["slots"]],
+            "ms": round(ms, 5), "GB/s": round(B / (ms * 1e-3) / 1e9, 2), "bytes": B,
+            "layout_bytes": sum(lb), "layout_GBps": round(sum(lb) / (ms * 1e-3) / 1e9, 2),
+            "layout_frac": round(sum(lb) / (ms * 1e-3) / 1e9 / PEAK[0], 4),
+            "stage_ms": [round(st[1], 5), round(st[2], 5)],
+            "stage_layout_frac": [round(lb[i] / (st[i + 1] * 1e-3) / 1e9 / PEAK[0], 4)
+                                  for i in range(2)]}
 
 
 def run_variants(ainv, torch, dev, irp, ja, val, A, b, bn, xs, x, y, flush, stream):
@@ -581,7 +737,8 @@ def run_variants(ainv, torch, dev, irp, ja, val, A, b, bn, xs, x, y, flush, stre
         Bv = csr_apply_bytes(n, rec["nnz_wt"], rec["nnz_z"])
         rec["apply"] = {"ms": round(ms, 5), "GB/s": round(Bv / (ms * 1e-3) / 1e9, 2),
                         "bytes": Bv, "layout_bytes": Bl,
-                        "layout_GBps": round(Bl / (ms * 1e-3) / 1e9, 2)}
+                        "layout_GBps": round(Bl / (ms * 1e-3) / 1e9, 2),
+                        "layout_frac": round(Bl / (ms * 1e-3) / 1e9 / PEAK[0], 4)}
         rec["solve"] = {}
         for prec in ("FP64", "FP32"):
             if prec != "FP64":

@@ -171,6 +171,12 @@ int ainv_gpu_solve(ainv_handle *h, const ainv_csr *a, const double *b_dev,
  * claimed convergence the true residual did not confirm, and how often the
  * recurrence residual was replaced by b - A x. */
 int ainv_csr_solve_info(const ainv_csr *a, int *verify_fails, int *replacements);
+/* Relative residual ||r_k||/||b|| after each iteration k of the last
+ * ainv_gpu_solve on this operator (the first 8192 iterations), written to
+ * rel_res[0 .. min(cap, count)); *count receives the number recorded.  The
+ * reference prints the same quantity per iteration when its itrace > 0
+ * (psb_krylov's trace; tests/pdegen/ppde3d.f90:280-281 passes itrace). */
+int ainv_csr_solve_history(const ainv_csr *a, double *rel_res, int cap, int *count);
 
 /* update_a (src/impl/mld_d_base_ainv_update_a.f90:53-79): reuse the factors
  * for the shifted system A + diag(x) by refreshing the diagonal,

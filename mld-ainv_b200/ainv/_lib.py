@@ -54,6 +54,7 @@ SIGNATURES = [
     ("ainv_csr_destroy", _i, [_vp]),
     ("ainv_csr_check", _i, [_vp]),
     ("ainv_csr_solve_info", _i, [_vp, _ip, _ip]),
+    ("ainv_csr_solve_history", _i, [_vp, _vp, _i, _ip]),
     ("ainv_gpu_solve", _i, [_vp, _vp, _vp, _vp, _i, _d, _i, _ip, _dp, _vp]),
     ("ainv_gpu_update_a", _i, [_vp, _vp, _vp, _vp]),
     ("mld_d_solver_update_a", _i, [_vp, _vp, _i]),

@@ -241,6 +241,17 @@ class DeviceOperator:
         lib().ainv_csr_solve_info(self._h, C.byref(vf), C.byref(rp))
         return SolveResult(info, it.value, err.value, vf.value, rp.value)
 
+    def history(self) -> np.ndarray:
+        """||r_k||/||b|| after each iteration of the last solve on this
+        operator (the first 8192 iterations)."""
+        cnt = C.c_int(0)
+        check(lib().ainv_csr_solve_history(self._h, None, 0, C.byref(cnt)))
+        out = np.zeros(cnt.value)
+        if cnt.value:
+            check(lib().ainv_csr_solve_history(self._h, C.c_void_p(out.ctypes.data), cnt.value,
+                                               C.byref(cnt)))
+        return out
+
     def block_solve(self, B, X, factors: DeviceFactors | None = None, eps=1e-9, itmax=1000,
                     stream=None) -> "BlockSolveResult":
         """CG on the m columns of B (a CUDA float64 tensor of shape (n, m),

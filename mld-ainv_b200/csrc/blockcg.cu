@@ -126,7 +126,7 @@ __device__ __forceinline__ void row_mm(const SellView<V> &m, int pack, int vb, i
 #pragma unroll
     for (int j = 0; j < kSlotBatch; j++)
 #pragma unroll
-      for (int e = 0; e < kColsPerLane; e++) acc[e] = fma(v[j], xv[j][e], acc[e]);
+      for (int e = 0; e < kColsPerLane; e++) acc[e] = madd(v[j], xv[j][e], acc[e]);
   }
 }
 

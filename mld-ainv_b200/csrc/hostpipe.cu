@@ -151,10 +151,9 @@ __global__ void __launch_bounds__(kBlock) k_host_pipe(PipeArgs<V, T> a) {
 #pragma unroll
           for (int q = 0; q < S; q++) {
             const int row = (g * S + q) * kSlice + lane;
-            if (row < a.m2.n) {
-              const double r = __dmul_rn(a.alpha, (double)acc[q]);
-              a.y[row] = (a.beta == 0.0) ? r : __fma_rn(a.beta, __ldcg(a.ys + row), r);
-            }
+            if (row < a.m2.n)
+              a.y[row] = axpby_row(a.alpha, (double)acc[q], a.beta,
+                                   a.beta == 0.0 ? 0.0 : __ldcg(a.ys + row));
           }
         }
       }

@@ -39,16 +39,14 @@ __global__ void __launch_bounds__(kBlock)
 }
 
 // Every sweep-2 epilogue (register, slice-range, streaming and the host-array
-// pipeline kernels) rounds alike: r = alpha*acc rounded, then y = beta*y + r
-// as one fused multiply-add, so all forms give the same bits.
+// pipeline kernels) uses axpby_row, so all forms give the same bits.
 template <class V, class T, int S, int P>
 __global__ void __launch_bounds__(kBlock)
     k_sweep_axpby(SellView<V> m, const T *__restrict__ t, double alpha, double beta,
                   double *__restrict__ y, const int *__restrict__ stop) {
   if (stop && *stop) return;
   for_each_row<S, P>(m, t, [&](int row, auto acc) {
-    const double r = __dmul_rn(alpha, (double)acc);
-    y[row] = (beta == 0.0) ? r : __fma_rn(beta, y[row], r);
+    y[row] = axpby_row(alpha, (double)acc, beta, beta == 0.0 ? 0.0 : y[row]);
   });
 }
 
@@ -68,8 +66,7 @@ __global__ void __launch_bounds__(kBlock)
   for_each_row<S, P>(
       m, t,
       [&](int row, auto acc) {
-        const double r = __dmul_rn(alpha, (double)acc);
-        y[row] = (beta == 0.0) ? r : __fma_rn(beta, y[row], r);
+        y[row] = axpby_row(alpha, (double)acc, beta, beta == 0.0 ? 0.0 : y[row]);
       },
       g0, g1);
 }
@@ -113,8 +110,7 @@ struct EpiAxpby {
   }
   template <class A>
   __device__ __forceinline__ void post(int row, A acc, const StagedRows &r) const {
-    const double v = __dmul_rn(alpha, (double)acc);
-    y[row] = (beta == 0.0) ? v : __fma_rn(beta, r.get<double>(0, row), v);
+    y[row] = axpby_row(alpha, (double)acc, beta, beta == 0.0 ? 0.0 : r.get<double>(0, row));
   }
 };
 

@@ -3,13 +3,23 @@
 // as driven at tests/pdegen/ppde3d.f90:280-281.
 //
 // Every scalar of the recurrence (rho, alpha, omega, beta, norms, status)
-// lives in device memory and is produced by the last block of the kernel
-// that computes the corresponding reduction, so one iteration is a fixed
-// sequence of launches with no host round trip.  Reductions are
-// deterministic: per-block partials are folded in block order.  Iterations
-// are issued in chunks captured once into a CUDA graph; when the loop has
-// converged (or broken down) a device flag makes every later kernel of the
-// chunk return at once, and the host inspects the state once per chunk.
+// lives in device memory and is produced by the fold kernel that completes
+// the corresponding reduction, so one iteration is a fixed sequence of
+// launches with no host round trip.  Iterations are issued in chunks
+// captured once into a CUDA graph; when the loop has converged (or broken
+// down) a device flag makes every later kernel of the chunk return at once,
+// and the host inspects the state once per chunk.
+//
+// Reproducible iterates.  Every dot is summed in the canonical order of
+// sell_device.cuh (slice trees, then 1024-slice ranges, then the ranges),
+// which does not depend on the grid, the kernel that computes the products
+// or the device: the producing kernel stores one sum per 32-row slice and a
+// fold kernel (k_fold) reduces them.  The library is compiled without
+// floating-point contraction, so every FP64 product and sum of the vector
+// updates rounds once, as in the reference's Fortran on a target without
+// fused multiply-add, and the row sums of the sweeps and of A use the same
+// unfused order (madd).  With FP64 factors the iterates therefore equal,
+// bit for bit, those of the oracle's ordered-dot Krylov loop.
 //
 // Fused steps: the A product and the dots that consume it (p.q, rt.v, t.t
 // and t.s) share one kernel; the Z sweep of the preconditioner and the CG
@@ -20,7 +30,9 @@
 #include <cstdint>
 #include <cmath>
 #include <cstdlib>
+#include <cstring>
 #include <new>
+#include <vector>
 
 #include "kstate.cuh"
 #include "stream.cuh"
@@ -33,16 +45,134 @@ using namespace dev;
 using namespace kstate;
 
 constexpr int kChunk = 8;  // iterations per captured graph launch
+constexpr int kHistCap = 8192;  // iterations whose residual is recorded
+
+// Where a reduction kernel stores its slice sums: dot k of slice s at
+// sp[k*ld + s].
+struct SliceOut {
+  double *sp;
+  int ld;
+};
+
+// ---- the fold ----------------------------------------------------------------
+// Block j reduces the slice sums of range j (kFoldRange slices) and stores
+// the range sums; the last block to finish (atomic ticket, no waiting)
+// folds the range sums and hands the totals to fin.  fin.skip(st) repeats
+// the producing kernel's early-exit test, so a reduction that did not run
+// is not folded.
+template <int NV, class Fin>
+__global__ void __launch_bounds__(kFoldThreads)
+    k_fold(const double *__restrict__ sp, int ld, int ns, double *__restrict__ rs, int ldr,
+           KState *st, Fin fin) {
+  if (fin.skip(st)) return;
+  __shared__ bool is_last;
+  const int nr = gridDim.x;
+  const int s0 = blockIdx.x * kFoldRange, s1 = min(ns, s0 + kFoldRange);
+  double v[NV];
+#pragma unroll
+  for (int k = 0; k < NV; k++) {
+    double a = 0.0;
+    for (int s = s0 + threadIdx.x; s < s1; s += kFoldThreads) a = __dadd_rn(a, sp[(size_t)k * ld + s]);
+    v[k] = a;
+  }
+  block_sum<NV>(v);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; k++) rs[(size_t)k * ldr + blockIdx.x] = v[k];
+    __threadfence();
+    is_last = atomicAdd(&st->ticket[3], 1u) == (unsigned)nr - 1;
+  }
+  __syncthreads();
+  if (!is_last) return;
+  __threadfence();
+#pragma unroll
+  for (int k = 0; k < NV; k++) {
+    double a = 0.0;
+    for (int r = threadIdx.x; r < nr; r += kFoldThreads)
+      a = __dadd_rn(a, __ldcg(rs + (size_t)k * ldr + r));
+    v[k] = a;
+  }
+  block_sum<NV>(v);
+  if (threadIdx.x == 0) {
+    st->ticket[3] = 0u;
+    fin(st, v);
+  }
+}
+
+// Early-exit test of the reductions that stop once the loop is done.
+struct UntilDone {
+  __device__ __forceinline__ bool skip(const KState *st) const { return st->done != 0; }
+};
+
+struct FinBnorm {
+  __device__ __forceinline__ bool skip(const KState *) const { return false; }
+  __device__ __forceinline__ void operator()(KState *st, const double (&v)[1]) const {
+    const double bn = sqrt(v[0]);
+    st->bn2 = (bn == 0.0) ? 1.0 : bn;
+  }
+};
+
+__device__ __forceinline__ bool true_res_verify(const KState *st) {
+  return st->done && st->status == AINV_SUCCESS && !st->verified;
+}
+__device__ __forceinline__ bool true_res_periodic(const KState *st) {
+  return !st->done && st->check_every > 0 && st->iter > 0 && st->iter % st->check_every == 0;
+}
+
+constexpr int dots_of(int mode) {
+  return mode == kTrueRes ? 3 : (mode == kInit || mode == kBicgOmega) ? 2 : 1;
+}
+
+// Scalar step of an SpMV-with-dots reduction (w2: rt for BiCGSTAB, else
+// null, as finish_dots expects).
+template <int MODE>
+struct FinDots {
+  const double *w2;
+  __device__ __forceinline__ bool skip(const KState *st) const {
+    if (MODE == kTrueRes) return !true_res_verify(st) && !true_res_periodic(st);
+    return st->done != 0;
+  }
+  __device__ __forceinline__ void operator()(KState *st, const double (&v)[dots_of(MODE)]) const {
+    double pr[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < dots_of(MODE); k++) pr[k] = v[k];
+    finish_dots<MODE>(st, pr, MODE == kTrueRes && true_res_verify(st), w2);
+  }
+};
+
+struct FinCgRho : UntilDone {
+  __device__ __forceinline__ void operator()(KState *st, const double (&v)[1]) const {
+    cg_take_rho(st, v[0]);
+  }
+};
+
+struct FinCgXr : UntilDone {
+  __device__ __forceinline__ void operator()(KState *st, const double (&v)[1]) const {
+    finish_iteration(st, v[0]);
+  }
+};
+
+struct FinBicgXr : UntilDone {
+  __device__ __forceinline__ void operator()(KState *st, const double (&v)[2]) const {
+    finish_iteration(st, v[0]);
+    bicg_next_rho(st, v[1]);
+  }
+};
+
+// ---- reduction kernels ---------------------------------------------------------
+// Vector-only kernels walk warp-per-slice (lane = row), so the slice trees
+// see the same lane order as in the SpMV kernels.
+__device__ __forceinline__ int nslices_of(int n) { return (n + kSlice - 1) / kSlice; }
 
 // ||b||_2 (istop=2 denominator).
 __global__ void __launch_bounds__(kBlock)
-    k_bnorm(int n, const double *__restrict__ b, KState *st, double *partials) {
-  double pr[1] = {0.0};
-  for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock)
-    pr[0] += b[i] * b[i];
-  if (grid_sum<1>(pr, partials, &st->ticket[0]) && threadIdx.x == 0) {
-    const double bn = sqrt(pr[0]);
-    st->bn2 = (bn == 0.0) ? 1.0 : bn;
+    k_bnorm(int n, const double *__restrict__ b, SliceOut o) {
+  SliceSums<1> ss{o.sp, o.ld, {0.0}};
+  const int ns = nslices_of(n), lane = threadIdx.x & 31;
+  for (int s = first_slice(); s < ns; s += slice_stride()) {
+    const int i = s * kSlice + lane;
+    if (i < n) ss.v[0] = b[i] * b[i];
+    ss.end(s);
   }
 }
 
@@ -56,48 +186,52 @@ __global__ void __launch_bounds__(kBlock)
 //               iterations and once when the recurrence claims convergence.
 //               Decides whether r is replaced (k_replace_r) and whether the
 //               convergence stands; w2 = rt for BiCGSTAB's rho.
+// The row products of the dots go to ss; the fold does the scalar step.
+template <int MODE>
+__device__ __forceinline__ void dots_row(int i, double acc, const double *__restrict__ x,
+                                         double *__restrict__ y, const double *w1, double *w2,
+                                         const double *w3, SliceSums<dots_of(MODE)> &ss) {
+  if constexpr (MODE == kTrueRes || MODE == kInit) {
+    const double ri = w1[i] - acc;
+    y[i] = ri;
+    ss.v[0] = ri * ri;
+    if constexpr (MODE == kInit) {
+      if (w2) {
+        w2[i] = ri;
+        ss.v[1] = ri * ri;
+      }
+    } else {
+      const double g = ri - w3[i];
+      ss.v[1] = g * g;
+      if (w2) ss.v[2] = w2[i] * ri;
+    }
+  } else {
+    y[i] = acc;
+    if constexpr (MODE == kCgSigma) ss.v[0] = x[i] * acc;
+    if constexpr (MODE == kBicgSigma) ss.v[0] = w1[i] * acc;
+    if constexpr (MODE == kBicgOmega) {
+      ss.v[0] = acc * acc;
+      ss.v[1] = acc * w1[i];
+    }
+  }
+}
+
+template <int MODE>
+__device__ __forceinline__ bool dots_skip(const KState *st) {
+  if (MODE == kTrueRes) return !true_res_verify(st) && !true_res_periodic(st);
+  return st->done != 0;
+}
+
 template <int MODE, int S, int P>
 __global__ void __launch_bounds__(kBlock)
     k_spmv_dots(SellView<double> m, const double *__restrict__ x, double *__restrict__ y,
                 const double *__restrict__ w1, double *__restrict__ w2,
-                const double *__restrict__ w3, KState *st, double *partials) {
-  bool verify = false;
-  if (MODE == kTrueRes) {
-    verify = st->done && st->status == AINV_SUCCESS && !st->verified;
-    const bool periodic = !st->done && st->check_every > 0 && st->iter > 0 &&
-                          st->iter % st->check_every == 0;
-    if (!verify && !periodic) return;
-  } else if (st->done) {
-    return;
-  }
-  double pr[3] = {0.0, 0.0, 0.0};
-  for_each_row<S, P>(m, x, [&](int i, double acc) {
-    if (MODE == kTrueRes || MODE == kInit) {
-      const double ri = w1[i] - acc;
-      y[i] = ri;
-      pr[0] += ri * ri;
-      if (MODE == kInit) {
-        if (w2) {
-          w2[i] = ri;
-          pr[1] += ri * ri;
-        }
-      } else {
-        const double g = ri - w3[i];
-        pr[1] += g * g;
-        if (w2) pr[2] += w2[i] * ri;
-      }
-    } else {
-      y[i] = acc;
-      if (MODE == kCgSigma) pr[0] += x[i] * acc;
-      if (MODE == kBicgSigma) pr[0] += w1[i] * acc;
-      if (MODE == kBicgOmega) {
-        pr[0] += acc * acc;
-        pr[1] += acc * w1[i];
-      }
-    }
-  });
-  if (grid_sum<3>(pr, partials, &st->ticket[1]) && threadIdx.x == 0)
-    finish_dots<MODE>(st, pr, verify, w2);
+                const double *__restrict__ w3, const KState *st, SliceOut o) {
+  if (dots_skip<MODE>(st)) return;
+  SliceSums<dots_of(MODE)> ss{o.sp, o.ld, {}};
+  for_each_row_sliced<S, P>(
+      m, x, [&](int i, double acc) { dots_row<MODE>(i, acc, x, y, w1, w2, w3, ss); },
+      [&](int s) { ss.end(s); });
 }
 
 // r := b - A x when the last true-residual check asked for it.
@@ -110,7 +244,7 @@ __global__ void __launch_bounds__(kBlock)
 
 // ---- streaming variants (stream.cuh) ----------------------------------------
 // Epilogue of the SpMV-with-dots kernels: the per-row operands are loaded
-// while the stage's copies land, the dots accumulate in pr.
+// while the stage's copies land, the row products go to the slice sums.
 template <int MODE>
 struct EpiDots {
   double *__restrict__ y;
@@ -118,7 +252,7 @@ struct EpiDots {
   const double *__restrict__ w1;
   double *__restrict__ w2;
   const double *__restrict__ w3;
-  double pr[3];
+  SliceSums<dots_of(MODE)> ss;
   static constexpr int kRowVecs = (MODE == kTrueRes) ? 3 : 1;
   // row operands: b (init / true residual, with r and rt), p (CG sigma),
   // rt (BiCGSTAB sigma), s (BiCGSTAB omega)
@@ -128,30 +262,31 @@ struct EpiDots {
     return RowVecs{{w1, nullptr, nullptr}, {8, 0, 0}};
   }
   __device__ __forceinline__ void post(int i, double acc, const StagedRows &r) {
-    if (MODE == kTrueRes || MODE == kInit) {
+    if constexpr (MODE == kTrueRes || MODE == kInit) {
       const double ri = r.get<double>(0, i) - acc;
       y[i] = ri;
-      pr[0] += ri * ri;
-      if (MODE == kInit) {
+      ss.v[0] = ri * ri;
+      if constexpr (MODE == kInit) {
         if (w2) {
           w2[i] = ri;
-          pr[1] += ri * ri;
+          ss.v[1] = ri * ri;
         }
       } else {
         const double g = ri - r.get<double>(1, i);
-        pr[1] += g * g;
-        if (w2) pr[2] += r.get<double>(2, i) * ri;
+        ss.v[1] = g * g;
+        if (w2) ss.v[2] = r.get<double>(2, i) * ri;
       }
     } else {
       y[i] = acc;
       const double a = r.get<double>(0, i);
-      if (MODE == kCgSigma || MODE == kBicgSigma) pr[0] += a * acc;
-      if (MODE == kBicgOmega) {
-        pr[0] += acc * acc;
-        pr[1] += acc * a;
+      if constexpr (MODE == kCgSigma || MODE == kBicgSigma) ss.v[0] = a * acc;
+      if constexpr (MODE == kBicgOmega) {
+        ss.v[0] = acc * acc;
+        ss.v[1] = acc * a;
       }
     }
   }
+  __device__ __forceinline__ void end_slice(int s) { ss.end(s); }
 };
 
 template <int MODE, int P>
@@ -159,20 +294,10 @@ __global__ void __launch_bounds__(kStreamThreads)
     k_stream_dots(SellView<double> m, const StageDesc *__restrict__ stages, int nstages,
                   StreamLayout L, const double *__restrict__ x, double *__restrict__ y,
                   const double *__restrict__ w1, double *__restrict__ w2,
-                  const double *__restrict__ w3, KState *st, double *partials) {
-  bool verify = false;
-  if (MODE == kTrueRes) {
-    verify = st->done && st->status == AINV_SUCCESS && !st->verified;
-    const bool periodic = !st->done && st->check_every > 0 && st->iter > 0 &&
-                          st->iter % st->check_every == 0;
-    if (!verify && !periodic) return;
-  } else if (st->done) {
-    return;
-  }
-  EpiDots<MODE> epi{y, x, w1, w2, w3, {0.0, 0.0, 0.0}};
+                  const double *__restrict__ w3, KState *st, SliceOut o) {
+  if (dots_skip<MODE>(st)) return;
+  EpiDots<MODE> epi{y, x, w1, w2, w3, {o.sp, o.ld, {}}};
   stream_rows<P, 1>(m, stages, nstages, x, L, epi, &st->timeout);
-  if (grid_sum<3>(epi.pr, partials, &st->ticket[1]) && threadIdx.x == 0)
-    finish_dots<MODE>(st, epi.pr, verify, w2);
 }
 
 // CG sweep 2 with rho = r.z, streaming.
@@ -180,7 +305,7 @@ template <class T>
 struct EpiCgZ {
   const double *__restrict__ r;
   double *__restrict__ z;
-  double pr[1];
+  SliceSums<1> ss;
   static constexpr int kRowVecs = 1;
   __device__ __host__ __forceinline__ RowVecs row_vecs() const {
     return RowVecs{{r, nullptr, nullptr}, {8, 0, 0}};
@@ -189,62 +314,53 @@ struct EpiCgZ {
   __device__ __forceinline__ void post(int i, A acc, const StagedRows &rows) {
     const double zi = (double)acc;
     z[i] = zi;
-    pr[0] += rows.get<double>(0, i) * zi;
+    ss.v[0] = rows.get<double>(0, i) * zi;
   }
+  __device__ __forceinline__ void end_slice(int s) { ss.end(s); }
 };
-
-__device__ __forceinline__ void finish_cg_rho(KState *st, double rz) {
-  st->replace = 0;
-  st->rho_old = st->rho;
-  st->rho = rz;
-  if (st->iter > 0) {
-    if (st->rho_old == 0.0) {
-      st->status = AINV_ERR_BREAKDOWN;
-      st->done = 1;
-    } else {
-      st->beta = st->rho / st->rho_old;
-    }
-  }
-}
 
 template <class V, class T, int P>
 __global__ void __launch_bounds__(kStreamThreads)
     k_stream_cg_sweep2(SellView<V> m, const StageDesc *__restrict__ stages, int nstages,
                        StreamLayout L, const T *__restrict__ t, const double *__restrict__ r,
-                       double *__restrict__ z, KState *st, double *partials) {
+                       double *__restrict__ z, KState *st, SliceOut o) {
   if (st->done) return;
-  EpiCgZ<T> epi{r, z, {0.0}};
+  EpiCgZ<T> epi{r, z, {o.sp, o.ld, {0.0}}};
   stream_rows<P, stream_rmax<V>()>(m, stages, nstages, t, L, epi, &st->timeout);
-  if (grid_sum<1>(epi.pr, partials, &st->ticket[0]) && threadIdx.x == 0)
-    finish_cg_rho(st, epi.pr[0]);
 }
 
-// CG: z = Z t (sweep 2 of the AINV apply) fused with rho = r.z, then beta.
+// CG: z = Z t (sweep 2 of the AINV apply) fused with rho = r.z.
 template <class V, class T, int S, int P>
 __global__ void __launch_bounds__(kBlock)
     k_cg_sweep2(SellView<V> m, const T *__restrict__ t, const double *__restrict__ r,
-                double *__restrict__ z, KState *st, double *partials) {
+                double *__restrict__ z, const KState *st, SliceOut o) {
   if (st->done) return;
-  double pr[1] = {0.0};
-  for_each_row<S, P>(m, t, [&](int i, auto acc) {
-    const double zi = (double)acc;
-    z[i] = zi;
-    pr[0] += r[i] * zi;
-  });
-  if (grid_sum<1>(pr, partials, &st->ticket[0]) && threadIdx.x == 0) cg_take_rho(st, pr[0]);
+  SliceSums<1> ss{o.sp, o.ld, {0.0}};
+  for_each_row_sliced<S, P>(
+      m, t,
+      [&](int i, auto acc) {
+        const double zi = (double)acc;
+        z[i] = zi;
+        ss.v[0] = r[i] * zi;
+      },
+      [&](int s) { ss.end(s); });
 }
 
 // CG without preconditioner: z = r, rho = r.r.
 __global__ void __launch_bounds__(kBlock)
-    k_cg_ident(int n, const double *__restrict__ r, double *__restrict__ z, KState *st,
-               double *partials) {
+    k_cg_ident(int n, const double *__restrict__ r, double *__restrict__ z, const KState *st,
+               SliceOut o) {
   if (st->done) return;
-  double pr[1] = {0.0};
-  for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
-    z[i] = r[i];
-    pr[0] += r[i] * r[i];
+  SliceSums<1> ss{o.sp, o.ld, {0.0}};
+  const int ns = nslices_of(n), lane = threadIdx.x & 31;
+  for (int s = first_slice(); s < ns; s += slice_stride()) {
+    const int i = s * kSlice + lane;
+    if (i < n) {
+      z[i] = r[i];
+      ss.v[0] = r[i] * r[i];
+    }
+    ss.end(s);
   }
-  if (grid_sum<1>(pr, partials, &st->ticket[0]) && threadIdx.x == 0) cg_take_rho(st, pr[0]);
 }
 
 // CG: p = z (first iteration) or p = z + beta p.
@@ -256,21 +372,24 @@ __global__ void __launch_bounds__(kBlock)
   p[i] = (st->iter == 0) ? z[i] : z[i] + st->beta * p[i];
 }
 
-// CG: x += alpha p, r -= alpha q, rn2 = r.r, convergence.
+// CG: x += alpha p, r -= alpha q, rn2 = r.r.
 __global__ void __launch_bounds__(kBlock)
     k_cg_xr(int n, const double *__restrict__ p, const double *__restrict__ q,
-            double *__restrict__ x, double *__restrict__ r, KState *st, double *partials) {
+            double *__restrict__ x, double *__restrict__ r, const KState *st, SliceOut o) {
   if (st->done) return;
   const double alpha = st->alpha;
-  double pr[1] = {0.0};
-  for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
-    x[i] = x[i] + alpha * p[i];
-    const double ri = r[i] - alpha * q[i];
-    r[i] = ri;
-    pr[0] += ri * ri;
+  SliceSums<1> ss{o.sp, o.ld, {0.0}};
+  const int ns = nslices_of(n), lane = threadIdx.x & 31;
+  for (int s = first_slice(); s < ns; s += slice_stride()) {
+    const int i = s * kSlice + lane;
+    if (i < n) {
+      x[i] = x[i] + alpha * p[i];
+      const double ri = r[i] - alpha * q[i];
+      r[i] = ri;
+      ss.v[0] = ri * ri;
+    }
+    ss.end(s);
   }
-  if (grid_sum<1>(pr, partials, &st->ticket[2]) && threadIdx.x == 0)
-    finish_iteration(st, pr[0]);
 }
 
 // BiCGSTAB: p = r (first iteration) or p = r + beta (p - omega v).
@@ -298,22 +417,24 @@ __global__ void __launch_bounds__(kBlock)
     k_bicg_xr(int n, const double *__restrict__ f, const double *__restrict__ z,
               const double *__restrict__ s, const double *__restrict__ t,
               const double *__restrict__ rt, double *__restrict__ x,
-              double *__restrict__ r, KState *st, double *partials) {
+              double *__restrict__ r, const KState *st, SliceOut o) {
   if (st->done) return;
   const double alpha = st->alpha, omega = st->omega;
-  double pr[2] = {0.0, 0.0};
-  for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
-    x[i] = (x[i] + alpha * f[i]) + omega * z[i];
-    const double ri = s[i] - omega * t[i];
-    r[i] = ri;
-    pr[0] += ri * ri;
-    pr[1] += rt[i] * ri;
-  }
-  if (grid_sum<2>(pr, partials, &st->ticket[2]) && threadIdx.x == 0) {
-    finish_iteration(st, pr[0]);
-    bicg_next_rho(st, pr[1]);
+  SliceSums<2> ss{o.sp, o.ld, {0.0, 0.0}};
+  const int ns = nslices_of(n), lane = threadIdx.x & 31;
+  for (int sl = first_slice(); sl < ns; sl += slice_stride()) {
+    const int i = sl * kSlice + lane;
+    if (i < n) {
+      x[i] = (x[i] + alpha * f[i]) + omega * z[i];
+      const double ri = s[i] - omega * t[i];
+      r[i] = ri;
+      ss.v[0] = ri * ri;
+      ss.v[1] = rt[i] * ri;
+    }
+    ss.end(sl);
   }
 }
+
 
 template <class V, class T>
 struct CgSweep2Launch {
@@ -322,14 +443,14 @@ struct CgSweep2Launch {
   const double *r;
   double *z;
   KState *st;
-  double *partials;
+  SliceOut o;
   int G;
   cudaStream_t s;
   template <int S, int P>
   void run() const {
     auto kern = k_cg_sweep2<V, T, S, P>;
     kern<<<std::min(G, wave_grid((const void *)kern, m.n)), kBlock, 0, s>>>(
-        view<V>(m), (const T *)t, r, z, st, partials);
+        view<V>(m), (const T *)t, r, z, st, o);
   }
 };
 
@@ -345,7 +466,7 @@ struct StreamCgSweep2Launch {
   const double *r;
   double *z;
   KState *st;
-  double *partials;
+  SliceOut o;
   cudaStream_t s;
   bool *launched;
   template <int S, int P>
@@ -354,26 +475,26 @@ struct StreamCgSweep2Launch {
     if (!set_smem_attr((const void *)kern, smem)) return;
     const int g = occupancy_grid((const void *)kern, kStreamThreads, smem, grid);
     kern<<<g, kStreamThreads, smem, s>>>(view<V>(m), m.stages, m.nstages, L, (const T *)t, r,
-                                            z, st, partials);
+                                            z, st, o);
     *launched = true;
   }
 };
 
 template <class V, class T>
 void launch_cg_sweep2(const DevSell &m, const void *t, const double *r, double *z,
-                      KState *st, double *partials, int G, cudaStream_t s) {
+                      KState *st, SliceOut o, int G, cudaStream_t s) {
   if (stream_enabled(m.prec)) {
     StreamLayout L;
     size_t smem = 0;
     const int grid = stream_plan(m, (int)sizeof(T), EpiCgZ<T>::kRowVecs, L, smem);
     bool launched = false;
     if (grid > 0 && grid <= G && aligned16(t) && aligned16(r))
-      with_pack<V, 1>(m.pack, StreamCgSweep2Launch<V, T>{m, L, grid, smem, t, r, z, st, partials,
+      with_pack<V, 1>(m.pack, StreamCgSweep2Launch<V, T>{m, L, grid, smem, t, r, z, st, o,
                                                           s, &launched});
     if (launched) return;
   }
   with_group_pack<V>(group_size(m.prec), m.pack,
-                     CgSweep2Launch<V, T>{m, t, r, z, st, partials, G, s});
+                     CgSweep2Launch<V, T>{m, t, r, z, st, o, G, s});
 }
 
 template <int MODE>
@@ -387,7 +508,7 @@ struct SpmvDotsLaunch {
   double *w2;
   const double *w3;
   KState *st;
-  double *pp;
+  SliceOut pp;
   template <int S, int P>
   void run() const {
     auto kern = k_spmv_dots<MODE, S, P>;
@@ -409,7 +530,7 @@ struct StreamDotsLaunch {
   double *w2;
   const double *w3;
   KState *st;
-  double *pp;
+  SliceOut pp;
   bool *launched;
   template <int S, int P>
   void run() const {
@@ -425,12 +546,12 @@ struct StreamDotsLaunch {
 // y = A x with the dots of MODE (streaming when the layout allows).
 template <int MODE>
 void spmv_dots(const DevSell &Am, int G, cudaStream_t s, const double *x, double *y,
-               const double *w1, double *w2, const double *w3, KState *st, double *pp) {
+               const double *w1, double *w2, const double *w3, KState *st, SliceOut pp) {
   if (stream_enabled(Am.prec)) {
     StreamLayout L;
     size_t smem = 0;
     const int grid = stream_plan(Am, 8, EpiDots<MODE>::kRowVecs, L, smem);
-    const RowVecs rv = EpiDots<MODE>{y, x, w1, w2, w3, {0.0, 0.0, 0.0}}.row_vecs();
+    const RowVecs rv = EpiDots<MODE>{y, x, w1, w2, w3, {}}.row_vecs();
     bool launched = false;
     if (grid > 0 && grid <= G && aligned16(x) && aligned16(rv.p[0]) && aligned16(rv.p[1]) &&
         aligned16(rv.p[2]))
@@ -443,6 +564,7 @@ void spmv_dots(const DevSell &Am, int G, cudaStream_t s, const double *x, double
                           SpmvDotsLaunch<MODE>{A, G, s, x, y, w1, w2, w3, st, pp});
 }
 
+
 std::atomic<unsigned long long> g_serial{1};
 
 }  // namespace
@@ -454,7 +576,14 @@ struct KrylovWs {
   int n = 0, G = 0;
   size_t stride = 0;      // doubles between vectors (n rounded up to 32: 256 B aligned)
   double *vec = nullptr;  // 11 vectors of n
-  double *partials = nullptr;
+  // canonical-order reductions: up to 3 dots' slice sums (ld per dot) and
+  // range sums (ldr per dot)
+  int ns = 0, ld = 0, nr = 0, ldr = 0;
+  double *sp = nullptr, *rs = nullptr;
+  // relative residual per iteration of the last solve (device, host copy)
+  double *hist = nullptr;
+  std::vector<double> hhist;
+  int hcount = 0;
   KState *st = nullptr;
   KState *hst = nullptr;  // pinned mirror
   cudaStream_t s = nullptr;
@@ -464,13 +593,21 @@ struct KrylovWs {
   int key_method = -1, key_replace = -1;
   KState last{};  // final state of the last solve (statistics)
   double *v(int i) const { return vec + (size_t)i * stride; }
+  SliceOut out() const { return SliceOut{sp, ld}; }
+  // Fold the slice sums of the reduction just enqueued (NV dots).
+  template <int NV, class Fin>
+  void fold(const Fin &fin) const {
+    k_fold<NV, Fin><<<nr, kFoldThreads, 0, s>>>(sp, ld, ns, rs, ldr, st, fin);
+  }
 };
 
 void destroy_ws(KrylovWs *w) {
   if (!w) return;
   if (w->exec) cudaGraphExecDestroy(w->exec);
   if (w->vec) cudaFree(w->vec);
-  if (w->partials) cudaFree(w->partials);
+  if (w->hist) cudaFree(w->hist);
+  if (w->sp) cudaFree(w->sp);
+  if (w->rs) cudaFree(w->rs);
   if (w->st) cudaFree(w->st);
   if (w->hst) cudaFreeHost(w->hst);
   if (w->ev) cudaEventDestroy(w->ev);
@@ -496,7 +633,13 @@ int get_ws(ainv_csr *a, KrylovWs **out) {
   w->stride = ((size_t)a->n + 31) / 32 * 32;
   w->G = reduction_grid(a->n);
   cudaError_t e = cudaMalloc(&w->vec, sizeof(double) * kNumVec * w->stride);
-  if (e == cudaSuccess) e = cudaMalloc(&w->partials, sizeof(double) * 4 * (size_t)w->G);
+  w->ns = (a->n + kSlice - 1) / kSlice;
+  w->ld = (w->ns + 31) / 32 * 32;
+  w->nr = (w->ns + kFoldRange - 1) / kFoldRange;
+  w->ldr = (w->nr + 31) / 32 * 32;
+  if (e == cudaSuccess) e = cudaMalloc(&w->sp, sizeof(double) * 3 * (size_t)w->ld);
+  if (e == cudaSuccess) e = cudaMalloc(&w->rs, sizeof(double) * 3 * (size_t)w->ldr);
+  if (e == cudaSuccess) e = cudaMalloc(&w->hist, sizeof(double) * kHistCap);
   if (e == cudaSuccess) e = cudaMalloc(&w->st, sizeof(KState));
   if (e == cudaSuccess) e = cudaMallocHost(&w->hst, sizeof(KState));
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&w->s, cudaStreamNonBlocking);
@@ -513,7 +656,7 @@ int get_ws(ainv_csr *a, KrylovWs **out) {
 }
 
 void precond_sweep2_cg(const ainv_handle *h, const double *r, double *z, KState *st,
-                       double *partials, int G, cudaStream_t s) {
+                       SliceOut partials, int G, cudaStream_t s) {
   switch (h->prec) {
     case AINV_PREC_FP64: launch_cg_sweep2<double, double>(h->z, h->t, r, z, st, partials, G, s); break;
     case AINV_PREC_FP32: launch_cg_sweep2<float, float>(h->z, h->t, r, z, st, partials, G, s); break;
@@ -531,7 +674,7 @@ int enqueue_iteration(KrylovWs *w, const ainv_handle *h, const ainv_csr *a, int 
   const int Gv = (n + kBlock - 1) / kBlock;
   const DevSell &A = a->a;
   KState *st = w->st;
-  double *pp = w->partials;
+  const SliceOut pp = w->out();
   cudaStream_t s = w->s;
   const int *stop = &st->done;
   if (method == AINV_KRYLOV_CG) {
@@ -543,11 +686,15 @@ int enqueue_iteration(KrylovWs *w, const ainv_handle *h, const ainv_csr *a, int 
       k_cg_ident<<<std::min(G, wave_grid((const void *)k_cg_ident, n)), kBlock, 0, s>>>(n, r, z,
                                                                                          st, pp);
     }
+    w->fold<1>(FinCgRho{});
     k_cg_p<<<Gv, kBlock, 0, s>>>(n, z, p, st);
     spmv_dots<kCgSigma>(A, G, s, p, q, nullptr, nullptr, nullptr, st, pp);
+    w->fold<1>(FinDots<kCgSigma>{nullptr});
     k_cg_xr<<<std::min(G, wave_grid((const void *)k_cg_xr, n)), kBlock, 0, s>>>(n, p, q, x, r,
                                                                                  st, pp);
+    w->fold<1>(FinCgXr{});
     spmv_dots<kTrueRes>(A, G, s, x, w->v(RTRUE), w->v(BW), nullptr, r, st, pp);
+    w->fold<3>(FinDots<kTrueRes>{nullptr});
     k_replace_r<<<wave_grid((const void *)k_replace_r, n), kBlock, 0, s>>>(n, w->v(RTRUE), r,
                                                                          st);
   } else {
@@ -560,6 +707,7 @@ int enqueue_iteration(KrylovWs *w, const ainv_handle *h, const ainv_csr *a, int 
       AINV_CUDA_TRY(cudaMemcpyAsync(f, p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     }
     spmv_dots<kBicgSigma>(A, G, s, f, v, rt, nullptr, nullptr, st, pp);
+    w->fold<1>(FinDots<kBicgSigma>{rt});
     k_bicg_s<<<Gv, kBlock, 0, s>>>(n, r, v, sv, st);
     if (h) {
       AINV_TRY(ainv_apply_async(h, 'N', 1.0, sv, 0.0, z, s, stop, &st->timeout));
@@ -567,9 +715,12 @@ int enqueue_iteration(KrylovWs *w, const ainv_handle *h, const ainv_csr *a, int 
       AINV_CUDA_TRY(cudaMemcpyAsync(z, sv, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     }
     spmv_dots<kBicgOmega>(A, G, s, z, t, sv, nullptr, nullptr, st, pp);
+    w->fold<2>(FinDots<kBicgOmega>{rt});
     k_bicg_xr<<<std::min(G, wave_grid((const void *)k_bicg_xr, n)), kBlock, 0, s>>>(
         n, f, z, sv, t, rt, x, r, st, pp);
+    w->fold<2>(FinBicgXr{});
     spmv_dots<kTrueRes>(A, G, s, x, w->v(RTRUE), w->v(BW), rt, r, st, pp);
+    w->fold<3>(FinDots<kTrueRes>{rt});
     k_replace_r<<<wave_grid((const void *)k_replace_r, n), kBlock, 0, s>>>(n, w->v(RTRUE), r,
                                                                          st);
   }
@@ -636,13 +787,17 @@ int krylov_solve(const ainv_handle *h, ainv_csr *a, const double *b, double *x, 
   init.itmax = itmax;
   init.check_every = replace_every;
   init.method = method;
+  init.hist = w->hist;
+  init.hist_cap = kHistCap;
   *w->hst = init;
   AINV_CUDA_TRY(cudaMemcpyAsync(w->st, w->hst, sizeof(KState), cudaMemcpyHostToDevice, w->s));
   const DevSell &A = a->a;
   k_bnorm<<<std::min(w->G, wave_grid((const void *)k_bnorm, n)), kBlock, 0, w->s>>>(
-      n, w->v(BW), w->st, w->partials);
-  spmv_dots<kInit>(A, w->G, w->s, w->v(XW), w->v(R), w->v(BW),
-      method == AINV_KRYLOV_BICGSTAB ? w->v(RT) : nullptr, nullptr, w->st, w->partials);
+      n, w->v(BW), w->out());
+  w->fold<1>(FinBnorm{});
+  double *rt0 = method == AINV_KRYLOV_BICGSTAB ? w->v(RT) : nullptr;
+  spmv_dots<kInit>(A, w->G, w->s, w->v(XW), w->v(R), w->v(BW), rt0, nullptr, w->st, w->out());
+  w->fold<2>(FinDots<kInit>{rt0});
   AINV_CUDA_TRY(cudaGetLastError());
 
   // The first chunk always runs as plain launches (kernel attributes are
@@ -667,6 +822,11 @@ int krylov_solve(const ainv_handle *h, ainv_csr *a, const double *b, double *x, 
   AINV_CUDA_TRY(cudaStreamWaitEvent(user, w->ev, 0));
   const KState &f = *w->hst;
   w->last = f;
+  w->hcount = std::min(std::max(f.iter, 0), kHistCap);
+  w->hhist.resize((size_t)w->hcount);
+  if (w->hcount > 0)
+    AINV_CUDA_TRY(cudaMemcpy(w->hhist.data(), w->hist, sizeof(double) * (size_t)w->hcount,
+                             cudaMemcpyDeviceToHost));
   if (iter) *iter = f.iter;
   if (err) *err = sqrt(f.rn2) / f.bn2;
   if (f.timeout) {
@@ -697,6 +857,19 @@ extern "C" int ainv_csr_solve_info(const ainv_csr *a, int *verify_fails, int *re
   const ainv::KState *s = a->ws ? &a->ws->last : nullptr;
   if (verify_fails) *verify_fails = s ? s->fails : 0;
   if (replacements) *replacements = s ? s->replacements : 0;
+  return AINV_SUCCESS;
+}
+
+extern "C" int ainv_csr_solve_history(const ainv_csr *a, double *rel_res, int cap,
+                                      int *count) {
+  if (!a || cap < 0 || (cap > 0 && !rel_res)) {
+    ainv::set_error("ainv_csr_solve_history: invalid argument");
+    return AINV_ERR_ARG;
+  }
+  const int have = a->ws ? a->ws->hcount : 0;
+  const int k = std::min(have, cap);
+  if (k > 0) std::memcpy(rel_res, a->ws->hhist.data(), sizeof(double) * (size_t)k);
+  if (count) *count = have;
   return AINV_SUCCESS;
 }
 

@@ -20,6 +20,8 @@ struct KState {
   int replacements;
   int timeout;  // a streaming kernel gave up a bounded wait
   unsigned ticket[4];
+  double *hist;  // ||r_k||/||b|| of iteration k at hist[k-1] (k <= hist_cap), or null
+  int hist_cap;
 };
 
 namespace kstate {
@@ -32,6 +34,7 @@ __device__ __forceinline__ void finish_iteration(KState *st, double rn2) {
   st->rn2 = rn2;
   st->iter += 1;
   const double err = sqrt(rn2) / st->bn2;
+  if (st->hist && st->iter <= st->hist_cap) st->hist[st->iter - 1] = err;
   if (!isfinite(rn2)) {
     st->status = AINV_ERR_NONFINITE;
     st->done = 1;

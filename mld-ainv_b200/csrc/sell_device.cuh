@@ -36,6 +36,25 @@ __device__ __forceinline__ float ldd(const __nv_bfloat16 *p) {
   return __uint_as_float(((unsigned)u) << 16);
 }
 
+// c + a*b of the row accumulations.  In FP64 the product and the sum each
+// round once, with no fused multiply-add: the arithmetic of the reference's
+// CSR product compiled for a target without FMA, so an FP64 row sum here
+// equals the oracle's bit for bit (same operations, same column order).
+// FP32 accumulation keeps the fused form.
+__device__ __forceinline__ double madd(double a, double b, double c) {
+  return __dadd_rn(c, __dmul_rn(a, b));
+}
+__device__ __forceinline__ float madd(float a, float b, float c) { return fmaf(a, b, c); }
+
+// Sweep-2 epilogue of a row: y = alpha*acc + beta*y as the reference's CSR
+// product forms it (src/impl/mld_d_base_ainv_solver_apply_vect.f90:117-119
+// through psb_spmm), each product and the sum rounded once; y is not read
+// when beta is zero.
+__device__ __forceinline__ double axpby_row(double alpha, double acc, double beta, double y) {
+  const double r = __dmul_rn(alpha, acc);
+  return (beta == 0.0) ? r : __dadd_rn(r, __dmul_rn(beta, y));
+}
+
 // Storage types of the FP64-accumulating modes (AINV_PREC_FP32_ACC64,
 // AINV_PREC_BF16_ACC64): FP32 / BF16 values whose loads yield FP64, so the
 // products, sums and the intermediate are those of the FP64 apply.
@@ -80,6 +99,14 @@ inline SellView<V> view(const DevSell &m) {
 }
 
 // ---- packed loads: P adjacent slots of one lane in one vector load --------
+// EF (evict first): values read once per pass stream through with the
+// evict-first hint; EF = false keeps them cached, for kernels in which
+// several right-hand sides read the same slice back to back.
+template <bool EF, class T>
+__device__ __forceinline__ T ldp(const T *p) {
+  if constexpr (EF) return __ldcs(p);
+  else return __ldg(p);
+}
 __device__ __forceinline__ float bf16lo(unsigned w) { return __uint_as_float(w << 16); }
 __device__ __forceinline__ float bf16hi(unsigned w) { return __uint_as_float(w & 0xffff0000u); }
 
@@ -87,32 +114,37 @@ template <class V, int P>
 struct Pack;
 template <>
 struct Pack<double, 1> {
-  static __device__ __forceinline__ void load(const double *p, double (&o)[1]) { o[0] = __ldcs(p); }
+  template <bool EF = true>
+  static __device__ __forceinline__ void load(const double *p, double (&o)[1]) { o[0] = ldp<EF>(p); }
 };
 template <>
 struct Pack<double, 2> {
+  template <bool EF = true>
   static __device__ __forceinline__ void load(const double *p, double (&o)[2]) {
-    const double2 v = __ldcs(reinterpret_cast<const double2 *>(p));
+    const double2 v = ldp<EF>(reinterpret_cast<const double2 *>(p));
     o[0] = v.x;
     o[1] = v.y;
   }
 };
 template <>
 struct Pack<float, 1> {
-  static __device__ __forceinline__ void load(const float *p, float (&o)[1]) { o[0] = __ldcs(p); }
+  template <bool EF = true>
+  static __device__ __forceinline__ void load(const float *p, float (&o)[1]) { o[0] = ldp<EF>(p); }
 };
 template <>
 struct Pack<float, 2> {
+  template <bool EF = true>
   static __device__ __forceinline__ void load(const float *p, float (&o)[2]) {
-    const float2 v = __ldcs(reinterpret_cast<const float2 *>(p));
+    const float2 v = ldp<EF>(reinterpret_cast<const float2 *>(p));
     o[0] = v.x;
     o[1] = v.y;
   }
 };
 template <>
 struct Pack<float, 4> {
+  template <bool EF = true>
   static __device__ __forceinline__ void load(const float *p, float (&o)[4]) {
-    const float4 v = __ldcs(reinterpret_cast<const float4 *>(p));
+    const float4 v = ldp<EF>(reinterpret_cast<const float4 *>(p));
     o[0] = v.x;
     o[1] = v.y;
     o[2] = v.z;
@@ -121,22 +153,25 @@ struct Pack<float, 4> {
 };
 template <>
 struct Pack<__nv_bfloat16, 1> {
+  template <bool EF = true>
   static __device__ __forceinline__ void load(const __nv_bfloat16 *p, float (&o)[1]) {
-    o[0] = bf16lo(__ldcs(reinterpret_cast<const unsigned short *>(p)));
+    o[0] = bf16lo(ldp<EF>(reinterpret_cast<const unsigned short *>(p)));
   }
 };
 template <>
 struct Pack<__nv_bfloat16, 2> {
+  template <bool EF = true>
   static __device__ __forceinline__ void load(const __nv_bfloat16 *p, float (&o)[2]) {
-    const unsigned v = __ldcs(reinterpret_cast<const unsigned *>(p));
+    const unsigned v = ldp<EF>(reinterpret_cast<const unsigned *>(p));
     o[0] = bf16lo(v);
     o[1] = bf16hi(v);
   }
 };
 template <>
 struct Pack<__nv_bfloat16, 4> {
+  template <bool EF = true>
   static __device__ __forceinline__ void load(const __nv_bfloat16 *p, float (&o)[4]) {
-    const uint2 v = __ldcs(reinterpret_cast<const uint2 *>(p));
+    const uint2 v = ldp<EF>(reinterpret_cast<const uint2 *>(p));
     o[0] = bf16lo(v.x);
     o[1] = bf16hi(v.x);
     o[2] = bf16lo(v.y);
@@ -145,8 +180,9 @@ struct Pack<__nv_bfloat16, 4> {
 };
 template <>
 struct Pack<__nv_bfloat16, 8> {
+  template <bool EF = true>
   static __device__ __forceinline__ void load(const __nv_bfloat16 *p, float (&o)[8]) {
-    const uint4 v = __ldcs(reinterpret_cast<const uint4 *>(p));
+    const uint4 v = ldp<EF>(reinterpret_cast<const uint4 *>(p));
     o[0] = bf16lo(v.x);
     o[1] = bf16hi(v.x);
     o[2] = bf16lo(v.y);
@@ -160,18 +196,20 @@ struct Pack<__nv_bfloat16, 8> {
 
 template <int P>
 struct Pack<f32w, P> {
+  template <bool EF = true>
   static __device__ __forceinline__ void load(const f32w *p, double (&o)[P]) {
     float f[P];
-    Pack<float, P>::load(reinterpret_cast<const float *>(p), f);
+    Pack<float, P>::template load<EF>(reinterpret_cast<const float *>(p), f);
 #pragma unroll
     for (int e = 0; e < P; e++) o[e] = (double)f[e];
   }
 };
 template <int P>
 struct Pack<b16w, P> {
+  template <bool EF = true>
   static __device__ __forceinline__ void load(const b16w *p, double (&o)[P]) {
     float f[P];
-    Pack<__nv_bfloat16, P>::load(reinterpret_cast<const __nv_bfloat16 *>(p), f);
+    Pack<__nv_bfloat16, P>::template load<EF>(reinterpret_cast<const __nv_bfloat16 *>(p), f);
 #pragma unroll
     for (int e = 0; e < P; e++) o[e] = (double)f[e];
   }
@@ -277,7 +315,7 @@ struct Step { static constexpr int kPacks = P >= K ? 1 : K / P; };
 // predicated per pack (w is a multiple of P), so all value / index loads of
 // the step are in flight before the first dependent gather; the FMAs then
 // run in slot order, which is the row's column order.
-template <bool OM, int P, int K, bool NC = true, class V, class X, int S>
+template <bool OM, int P, int K, bool NC = true, bool EF = true, class V, class X, int S>
 __device__ __forceinline__ void group_slots(const SellView<V> &m, const GroupCtx<S> &c,
                                             const int (&row)[S], int k0,
                                             const X *__restrict__ x,
@@ -295,13 +333,13 @@ __device__ __forceinline__ void group_slots(const SellView<V> &m, const GroupCtx
       const bool ok = k < c.w[q];
       const size_t pos = (size_t)(k / P) * (kSlice * P) + (size_t)lane * P;
       if (ok) {
-        Pack<V, P>::load(m.val + c.vb[q] + pos, vv[q][j]);
+        Pack<V, P>::template load<EF>(m.val + c.vb[q] + pos, vv[q][j]);
         if (OM) {
           load_ints<P, false>(m.idx + c.ib[q] + k, col[q][j]);
 #pragma unroll
           for (int e = 0; e < P; e++) col[q][j][e] += row[q];
         } else {
-          load_ints<P, true>(m.idx + c.ib[q] + pos, col[q][j]);
+          load_ints<P, EF>(m.idx + c.ib[q] + pos, col[q][j]);
         }
       } else {
 #pragma unroll
@@ -327,13 +365,13 @@ __device__ __forceinline__ void group_slots(const SellView<V> &m, const GroupCtx
 #pragma unroll
     for (int j = 0; j < J; j++)
 #pragma unroll
-      for (int e = 0; e < P; e++) acc[q] = fma(vv[q][j][e], xv[q][j][e], acc[q]);
+      for (int e = 0; e < P; e++) acc[q] = madd(vv[q][j][e], xv[q][j][e], acc[q]);
 }
 
 // acc[q] = row (g*S+q)*32+lane of M dotted with x.  The encoding test is
 // warp-uniform and sits outside the slot loop; a group mixing both
 // encodings is walked one slice at a time.
-template <int P, int K = 4, bool NC = true, class V, class X, int S>
+template <int P, int K = 4, bool NC = true, bool EF = true, class V, class X, int S>
 __device__ __forceinline__ void group_dot(const SellView<V> &m, const GroupCtx<S> &c, int g,
                                           const X *__restrict__ x,
                                           typename Acc<V>::type (&acc)[S]) {
@@ -352,9 +390,9 @@ __device__ __forceinline__ void group_dot(const SellView<V> &m, const GroupCtx<S
     }
   }
   if (all_om) {
-    for (int k0 = 0; k0 < c.maxw; k0 += KS) group_slots<true, P, K, NC>(m, c, row, k0, x, acc);
+    for (int k0 = 0; k0 < c.maxw; k0 += KS) group_slots<true, P, K, NC, EF>(m, c, row, k0, x, acc);
   } else if (all_col) {
-    for (int k0 = 0; k0 < c.maxw; k0 += KS) group_slots<false, P, K, NC>(m, c, row, k0, x, acc);
+    for (int k0 = 0; k0 < c.maxw; k0 += KS) group_slots<false, P, K, NC, EF>(m, c, row, k0, x, acc);
   } else {
 #pragma unroll
     for (int q = 0; q < S; q++) {
@@ -367,9 +405,9 @@ __device__ __forceinline__ void group_dot(const SellView<V> &m, const GroupCtx<S
       const int r1[1] = {row[q]};
       A a1[1] = {A(0)};
       if (c.om[q]) {
-        for (int k0 = 0; k0 < c1.maxw; k0 += KS) group_slots<true, P, K, NC>(m, c1, r1, k0, x, a1);
+        for (int k0 = 0; k0 < c1.maxw; k0 += KS) group_slots<true, P, K, NC, EF>(m, c1, r1, k0, x, a1);
       } else {
-        for (int k0 = 0; k0 < c1.maxw; k0 += KS) group_slots<false, P, K, NC>(m, c1, r1, k0, x, a1);
+        for (int k0 = 0; k0 < c1.maxw; k0 += KS) group_slots<false, P, K, NC, EF>(m, c1, r1, k0, x, a1);
       }
       acc[q] = a1[0];
     }
@@ -396,6 +434,70 @@ __device__ __forceinline__ void for_each_row(const SellView<V> &m, const X *__re
     }
   }
 }
+
+// Visit every slice: epi(row, acc) for each lane whose row is < n, then,
+// with the whole warp, end(slice) once the slice's rows are done.
+template <int S, int P, int K = 4, class V, class X, class Epi, class End>
+__device__ __forceinline__ void for_each_row_sliced(const SellView<V> &m,
+                                                    const X *__restrict__ x, Epi &&epi,
+                                                    End &&end) {
+  const int ngroups = (m.nslices + S - 1) / S;
+  const int lane = threadIdx.x & 31;
+  for (int g = first_slice(); g < ngroups; g += slice_stride()) {
+    GroupCtx<S> c;
+    group_ctx(m, g, c);
+    typename Acc<V>::type acc[S];
+    group_dot<P, K>(m, c, g, x, acc);
+#pragma unroll
+    for (int q = 0; q < S; q++) {
+      const int s = g * S + q;
+      if (s < m.nslices) {
+        const int row = s * kSlice + lane;
+        if (row < m.n) epi(row, acc[q]);
+        end(s);
+      }
+    }
+  }
+}
+
+// ---- canonical reduction order of the Krylov dots ---------------------------
+// A dot of two n-vectors is summed in one fixed order whatever the grid, the
+// kernel or the device, and the oracle's ordered dot restates that order:
+//   1. slice sums: the 32 products of slice s (rows 32s..32s+31, zero past
+//      n) go through the warp tree below (lane l adds lane l+16, then l+8,
+//      4, 2, 1; lane 0's value);
+//   2. range sums: slices [1024j, 1024j+1024) are folded by 256 threads,
+//      thread t adding slices t, t+256, t+512, t+768 in that order from
+//      zero, then the warp tree over each warp's 32 thread sums and the 8
+//      warp sums added from zero in warp order (block_sum);
+//   3. the total: the range sums folded the same way (thread t adds ranges
+//      t, t+256, ... in order).
+constexpr int kFoldThreads = 256;
+constexpr int kFoldRange = 1024;  // slices per range
+
+__device__ __forceinline__ double warp_tree(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = __dadd_rn(v, __shfl_down_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Per-slice sums of NV dots.  Each lane sets v[k] to its row's product;
+// end(s), called by the whole warp, stores the slice's warp tree at
+// sp[k*ld + s] and clears v for the next slice (lanes past n keep zero).
+template <int NV>
+struct SliceSums {
+  double *__restrict__ sp;
+  int ld;
+  double v[NV];
+  __device__ __forceinline__ void end(int s) {
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+      const double t = warp_tree(v[k]);
+      if ((threadIdx.x & 31) == 0) sp[(size_t)k * ld + s] = t;
+      v[k] = 0.0;
+    }
+  }
+};
 
 inline int grid_for(int nslices) { return (nslices + kSlicesPerBlock - 1) / kSlicesPerBlock; }
 

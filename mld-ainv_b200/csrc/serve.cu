@@ -18,6 +18,13 @@
 // many blocks a slot gets, changes nothing.  A request's iterates are thus
 // bit-identical whether it runs alone or beside others.
 //
+// Requests on the same operator share its reads.  Active slots are grouped
+// by operator (up to kMaxMembers per group); the kernels that read A or the
+// factors (the two sweeps and the three A products) walk the group's
+// chunks, and for each chunk compute the rows of every member in turn, so a
+// chunk's values and indices come from HBM once and from the cache for the
+// other members.  The per-member arithmetic is that of a slot alone.
+//
 // The host side is an engine thread: requests queue on submit, are admitted
 // first-come first-served while a slot is free and their vectors fit in the
 // server's device arena (sized from free HBM at creation), are launched
@@ -46,6 +53,7 @@ using namespace dev;
 using namespace kstate;
 
 constexpr int kMaxSlots = 64;
+constexpr int kMaxMembers = 8;  // slots per operator group
 constexpr int kMaxGrid = 4096;
 constexpr int kGroupS = 2;                    // slices per warp in one chunk
 constexpr int kChunkRows = kBlock * kGroupS;  // 512 rows: 8 warps x 2 slices
@@ -70,9 +78,18 @@ struct SlotDesc {
   double *partials;  // 3 * nchunks
 };
 
+// Slots on one operator, served together by the operator kernels.
+struct GroupDesc {
+  int b0, nb;  // launch blocks [b0, b0 + nb)
+  int nchunks, nmem;
+  short mem[kMaxMembers];
+};
+
 struct Table {
   SlotDesc slot[kMaxSlots];
-  short block_slot[kMaxGrid];  // -1: idle block
+  GroupDesc group[kMaxSlots];
+  short block_slot[kMaxGrid];   // vector kernels: the block's slot, -1 idle
+  short block_group[kMaxGrid];  // operator kernels: the block's group, -1 idle
 };
 
 struct SlotState {
@@ -92,6 +109,7 @@ __device__ __forceinline__ SellView<V> sview(const Mat &m) {
 }
 
 // Rows of chunk c of M (warp w takes slice group 8c + w), epi(row, acc).
+// Values and indices stay cached (a group's members read them in turn).
 template <class V, int P, class X, class Epi>
 __device__ __forceinline__ void chunk_rows_p(const Mat &mm, int c, const X *__restrict__ x,
                                              Epi &epi) {
@@ -102,7 +120,7 @@ __device__ __forceinline__ void chunk_rows_p(const Mat &mm, int c, const X *__re
   GroupCtx<kGroupS> ctx;
   group_ctx(m, g, ctx);
   typename Acc<V>::type acc[kGroupS];
-  group_dot<P>(m, ctx, g, x, acc);
+  group_dot<P, 4, true, false>(m, ctx, g, x, acc);
   const int lane = threadIdx.x & 31;
 #pragma unroll
   for (int q = 0; q < kGroupS; q++) {
@@ -178,6 +196,49 @@ __device__ __forceinline__ void for_chunks(int lb, int nb, int nchunks,
   }
 }
 
+// for_chunks for the members of a group: body(c, i, pr) accumulates member
+// i's NV sums of chunk c; the chunk sums of member i go to its slot's
+// partials, folded exactly as for_chunks folds them.
+template <int NV, class Body>
+__device__ __forceinline__ void for_chunks_group(const Table *tab, const GroupDesc &gd,
+                                                 unsigned act, int lb, Body &&body) {
+  __shared__ double sh[kChunkBatch][kMaxMembers][NV][kWarps];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nb = gd.nb, nchunks = gd.nchunks;
+  for (int c0 = lb; c0 < nchunks; c0 += kChunkBatch * nb) {
+#pragma unroll
+    for (int q = 0; q < kChunkBatch; q++) {
+      const int c = c0 + q * nb;
+      if (c >= nchunks) break;  // block-uniform
+      for (int i = 0; i < gd.nmem; i++) {
+        if (!((act >> i) & 1u)) continue;
+        double pr[NV];
+#pragma unroll
+        for (int k = 0; k < NV; k++) pr[k] = 0.0;
+        body(c, i, pr);
+#pragma unroll
+        for (int k = 0; k < NV; k++) {
+          double v = pr[k];
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+          if (lane == 0) sh[q][i][k][warp] = v;
+        }
+      }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < kChunkBatch * kMaxMembers * NV; e += blockDim.x) {
+      const int q = e / (kMaxMembers * NV), i = (e / NV) % kMaxMembers, k = e % NV;
+      const int c = c0 + q * nb;
+      if (c < nchunks && i < gd.nmem && ((act >> i) & 1u)) {
+        double sum = 0.0;
+        for (int w = 0; w < kWarps; w++) sum += sh[q][i][k][w];
+        tab->slot[gd.mem[i]].partials[k * nchunks + c] = sum;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // The slot's last block (atomic ticket, no waiting) folds the chunk sums in
 // chunk order; true in that block, totals in thread 0.
 template <int NV>
@@ -218,6 +279,17 @@ __device__ __forceinline__ bool slot_fold(double (&v)[NV], const double *partial
   (void)lb;
 
 #define SRV_RUNNING (ss->phase == kRun && !st->done)
+
+// Prologue of the operator kernels: the block's group, or return.
+#define SRV_GROUP_PROLOGUE                                         \
+  const int grp = tab->block_group[blockIdx.x];                   \
+  if (grp < 0) return;                                            \
+  const GroupDesc &gd = tab->group[grp];                          \
+  const int lb = blockIdx.x - gd.b0;
+
+__device__ __forceinline__ bool slot_running(const SlotState *ss) {
+  return ss->phase == kRun && !ss->k.done;
+}
 
 // r = rt = b, x = p = v = 0, ||b||; the first rho = r.r (x0 = 0).
 __global__ void __launch_bounds__(kBlock) k_srv_init(const Table *tab, SlotState *sts) {
@@ -269,14 +341,20 @@ __global__ void __launch_bounds__(kBlock) k_srv_s(const Table *tab, SlotState *s
   for (int i = lb * kBlock + threadIdx.x; i < n; i += nb * kBlock) s[i] = r[i] - alpha * v[i];
 }
 
-// Sweep 1 of the apply: t = D^-1 .* (W^T src).
+// Sweep 1 of the apply for the active members of a group:
+// t = D^-1 .* (W^T src), chunk by chunk, every member in turn.
 template <class V, class T>
-__device__ __forceinline__ void sweep1_body(const SlotDesc &sd, const double *src, int lb,
-                                            int nb) {
-  const V *__restrict__ d = (const V *)sd.d;
-  T *__restrict__ t = (T *)sd.t;
-  auto epi = [&](int row, auto acc) { t[row] = (T)(ldd(d + row) * acc); };
-  for (int c = lb; c < sd.nchunks; c += nb) chunk_rows<V>(sd.wt, c, src, epi);
+__device__ __forceinline__ void sweep1_group(const Table *tab, const GroupDesc &gd, unsigned act,
+                                             int src, int lb) {
+  for (int c = lb; c < gd.nchunks; c += gd.nb)
+    for (int i = 0; i < gd.nmem; i++) {
+      if (!((act >> i) & 1u)) continue;
+      const SlotDesc &sd = tab->slot[gd.mem[i]];
+      const V *__restrict__ d = (const V *)sd.d;
+      T *__restrict__ t = (T *)sd.t;
+      auto epi = [&](int row, auto acc) { t[row] = (T)(ldd(d + row) * acc); };
+      chunk_rows<V>(sd.wt, c, sd.vec[src], epi);
+    }
 }
 
 // Factor precisions come in two kernel families, so each kernel's register
@@ -286,48 +364,70 @@ __host__ __device__ inline bool acc64_prec(int prec) {
   return prec == AINV_PREC_FP32_ACC64 || prec == AINV_PREC_BF16_ACC64;
 }
 
+// Members of the group that run the sweeps of family ACC (all members share
+// the operator, hence its precision).
+template <bool ACC>
+__device__ __forceinline__ unsigned sweep_members(const Table *tab, const SlotState *sts,
+                                                  const GroupDesc &gd, int prec) {
+  if (acc64_prec(prec) != ACC) return 0u;
+  unsigned act = 0u;
+  for (int i = 0; i < gd.nmem; i++)
+    if (slot_running(sts + gd.mem[i])) act |= 1u << i;
+  return act;
+}
+
 template <bool ACC>
 __global__ void __launch_bounds__(kBlock) k_srv_sweep1(const Table *tab, SlotState *sts,
                                                        int src) {
-  SRV_PROLOGUE(SRV_RUNNING && acc64_prec(tab->slot[slot].wt.prec) == ACC)
-  const double *x = sd.vec[src];
+  SRV_GROUP_PROLOGUE
+  const int prec = tab->slot[gd.mem[0]].wt.prec;
+  const unsigned act = sweep_members<ACC>(tab, sts, gd, prec);
+  if (!act) return;
   if constexpr (ACC) {
-    if (sd.wt.prec == AINV_PREC_FP32_ACC64)
-      sweep1_body<f32w, double>(sd, x, lb, nb);
+    if (prec == AINV_PREC_FP32_ACC64)
+      sweep1_group<f32w, double>(tab, gd, act, src, lb);
     else
-      sweep1_body<b16w, double>(sd, x, lb, nb);
+      sweep1_group<b16w, double>(tab, gd, act, src, lb);
   } else {
-    switch (sd.wt.prec) {
-      case AINV_PREC_FP64: sweep1_body<double, double>(sd, x, lb, nb); break;
-      case AINV_PREC_FP32: sweep1_body<float, float>(sd, x, lb, nb); break;
-      default: sweep1_body<__nv_bfloat16, float>(sd, x, lb, nb); break;
+    switch (prec) {
+      case AINV_PREC_FP64: sweep1_group<double, double>(tab, gd, act, src, lb); break;
+      case AINV_PREC_FP32: sweep1_group<float, float>(tab, gd, act, src, lb); break;
+      default: sweep1_group<__nv_bfloat16, float>(tab, gd, act, src, lb); break;
     }
   }
 }
 
-// Sweep 2 of the apply: dst = Z t.
+// Sweep 2 of the apply for the active members: dst = Z t.
 template <class V, class T>
-__device__ __forceinline__ void sweep2_body(const SlotDesc &sd, double *dst, int lb, int nb) {
-  const T *__restrict__ t = (const T *)sd.t;
-  auto epi = [&](int row, auto acc) { dst[row] = 1.0 * (double)acc; };
-  for (int c = lb; c < sd.nchunks; c += nb) chunk_rows<V>(sd.z, c, t, epi);
+__device__ __forceinline__ void sweep2_group(const Table *tab, const GroupDesc &gd, unsigned act,
+                                             int dst, int lb) {
+  for (int c = lb; c < gd.nchunks; c += gd.nb)
+    for (int i = 0; i < gd.nmem; i++) {
+      if (!((act >> i) & 1u)) continue;
+      const SlotDesc &sd = tab->slot[gd.mem[i]];
+      double *__restrict__ y = sd.vec[dst];
+      auto epi = [&](int row, auto acc) { y[row] = 1.0 * (double)acc; };
+      chunk_rows<V>(sd.z, c, (const T *)sd.t, epi);
+    }
 }
 
 template <bool ACC>
 __global__ void __launch_bounds__(kBlock) k_srv_sweep2(const Table *tab, SlotState *sts,
                                                        int dst) {
-  SRV_PROLOGUE(SRV_RUNNING && acc64_prec(tab->slot[slot].z.prec) == ACC)
-  double *y = sd.vec[dst];
+  SRV_GROUP_PROLOGUE
+  const int prec = tab->slot[gd.mem[0]].z.prec;
+  const unsigned act = sweep_members<ACC>(tab, sts, gd, prec);
+  if (!act) return;
   if constexpr (ACC) {
-    if (sd.z.prec == AINV_PREC_FP32_ACC64)
-      sweep2_body<f32w, double>(sd, y, lb, nb);
+    if (prec == AINV_PREC_FP32_ACC64)
+      sweep2_group<f32w, double>(tab, gd, act, dst, lb);
     else
-      sweep2_body<b16w, double>(sd, y, lb, nb);
+      sweep2_group<b16w, double>(tab, gd, act, dst, lb);
   } else {
-    switch (sd.z.prec) {
-      case AINV_PREC_FP64: sweep2_body<double, double>(sd, y, lb, nb); break;
-      case AINV_PREC_FP32: sweep2_body<float, float>(sd, y, lb, nb); break;
-      default: sweep2_body<__nv_bfloat16, float>(sd, y, lb, nb); break;
+    switch (prec) {
+      case AINV_PREC_FP64: sweep2_group<double, double>(tab, gd, act, dst, lb); break;
+      case AINV_PREC_FP32: sweep2_group<float, float>(tab, gd, act, dst, lb); break;
+      default: sweep2_group<__nv_bfloat16, float>(tab, gd, act, dst, lb); break;
     }
   }
 }
@@ -352,26 +452,35 @@ __device__ __forceinline__ bool srv_spmv_active(const SlotState *ss, bool *verif
 
 template <int MODE>
 __global__ void __launch_bounds__(kBlock, 4) k_srv_spmv(const Table *tab, SlotState *sts) {
-  bool verify;
-  SRV_PROLOGUE(srv_spmv_active<MODE>(ss, &verify))
-  const double *x, *w1, *w3 = nullptr;
-  double *y, *w2 = nullptr;
-  if (MODE == kBicgSigma) {
-    x = sd.vec[VF];
-    y = sd.vec[VV];
-    w1 = sd.vec[VRT];
-  } else if (MODE == kBicgOmega) {
-    x = sd.vec[VZ];
-    y = sd.vec[VT];
-    w1 = sd.vec[VS];
-  } else {
-    x = sd.vec[VX];
-    y = sd.vec[VRTRUE];
-    w1 = sd.vec[VB];
-    w2 = sd.vec[VRT];
-    w3 = sd.vec[VR];
+  SRV_GROUP_PROLOGUE
+  unsigned act = 0u, ver = 0u;
+  for (int i = 0; i < gd.nmem; i++) {
+    bool v;
+    if (srv_spmv_active<MODE>(sts + gd.mem[i], &v)) {
+      act |= 1u << i;
+      if (v) ver |= 1u << i;
+    }
   }
-  for_chunks<3>(lb, nb, sd.nchunks, sd.partials, [&](int c, double (&pr)[3]) {
+  if (!act) return;
+  for_chunks_group<3>(tab, gd, act, lb, [&](int c, int m, double (&pr)[3]) {
+    const SlotDesc &sd = tab->slot[gd.mem[m]];
+    const double *x, *w1, *w3 = nullptr;
+    double *y, *w2 = nullptr;
+    if (MODE == kBicgSigma) {
+      x = sd.vec[VF];
+      y = sd.vec[VV];
+      w1 = sd.vec[VRT];
+    } else if (MODE == kBicgOmega) {
+      x = sd.vec[VZ];
+      y = sd.vec[VT];
+      w1 = sd.vec[VS];
+    } else {
+      x = sd.vec[VX];
+      y = sd.vec[VRTRUE];
+      w1 = sd.vec[VB];
+      w2 = sd.vec[VRT];
+      w3 = sd.vec[VR];
+    }
     auto epi = [&](int i, double acc) {
       if (MODE == kTrueRes) {
         const double ri = w1[i] - acc;
@@ -391,9 +500,16 @@ __global__ void __launch_bounds__(kBlock, 4) k_srv_spmv(const Table *tab, SlotSt
     };
     chunk_rows<double>(sd.A, c, x, epi);
   });
-  double tot[3] = {0.0, 0.0, 0.0};
-  if (slot_fold<3>(tot, sd.partials, sd.nchunks, nb, &st->ticket[0]) && threadIdx.x == 0)
-    finish_dots<MODE>(st, tot, verify, w2);
+  for (int m = 0; m < gd.nmem; m++) {
+    if (!((act >> m) & 1u)) continue;
+    const int sl = gd.mem[m];
+    const SlotDesc &sd = tab->slot[sl];
+    KState *st = &sts[sl].k;
+    double tot[3] = {0.0, 0.0, 0.0};
+    if (slot_fold<3>(tot, sd.partials, gd.nchunks, gd.nb, &st->ticket[0]) && threadIdx.x == 0)
+      finish_dots<MODE>(st, tot, (ver >> m) & 1u, MODE == kTrueRes ? sd.vec[VRT] : nullptr);
+    __syncthreads();  // slot_fold's shared flag is reused by the next member
+  }
 }
 
 // x += alpha f + omega z, r = s - omega t, rn2 = r.r, rho' = rt.r.
@@ -613,18 +729,22 @@ cudaError_t capture_graph(ainv_server *srv, int fam) {
   return cudaSuccess;
 }
 
-int plan(int nslots, const int *nchunks, int grid, int *b0, int *nb) {
+// Blocks for n units (slots, or operator groups): shares of the grid in
+// proportion to weight[k], at least one block and at most cap[k] each,
+// contiguous ranges [b0[k], b0[k] + nb[k]).
+int plan_weighted(int nslots, const long long *weight, const int *cap, int grid, int *b0,
+                  int *nb) {
   if (nslots < 0 || grid < 1 || nslots > grid) {
     set_error("server block plan: %d slots for a grid of %d blocks", nslots, grid);
     return AINV_ERR_ARG;
   }
   long long total = 0;
-  for (int k = 0; k < nslots; k++) total += std::max(1, nchunks[k]);
+  for (int k = 0; k < nslots; k++) total += std::max(1LL, weight[k]);
   int used = 0;
   for (int k = 0; k < nslots; k++) {
-    const int c = std::max(1, nchunks[k]);
-    int v = (int)((long long)grid * c / std::max(1LL, total));
-    nb[k] = std::min(c, std::max(1, v));
+    const long long w = std::max(1LL, weight[k]);
+    int v = (int)((long long)grid * w / std::max(1LL, total));
+    nb[k] = std::min(std::max(1, cap[k]), std::max(1, v));
     used += nb[k];
   }
   // rounding up to one block each may overshoot: trim the largest shares
@@ -641,6 +761,13 @@ int plan(int nslots, const int *nchunks, int grid, int *b0, int *nb) {
     at += nb[k];
   }
   return AINV_SUCCESS;
+}
+
+// Slots: shares in proportion to their chunks, at most one block per chunk.
+int plan(int nslots, const int *nchunks, int grid, int *b0, int *nb) {
+  std::vector<long long> w((size_t)std::max(nslots, 0));
+  for (int k = 0; k < nslots; k++) w[(size_t)k] = std::max(1, nchunks[k]);
+  return plan_weighted(nslots, w.data(), nchunks, grid, b0, nb);
 }
 
 void fail_all(ainv_server *srv, int code, const std::string &msg) {
@@ -752,6 +879,42 @@ void engine_loop(ainv_server *srv) {
         d.b0 = b0[q];
         d.nb = nb[q];
         for (int b = d.b0; b < d.b0 + d.nb; b++) srv->tab_h->block_slot[b] = (short)order[q];
+      }
+      // operator groups: active slots on one operator, in slot order, up to
+      // kMaxMembers each; blocks in proportion to chunks x members
+      int ng = 0;
+      std::vector<int> gop;
+      for (int k : order) {
+        const int op = srv->slots[(size_t)k].req->op;
+        int g = ng - 1;
+        while (g >= 0 && !(gop[(size_t)g] == op && srv->tab_h->group[g].nmem < kMaxMembers)) g--;
+        if (g < 0) {
+          g = ng++;
+          gop.push_back(op);
+          GroupDesc &gd = srv->tab_h->group[g];
+          std::memset(&gd, 0, sizeof(gd));
+          gd.nchunks = srv->tab_h->slot[k].nchunks;
+        }
+        GroupDesc &gd = srv->tab_h->group[g];
+        gd.mem[gd.nmem++] = (short)k;
+      }
+      std::vector<long long> gw((size_t)ng);
+      std::vector<int> gcap((size_t)ng), gb0((size_t)ng), gnb((size_t)ng);
+      for (int g = 0; g < ng; g++) {
+        gw[(size_t)g] = (long long)srv->tab_h->group[g].nchunks * srv->tab_h->group[g].nmem;
+        gcap[(size_t)g] = srv->tab_h->group[g].nchunks;
+      }
+      if (plan_weighted(ng, gw.data(), gcap.data(), srv->grid, gb0.data(), gnb.data()) !=
+          AINV_SUCCESS) {
+        fail_all(srv, AINV_ERR_INTERNAL, "server group plan failed");
+        return;
+      }
+      std::fill(srv->tab_h->block_group, srv->tab_h->block_group + kMaxGrid, (short)-1);
+      for (int g = 0; g < ng; g++) {
+        GroupDesc &gd = srv->tab_h->group[g];
+        gd.b0 = gb0[(size_t)g];
+        gd.nb = gnb[(size_t)g];
+        for (int b = gd.b0; b < gd.b0 + gd.nb; b++) srv->tab_h->block_group[b] = (short)g;
       }
       ENG_TRY(cudaMemcpyAsync(srv->tab_d, srv->tab_h, sizeof(Table), cudaMemcpyHostToDevice,
                               srv->s));
@@ -884,6 +1047,7 @@ int ainv_server_create(ainv_server **out, int max_slots, size_t hbm_bytes, int i
     return fail(e, "stream");
   std::memset(srv->tab_h, 0, sizeof(Table));
   std::fill(srv->tab_h->block_slot, srv->tab_h->block_slot + kMaxGrid, (short)-1);
+  std::fill(srv->tab_h->block_group, srv->tab_h->block_group + kMaxGrid, (short)-1);
   std::memset(srv->st_h, 0, sizeof(SlotState) * (size_t)max_slots);
   e = cudaMemcpy(srv->tab_d, srv->tab_h, sizeof(Table), cudaMemcpyHostToDevice);
   if (e == cudaSuccess)

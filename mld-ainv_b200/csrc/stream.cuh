@@ -396,7 +396,7 @@ __device__ __forceinline__ typename Acc<V>::type stream_row_dot(const SellView<V
         for (int e = 0; e < P; e++) {
           const int k = k0 + e;
           if (k < kStageMaxOffsets && k < u.noff && v[e] != A(0))
-            acc = fma(v[e], (A)win[u.wofs[k < kStageMaxOffsets ? k : 0]], acc);
+            acc = madd(v[e], (A)win[u.wofs[k < kStageMaxOffsets ? k : 0]], acc);
         }
       }
     }
@@ -416,7 +416,7 @@ __device__ __forceinline__ typename Acc<V>::type stream_row_dot(const SellView<V
           xv[e] = (v[e] != A(0) && (unsigned)c < (unsigned)m.n) ? (A)__ldg(x + c) : A(0);
         }
 #pragma unroll
-        for (int e = 0; e < P; e++) acc = fma(v[e], xv[e], acc);
+        for (int e = 0; e < P; e++) acc = madd(v[e], xv[e], acc);
       }
     } else {
       // per-slot columns from shared memory, gathers from global
@@ -431,12 +431,23 @@ __device__ __forceinline__ typename Acc<V>::type stream_row_dot(const SellView<V
           xv[e] = (v[e] != A(0) && (unsigned)c < (unsigned)m.n) ? (A)__ldg(x + c) : A(0);
         }
 #pragma unroll
-        for (int e = 0; e < P; e++) acc = fma(v[e], xv[e], acc);
+        for (int e = 0; e < P; e++) acc = madd(v[e], xv[e], acc);
       }
     }
   }
   return acc;
 }
+
+// Epilogues that reduce per slice (SliceSums) define end_slice(s); it runs
+// with the whole warp once slice s is done.  Others have nothing to do.
+template <class E>
+__device__ __forceinline__ auto slice_end_impl(E &e, int s, int) -> decltype(e.end_slice(s), void()) {
+  e.end_slice(s);
+}
+template <class E>
+__device__ __forceinline__ void slice_end_impl(E &, int, long) {}
+template <class E>
+__device__ __forceinline__ void slice_end(E &e, int s) { slice_end_impl(e, s, 0); }
 
 // Persistent streaming traversal: for every row r < n of M,
 // epi.post(r, acc, rows) with acc = (M x)[r] and `rows` the reader of the
@@ -538,6 +549,7 @@ __device__ __forceinline__ bool stream_rows(const SellView<V> &m,
           const auto acc = stream_row_dot<P>(m, d, u, s, buf, L, x);
           const int row = s * kSlice + lane;
           if (row < m.n) epi.post(row, acc, sr);
+          slice_end(epi, s);
         }
       }
       __syncwarp();

@@ -756,11 +756,82 @@ int orc_ainv_apply(int n, const int *wt_irp, const int *wt_ja,
 }
 
 /* ---------------------------------------------------------- Krylov */
+/* Summation order of the Krylov dots.  PSBLAS sums a dot with the BLAS it
+ * is linked to (psb_gedot -> ddot) and then across MPI ranks, so the
+ * reference fixes no order; its iteration counts move with the BLAS and
+ * the process count.  Two orders are offered:
+ *   ORC_DOT_DEVICE (default): the device library's canonical order -- the
+ *     32 products of each 32-row slice (zero past n) summed by the tree
+ *     u[l] += u[l+16], u[l] += u[l+8], ..., u[0] += u[1]; the slice sums of
+ *     each run of 1024 slices folded by 256 "threads" (thread t adds slices
+ *     t, t+256, t+512, t+768 in order from zero), the 256 thread sums by
+ *     the same tree per group of 32 and the 8 group sums added in order;
+ *     the range sums folded the same way.  The Krylov iterates then match
+ *     the device's bit for bit;
+ *   ORC_DOT_SEQUENTIAL: one running sum in index order, the order of the
+ *     reference BLAS ddot. */
+static int g_dot_order = ORC_DOT_DEVICE;
+static double *g_hist = NULL; /* relative residual per iteration, or NULL */
+static int g_hist_cap = 0;
+
+void orc_set_dot_order(int order) { g_dot_order = order; }
+void orc_set_history(double *rel_res, int cap) {
+  g_hist = rel_res;
+  g_hist_cap = rel_res ? cap : 0;
+}
+
+static double tree32(double *u) {
+  for (int o = 16; o > 0; o >>= 1)
+    for (int l = 0; l < o; l++) u[l] = u[l] + u[l + o];
+  return u[0];
+}
+
+/* 256 running sums over src[t], src[t+256], ... then the trees. */
+static double fold256(const double *src, long count) {
+  double t[256], w[8];
+  for (int j = 0; j < 256; j++) {
+    double a = 0.0;
+    for (long s = j; s < count; s += 256) a = a + src[s];
+    t[j] = a;
+  }
+  for (int k = 0; k < 8; k++) w[k] = tree32(t + 32 * k);
+  double tot = 0.0;
+  for (int k = 0; k < 8; k++) tot = tot + w[k];
+  return tot;
+}
+
+double orc_dot_device_order(int n, const double *a, const double *b) {
+  const long ns = ((long)n + 31) / 32, nr = (ns + 1023) / 1024;
+  double *S = (double *)malloc(sizeof(double) * (size_t)(ns + nr + 1));
+  double *R = S + ns;
+#pragma omp parallel for schedule(static)
+  for (long s = 0; s < ns; s++) {
+    double u[32];
+    for (int l = 0; l < 32; l++) {
+      const long i = 32 * s + l;
+      u[l] = i < n ? a[i] * b[i] : 0.0;
+    }
+    S[s] = tree32(u);
+  }
+#pragma omp parallel for schedule(static)
+  for (long j = 0; j < nr; j++) {
+    const long c = ns - 1024 * j < 1024 ? ns - 1024 * j : 1024;
+    R[j] = fold256(S + 1024 * j, c);
+  }
+  const double tot = fold256(R, nr);
+  free(S);
+  return tot;
+}
+
 static double dot(int n, const double *a, const double *b) {
+  if (g_dot_order == ORC_DOT_DEVICE) return orc_dot_device_order(n, a, b);
   double s = 0.0;
-#pragma omp parallel for reduction(+ : s) schedule(static)
-  for (int i = 0; i < n; i++) s += a[i] * b[i];
+  for (int i = 0; i < n; i++) s = s + a[i] * b[i];
   return s;
+}
+
+static void record(int it, double rn) {
+  if (g_hist && it >= 1 && it <= g_hist_cap) g_hist[it - 1] = rn;
 }
 
 typedef struct {
@@ -809,6 +880,7 @@ int orc_cg(int n, const int *irp, const int *ja, const double *val,
     double alpha = rho / sigma;
     for (int i = 0; i < n; i++) { x[i] = x[i] + alpha * p[i]; r[i] = r[i] - alpha * q[i]; }
     rn = sqrt(dot(n, r, r)) / bn2;
+    record(it, rn);
     if (rn <= eps) rc = 0;
   }
   *iter = it;
@@ -863,6 +935,7 @@ int orc_bicgstab(int n, const int *irp, const int *ja, const double *val,
       r[i] = s[i] - omega * t[i];
     }
     rn = sqrt(dot(n, r, r)) / bn2;
+    record(it, rn);
     if (rn <= eps) rc = 0;
   }
   *iter = it;

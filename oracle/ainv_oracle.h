@@ -113,6 +113,16 @@ int orc_bicgstab(int n, const int *irp, const int *ja, const double *val,
                  const double *d, const double *b, double *x, double eps,
                  int itmax, int *iter, double *err);
 
+/* Summation order of the Krylov dots (see ainv_oracle.c): the device
+ * library's canonical order (default; iterates equal the device's bit for
+ * bit) or a sequential sum (the reference BLAS ddot). */
+enum { ORC_DOT_DEVICE = 0, ORC_DOT_SEQUENTIAL = 1 };
+void orc_set_dot_order(int order);
+double orc_dot_device_order(int n, const double *a, const double *b);
+/* Record ||r_k||/||b|| of iteration k at rel_res[k-1] (k <= cap) during the
+ * following solves; NULL stops recording. */
+void orc_set_history(double *rel_res, int cap);
+
 /* OpenMP thread control for the timed CPU baseline. */
 void orc_set_threads(int nthreads);
 int orc_get_threads(void);

@@ -76,6 +76,10 @@ def lib():
         L.orc_update_a.restype = C.c_int
         L.orc_update_a.argtypes = [C.c_int, _i32p, _i32p, _f64p, _i32p, _i32p, _f64p,
                                    _f64p, _f64p, _f64p]
+        L.orc_set_dot_order.argtypes = [C.c_int]
+        L.orc_dot_device_order.restype = C.c_double
+        L.orc_dot_device_order.argtypes = [C.c_int, _f64p, _f64p]
+        L.orc_set_history.argtypes = [C.c_void_p, C.c_int]
         L.orc_set_threads.argtypes = [C.c_int]
         L.orc_get_threads.restype = C.c_int
         _lib = L
@@ -213,15 +217,39 @@ def ainv_apply(f: Factors, x, alpha=1.0, beta=0.0, y=None, trans="N") -> np.ndar
     return y
 
 
-def solve(method: str, a: CSR, f: Factors, b, x0=None, eps=1e-9, itmax=1000):
-    """Returns (x, iterations, relative residual, status)."""
+DOT_ORDERS = {"device": 0, "sequential": 1}
+
+
+def solve(method: str, a: CSR, f: Factors, b, x0=None, eps=1e-9, itmax=1000,
+          order: str = "device", history: bool = False):
+    """Returns (x, iterations, relative residual, status), plus the
+    per-iteration ||r_k||/||b|| when history is set.  order: the summation
+    order of the dots, "device" (the device library's canonical order) or
+    "sequential" (reference BLAS ddot)."""
     x = np.zeros(a.n) if x0 is None else np.ascontiguousarray(x0, np.float64).copy()
     b = np.ascontiguousarray(b, np.float64)
     it = C.c_int(0); err = C.c_double(0.0)
     fn = lib().orc_cg if method.upper() == "CG" else lib().orc_bicgstab
-    rc = fn(a.n, a.irp, a.ja, a.val, f.wt.irp, f.wt.ja, f.wt.val, f.z.irp,
-            f.z.ja, f.z.val, f.d, b, x, eps, itmax, C.byref(it), C.byref(err))
+    hist = np.zeros(max(itmax, 1)) if history else None
+    L = lib()
+    L.orc_set_dot_order(DOT_ORDERS[order])
+    L.orc_set_history(hist.ctypes.data if history else None, len(hist) if history else 0)
+    try:
+        rc = fn(a.n, a.irp, a.ja, a.val, f.wt.irp, f.wt.ja, f.wt.val, f.z.irp,
+                f.z.ja, f.z.val, f.d, b, x, eps, itmax, C.byref(it), C.byref(err))
+    finally:
+        L.orc_set_history(None, 0)
+        L.orc_set_dot_order(0)
+    if history:
+        return x, it.value, err.value, rc, hist[:it.value].copy()
     return x, it.value, err.value, rc
+
+
+def dot_device_order(a, b) -> float:
+    """The device library's canonical-order dot of two float64 vectors."""
+    a = np.ascontiguousarray(a, np.float64)
+    b = np.ascontiguousarray(b, np.float64)
+    return lib().orc_dot_device_order(len(a), a, b)
 
 
 def set_threads(n: int) -> None:

@@ -11,4 +11,4 @@ for p in (ROOT, os.path.join(ROOT, "oracle"), os.path.join(ROOT, "mld-ainv_b200"
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200)")
-    config.addinivalue_line("markers", "slow: long-running CPU test")
+    config.addinivalue_line("markers", "slow: long-running test (full-size configurations)")

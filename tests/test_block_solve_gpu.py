@@ -11,8 +11,7 @@ import pytest
 
 import ainv
 import oracle as O
-from test_krylov_gpu import _oracle_spread, _within_spread
-from util import build_factors, device_factors, oracle_factors
+from util import build_factors, device_factors, oracle_factors, oracle_spread, within_spread
 
 torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
@@ -50,8 +49,8 @@ def test_block_cg_poisson_matches_single(prec):
         x1 = torch.zeros(n, dtype=torch.float64, device=DEV)
         single = A.solve(torch.from_numpy(b).to(DEV), x1, df, "CG", 1e-9, 1000)
         if prec == "FP64":
-            lo, hi = _oracle_spread("CG", a, oracle_factors(f), b, 1e-9, 1000, k=3)
-            assert _within_spread(res.iters[l], lo, hi), (l, res.iters[l], lo, hi)
+            lo, hi = oracle_spread("CG", a, oracle_factors(f), b, 1e-9, 1000, k=3)
+            assert within_spread(res.iters[l], lo, hi), (l, res.iters[l], lo, hi)
         assert abs(res.iters[l] - single.iter) <= max(1, int(np.ceil(0.05 * single.iter))), \
             (l, res.iters[l], single.iter)
         np.testing.assert_allclose(Xh[:, l], x1.cpu().numpy(), rtol=0, atol=1e-7)

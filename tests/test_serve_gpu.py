@@ -16,8 +16,7 @@ import pytest
 import ainv
 import oracle as O
 from ainv import serve, workload
-from test_krylov_gpu import _oracle_spread, _within_spread
-from util import build_factors, device_factors, oracle_factors
+from util import build_factors, device_factors, oracle_factors, oracle_spread, within_spread
 
 torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
@@ -92,10 +91,10 @@ def test_fp64_iterations_within_oracle_spread():
     reqs = _requests(ops, 4)
     xs, res, _ = _run(ops, reqs, max_slots=4, iters=4)
     for j, (k, b) in enumerate(reqs):
-        lo, hi = _oracle_spread("BICGSTAB", ops[k]["csr"], oracle_factors(ops[k]["fac"]), b,
+        lo, hi = oracle_spread("BICGSTAB", ops[k]["csr"], oracle_factors(ops[k]["fac"]), b,
                                 EPS, 2000)
         assert res[j].converged
-        assert _within_spread(res[j].iter, lo, hi), (j, res[j].iter, lo, hi)
+        assert within_spread(res[j].iter, lo, hi), (j, res[j].iter, lo, hi)
 
 
 def test_admission_is_bounded_by_device_memory():
@@ -183,6 +182,22 @@ def test_both_precision_families_in_one_server():
     x1, r1, _ = _run(ops, reqs, max_slots=1, iters=4, alone=True)
     x2, r2, st = _run(ops, reqs, max_slots=8, iters=4, order=list(reversed(range(8))))
     assert st["peak_active"] > 1
+    for j, (k, b) in enumerate(reqs):
+        assert r1[j].converged and r2[j].converged
+        assert r1[j].iter == r2[j].iter and np.array_equal(x1[j], x2[j]), j
+        assert _true_relres(ops[k]["csr"], x2[j], b) <= 1.05 * EPS
+
+
+def test_requests_on_one_operator_share_reads():
+    """Ten concurrent requests on one operator: the operator kernels serve
+    them as groups (8 + 2 members) that read each chunk of A and of the
+    factors once for all members; each result equals its solo run bit for
+    bit and meets the tolerance."""
+    ops = _operators("FP32")[2:3]
+    reqs = _requests(ops, 10)
+    x1, r1, _ = _run(ops, reqs, max_slots=1, iters=4, alone=True)
+    x2, r2, st = _run(ops, reqs, max_slots=10, iters=3)
+    assert st["peak_active"] == 10
     for j, (k, b) in enumerate(reqs):
         assert r1[j].converged and r2[j].converged
         assert r1[j].iter == r2[j].iter and np.array_equal(x1[j], x2[j]), j

@@ -47,3 +47,22 @@ def build_inverse_factors(solver, irp, ja, val, settings=None):
         (sv.csetr if isinstance(v, float) else sv.cseti)(k, v)
     assert sv.build(irp, ja, val) == 0, ainv.last_error()
     return sv.factors()
+
+
+def oracle_spread(method, a, of, b, eps, itmax, k=6):
+    """Iteration counts of the oracle solve on b and on k copies of b
+    perturbed at rounding level (1e-15 relative): (min, max).  Used where a
+    device loop sums its dots in an order of its own (the multi-RHS CG and
+    the server), so its count is judged against this spread widened by 5%."""
+    rng = np.random.default_rng(7)
+    its = []
+    for j in range(k + 1):
+        bj = b if j == 0 else b * (1.0 + 1e-15 * rng.standard_normal(len(b)))
+        _, it, _, rc = O.solve(method, a, of, bj, eps=eps, itmax=itmax)
+        assert rc == 0
+        its.append(it)
+    return min(its), max(its)
+
+
+def within_spread(gpu_it, lo, hi):
+    return lo - max(1, np.ceil(0.05 * lo)) <= gpu_it <= hi + max(1, np.ceil(0.05 * hi))
