@@ -257,8 +257,14 @@ def main():
     ap.add_argument("--serve-prec", default="FP32",
                     help="factor precision of the served operators (FP32: the workload's)")
     ap.add_argument("--serve-iters", type=int, default=4)
-    ap.add_argument("--leg", default="all", choices=["all", "block", "solve", "serve"],
+    ap.add_argument("--leg", default="all", choices=["all", "block", "solve", "serve", "apply"],
                     help="run one leg alone (profiler captures of its kernels)")
+    ap.add_argument("--leg-prec", default="FP32",
+                    help="factor precision of the apply / solve legs run alone")
+    ap.add_argument("--leg-pattern", default="stencil", choices=["stencil", "permuted"],
+                    help="apply leg: the stencil factors, or the same factors under a random "
+                         "symmetric permutation (per-entry column layout)")
+    ap.add_argument("--leg-reps", type=int, default=5, help="applies of the apply leg")
     ap.add_argument("--leg-itmax", type=int, default=2000,
                     help="iteration cap of the solve / block legs run alone")
     ap.add_argument("--leg-idim", type=int, default=0,
@@ -904,18 +910,45 @@ def run_block_cg(ainv, torch, dev, idim=128, m=32, itmax=2000, reps=3, single=Tr
 
 def run_leg(ainv, torch, args):
     """One leg alone, e.g. under a profiler: `block` (multi-RHS CG),
-    `solve` (one FP32-factor BiCGSTAB solve of the convection-diffusion
-    workload) or `serve` (the serving stream)."""
+    `solve` (one BiCGSTAB solve of the convection-diffusion workload with
+    `--leg-prec` factors), `apply` (applies of those factors) or `serve`
+    (the serving stream)."""
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
     if args.leg == "block":
         out = run_block_cg(ainv, torch, dev, idim=args.leg_idim or 128, itmax=args.leg_itmax,
                            reps=1, single=False)
+    elif args.leg == "apply":
+        # `--leg-reps` applies ('N') of the convection-diffusion factors in
+        # `--leg-prec`, each after an L2 flush
+        (irp, ja, val), sv = build_workload(args.leg_idim or IDIM)
+        n = len(irp) - 1
+        f = sv.factors()
+        if args.leg_pattern == "permuted":
+            f = permuted_factors(f)
+        df = ainv.DeviceFactors((f["wt_irp"], f["wt_ja"], f["wt_val"]),
+                                (f["z_irp"], f["z_ja"], f["z_val"]), f["d"], prec=args.leg_prec)
+        x = torch.from_numpy(ainv.pde.rand_uniform(0, n)).to(dev)
+        y = torch.zeros(n, dtype=torch.float64, device=dev)
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+        evs = []
+        for _ in range(args.leg_reps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            df.apply(x, y, 1.0, 0.0, "N")
+            b.record()
+            evs.append((a, b))
+        torch.cuda.synchronize()
+        out = {"n": n, "prec": args.leg_prec, "pattern": args.leg_pattern,
+               "ms": [round(a.elapsed_time(b), 4) for a, b in evs],
+               "layout": {k: df.layout_info(k) for k in ("wt", "z")}}
+        df.close()
     elif args.leg == "serve":
         out = run_serving(ainv, torch, args)
     else:
         (irp, ja, val), sv = build_workload(args.leg_idim or IDIM)
         n = len(irp) - 1
-        assert sv.cnv("FP32") == 0, ainv.last_error()
+        assert sv.cnv(args.leg_prec) == 0, ainv.last_error()
         A = ainv.DeviceOperator(irp, ja, val)
         xs = torch.from_numpy(ainv.pde.rand_uniform(0, n)).to(dev)
         b = torch.zeros(n, dtype=torch.float64, device=dev)

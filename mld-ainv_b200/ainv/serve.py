@@ -73,9 +73,7 @@ class SolveServer:
         """Queue A_op x = b.  b and x are host float64 buffers (numpy arrays
         or pinned torch tensors) kept alive here until `wait`."""
         rid = C.c_longlong(0)
-        n = self._rows.get(op)
-        if n is None:
-            raise ValueError(f"unknown operator {op}")
+        n = self._rows.get(op, 0)  # an unknown operator is the library's argument error
         check(lib().ainv_server_submit(self._h, op, hptr(b, n, "b"), hptr(x, n, "x"), eps,
                                        itmax, C.byref(rid)))
         self._buffers[rid.value] = (b, x)
