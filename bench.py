@@ -261,9 +261,9 @@ def main():
                     help="run one leg alone (profiler captures of its kernels)")
     ap.add_argument("--leg-prec", default="FP32",
                     help="factor precision of the apply / solve legs run alone")
-    ap.add_argument("--leg-pattern", default="stencil", choices=["stencil", "permuted"],
-                    help="apply leg: the stencil factors, or the same factors under a random "
-                         "symmetric permutation (per-entry column layout)")
+    ap.add_argument("--leg-pattern", default="stencil", choices=["stencil", "scattered"],
+                    help="apply leg: the stencil factors, or the same rows with scattered "
+                         "columns (per-entry column layout)")
     ap.add_argument("--leg-reps", type=int, default=5, help="applies of the apply leg")
     ap.add_argument("--leg-itmax", type=int, default=2000,
                     help="iteration cap of the solve / block legs run alone")
@@ -634,31 +634,42 @@ def run_served_200(ainv, torch, dev, irp, ja, val, sv, requests=16, slots=16, it
     return out
 
 
-def permuted_factors(f, seed=1):
-    """The factors under a seeded random symmetric permutation P: P W^T P^T,
-    P Z P^T and P D^-1 (the apply of P M P^T).  Same entries and work as the
-    stencil factors, but every row's columns scattered: the layout falls
-    back to per-entry columns (no shared offsets)."""
-    import scipy.sparse as sps
+def scattered_factors(f, band=40_000, seed=1):
+    """General (not stencil-shaped) factors with the same rows, values and
+    diagonal as f: every off-diagonal entry of row i of W^T moves to a
+    column drawn uniformly from [i - band, i), and of Z from (i, i + band]
+    (band 40,000 = one z-plane of the 200^3 grid, the stencil's own reach).
+    The factors stay unit triangular, but no two rows share a column
+    pattern, so the layout falls back to one column index per entry."""
+    rng = np.random.default_rng(seed)
     n = len(f["d"])
-    p = np.random.default_rng(seed).permutation(n)
-    out = {"d": np.ascontiguousarray(f["d"][p])}
-    for k in ("wt", "z"):
-        m = sps.csr_matrix((f[k + "_val"], f[k + "_ja"], f[k + "_irp"]), shape=(n, n))
-        m = m[p][:, p].tocsr()
-        m.sort_indices()
-        out[k + "_irp"] = m.indptr.astype(np.int32)
-        out[k + "_ja"] = m.indices.astype(np.int32)
-        out[k + "_val"] = m.data.astype(np.float64)
+    out = {"d": np.ascontiguousarray(f["d"])}
+    for k, lower in (("wt", True), ("z", False)):
+        irp, ja, val = f[k + "_irp"], f[k + "_ja"], f[k + "_val"]
+        row = np.repeat(np.arange(n, dtype=np.int64), np.diff(irp))
+        diag = ja == row
+        reach = np.minimum(row, band) if lower else np.minimum(n - 1 - row, band)
+        off = 1 + (rng.random(len(ja)) * np.maximum(reach, 1)).astype(np.int64)
+        col = np.where(diag, row, row - off if lower else row + off)
+        ok = diag | (reach > 0)
+        row, col, v = row[ok], col[ok], val[ok]
+        order = np.lexsort((col, row))
+        row, col, v = row[order], col[order], v[order]
+        keep = np.ones(len(col), bool)
+        keep[1:] = (row[1:] != row[:-1]) | (col[1:] != col[:-1])  # drop collisions
+        row, col, v = row[keep], col[keep], v[keep]
+        out[k + "_irp"] = np.concatenate([[0], np.cumsum(np.bincount(row, minlength=n))]).astype(np.int32)
+        out[k + "_ja"] = col.astype(np.int32)
+        out[k + "_val"] = np.ascontiguousarray(v, np.float64)
     return out
 
 
 def run_general_pattern(ainv, torch, dev, f, x, y, flush, stream, reps=30):
     """The apply on factors that are not stencil-shaped: the 200^3 factors
-    under a random symmetric permutation (permuted_factors), FP64, L2
-    flushed between applies."""
+    with every off-diagonal column scattered within the stencil's reach
+    (scattered_factors), FP64, L2 flushed between applies."""
     n = len(f["d"])
-    g = permuted_factors(f)
+    g = scattered_factors(f)
     df = ainv.DeviceFactors((g["wt_irp"], g["wt_ja"], g["wt_val"]),
                             (g["z_irp"], g["z_ja"], g["z_val"]), g["d"])
     lay = {k: df.layout_info(k) for k in ("wt", "z")}
@@ -689,8 +700,8 @@ def run_general_pattern(ainv, torch, dev, f, x, y, flush, stream, reps=30):
     B = csr_apply_bytes(n, len(g["wt_ja"]), len(g["z_ja"]))
     lb = layout_bytes(n, lay, 8, 8)
     df.close()
-    return {"workload": "convdiff3d_200 AINV factors under a random symmetric permutation "
-                        "(seed 1), FP64 'N' apply",
+    return {"workload": "convdiff3d_200 AINV factors, off-diagonal columns scattered "
+                        "uniformly within 40,000 of the diagonal (seed 1), FP64 'N' apply",
             "offset_slices": [lay["wt"]["offset_slices"], lay["z"]["offset_slices"]],
             "nslices": lay["wt"]["nslices"], "slots": [lay["wt"]["slots"], lay["z"]["slots"]],
             "ms": round(ms, 5), "GB/s": round(B / (ms * 1e-3) / 1e9, 2), "bytes": B,
@@ -789,10 +800,10 @@ def run_cpu_solves(ainv, torch, dev, irp, ja, val, f, extras):
         return O.Factors(O.CSR(m, d["wt_irp"], d["wt_ja"], d["wt_val"]),
                          O.CSR(m, d["z_irp"], d["z_ja"], d["z_val"]), d["d"])
 
-    def cpu(method, a_irp, a_ja, a_val, fd, b):
+    def cpu(method, a_irp, a_ja, a_val, fd, b, order="device"):
         a = O.CSR(len(a_irp) - 1, a_irp, a_ja, a_val)
         t = time.perf_counter()
-        _, it, err, rc = O.solve(method, a, factors(fd), b, eps=1e-9, itmax=3000)
+        _, it, err, rc = O.solve(method, a, factors(fd), b, eps=1e-9, itmax=3000, order=order)
         return {"s_per_solve": round(time.perf_counter() - t, 4), "iters": it,
                 "relres": err, "info": rc}
 
@@ -833,9 +844,16 @@ def run_cpu_solves(ainv, torch, dev, irp, ja, val, f, extras):
     b2 = O.spmv(O.CSR(n, irp, ja, val), xs)
     c2 = cpu("BICGSTAB", irp, ja, val, f, b2)
     g2 = extras.get("solve", {}).get("FP64", {}).get("s_per_solve")
+    gi = extras.get("solve", {}).get("FP64", {}).get("iters")
+    # the same solve with sequential dots (the reference BLAS ddot order):
+    # the count the oracle reaches when only the summation order changes
+    c2s = cpu("BICGSTAB", irp, ja, val, f, b2, order="sequential")
     out["convdiff200_bicgstab"] = {"cpu": c2, "gpu_s_per_solve": g2,
-                                           "gpu_speedup": round(c2["s_per_solve"] / g2, 2)
-                                           if g2 else None}
+                                   "gpu_speedup": round(c2["s_per_solve"] / g2, 2)
+                                   if g2 else None,
+                                   "iterations": {"gpu": gi, "oracle_device_order": c2["iters"],
+                                                  "oracle_sequential_dots": c2s["iters"],
+                                                  "gpu_equals_oracle": gi == c2["iters"]}}
     # 128^3 Poisson, one of the block leg's right-hand sides
     i4, j4, v4 = ainv.pde.gen_pde3d(128, "poisson")
     f4 = build(i4, j4, v4)
@@ -923,8 +941,8 @@ def run_leg(ainv, torch, args):
         (irp, ja, val), sv = build_workload(args.leg_idim or IDIM)
         n = len(irp) - 1
         f = sv.factors()
-        if args.leg_pattern == "permuted":
-            f = permuted_factors(f)
+        if args.leg_pattern == "scattered":
+            f = scattered_factors(f)
         df = ainv.DeviceFactors((f["wt_irp"], f["wt_ja"], f["wt_val"]),
                                 (f["z_irp"], f["z_ja"], f["z_val"]), f["d"], prec=args.leg_prec)
         x = torch.from_numpy(ainv.pde.rand_uniform(0, n)).to(dev)

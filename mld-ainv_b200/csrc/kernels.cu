@@ -34,6 +34,7 @@ template <class V, class T, int S, int P>
 __global__ void __launch_bounds__(kBlock)
     k_sweep_dscale(SellView<V> m, const double *__restrict__ x, const V *__restrict__ d,
                    T *__restrict__ t, const int *__restrict__ stop) {
+  pdl_enter();
   if (stop && *stop) return;
   for_each_row<S, P>(m, x, [&](int row, auto acc) { t[row] = (T)(ldd(d + row) * acc); });
 }
@@ -44,6 +45,7 @@ template <class V, class T, int S, int P>
 __global__ void __launch_bounds__(kBlock)
     k_sweep_axpby(SellView<V> m, const T *__restrict__ t, double alpha, double beta,
                   double *__restrict__ y, const int *__restrict__ stop) {
+  pdl_enter();
   if (stop && *stop) return;
   for_each_row<S, P>(m, t, [&](int row, auto acc) {
     y[row] = axpby_row(alpha, (double)acc, beta, beta == 0.0 ? 0.0 : y[row]);
@@ -119,6 +121,7 @@ __global__ void __launch_bounds__(kStreamThreads)
     k_stream(SellView<V> m, const StageDesc *__restrict__ stages, int nstages,
              const X *__restrict__ x, StreamLayout L, Epi epi, int *status,
              const int *__restrict__ stop) {
+  pdl_enter();
   if (stop && *stop) return;
   stream_rows<P, stream_rmax<V>()>(m, stages, nstages, x, L, epi, status);
 }
@@ -160,6 +163,13 @@ int stream_forced() {
   return forced;
 }
 }  // namespace
+bool pdl_enabled() {
+  static const bool on = [] {
+    const char *e = std::getenv("AINV_PDL");
+    return !(e && std::atoi(e) == 0);
+  }();
+  return on;
+}
 bool stream_enabled(int prec) {
   if (stream_forced() >= 0) return stream_forced() == 1;
   return prec != AINV_PREC_FP64;
@@ -311,8 +321,8 @@ struct DscaleLaunch {
   const int *stop;
   template <int S, int P>
   void run() const {
-    k_sweep_dscale<V, T, S, P><<<grid_for_groups(m.nslices, S), kBlock, 0, s>>>(
-        view<V>(m), x, (const V *)d, (T *)t, stop);
+    launch(k_sweep_dscale<V, T, S, P>, grid_for_groups(m.nslices, S), kBlock, 0, s, view<V>(m),
+           x, (const V *)d, (T *)t, stop);
   }
 };
 
@@ -326,8 +336,8 @@ struct AxpbyLaunch {
   const int *stop;
   template <int S, int P>
   void run() const {
-    k_sweep_axpby<V, T, S, P><<<grid_for_groups(m.nslices, S), kBlock, 0, s>>>(
-        view<V>(m), (const T *)t, alpha, beta, y, stop);
+    launch(k_sweep_axpby<V, T, S, P>, grid_for_groups(m.nslices, S), kBlock, 0, s, view<V>(m),
+           (const T *)t, alpha, beta, y, stop);
   }
 };
 
@@ -389,8 +399,8 @@ struct StreamLaunch {
     auto kern = k_stream<V, X, P, Epi>;
     if (!set_smem_attr((const void *)kern, smem)) return;
     const int g = occupancy_grid((const void *)kern, kStreamThreads, smem, grid);
-    kern<<<g, kStreamThreads, smem, s>>>(view<V>(m), m.stages, m.nstages, x, L, epi, status,
-                                            stop);
+    launch(kern, g, kStreamThreads, smem, s, view<V>(m), (const StageDesc *)m.stages, m.nstages,
+           x, L, epi, status, stop);
     *launched = true;
   }
 };

@@ -64,6 +64,7 @@ template <int NV, class Fin>
 __global__ void __launch_bounds__(kFoldThreads)
     k_fold(const double *__restrict__ sp, int ld, int ns, double *__restrict__ rs, int ldr,
            KState *st, Fin fin) {
+  pdl_enter();
   if (fin.skip(st)) return;
   __shared__ bool is_last;
   const int nr = gridDim.x;
@@ -167,6 +168,7 @@ __device__ __forceinline__ int nslices_of(int n) { return (n + kSlice - 1) / kSl
 // ||b||_2 (istop=2 denominator).
 __global__ void __launch_bounds__(kBlock)
     k_bnorm(int n, const double *__restrict__ b, SliceOut o) {
+  pdl_enter();
   SliceSums<1> ss{o.sp, o.ld, {0.0}};
   const int ns = nslices_of(n), lane = threadIdx.x & 31;
   for (int s = first_slice(); s < ns; s += slice_stride()) {
@@ -227,6 +229,7 @@ __global__ void __launch_bounds__(kBlock)
     k_spmv_dots(SellView<double> m, const double *__restrict__ x, double *__restrict__ y,
                 const double *__restrict__ w1, double *__restrict__ w2,
                 const double *__restrict__ w3, const KState *st, SliceOut o) {
+  pdl_enter();
   if (dots_skip<MODE>(st)) return;
   SliceSums<dots_of(MODE)> ss{o.sp, o.ld, {}};
   for_each_row_sliced<S, P>(
@@ -238,6 +241,7 @@ __global__ void __launch_bounds__(kBlock)
 __global__ void __launch_bounds__(kBlock)
     k_replace_r(int n, const double *__restrict__ rtrue, double *__restrict__ r,
                 const KState *st) {
+  pdl_enter();
   if (!st->replace) return;
   for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) r[i] = rtrue[i];
 }
@@ -295,6 +299,7 @@ __global__ void __launch_bounds__(kStreamThreads)
                   StreamLayout L, const double *__restrict__ x, double *__restrict__ y,
                   const double *__restrict__ w1, double *__restrict__ w2,
                   const double *__restrict__ w3, KState *st, SliceOut o) {
+  pdl_enter();
   if (dots_skip<MODE>(st)) return;
   EpiDots<MODE> epi{y, x, w1, w2, w3, {o.sp, o.ld, {}}};
   stream_rows<P, 1>(m, stages, nstages, x, L, epi, &st->timeout);
@@ -324,6 +329,7 @@ __global__ void __launch_bounds__(kStreamThreads)
     k_stream_cg_sweep2(SellView<V> m, const StageDesc *__restrict__ stages, int nstages,
                        StreamLayout L, const T *__restrict__ t, const double *__restrict__ r,
                        double *__restrict__ z, KState *st, SliceOut o) {
+  pdl_enter();
   if (st->done) return;
   EpiCgZ<T> epi{r, z, {o.sp, o.ld, {0.0}}};
   stream_rows<P, stream_rmax<V>()>(m, stages, nstages, t, L, epi, &st->timeout);
@@ -334,6 +340,7 @@ template <class V, class T, int S, int P>
 __global__ void __launch_bounds__(kBlock)
     k_cg_sweep2(SellView<V> m, const T *__restrict__ t, const double *__restrict__ r,
                 double *__restrict__ z, const KState *st, SliceOut o) {
+  pdl_enter();
   if (st->done) return;
   SliceSums<1> ss{o.sp, o.ld, {0.0}};
   for_each_row_sliced<S, P>(
@@ -350,6 +357,7 @@ __global__ void __launch_bounds__(kBlock)
 __global__ void __launch_bounds__(kBlock)
     k_cg_ident(int n, const double *__restrict__ r, double *__restrict__ z, const KState *st,
                SliceOut o) {
+  pdl_enter();
   if (st->done) return;
   SliceSums<1> ss{o.sp, o.ld, {0.0}};
   const int ns = nslices_of(n), lane = threadIdx.x & 31;
@@ -366,6 +374,7 @@ __global__ void __launch_bounds__(kBlock)
 // CG: p = z (first iteration) or p = z + beta p.
 __global__ void __launch_bounds__(kBlock)
     k_cg_p(int n, const double *__restrict__ z, double *__restrict__ p, const KState *st) {
+  pdl_enter();
   if (st->done) return;
   const int i = blockIdx.x * kBlock + threadIdx.x;
   if (i >= n) return;
@@ -376,6 +385,7 @@ __global__ void __launch_bounds__(kBlock)
 __global__ void __launch_bounds__(kBlock)
     k_cg_xr(int n, const double *__restrict__ p, const double *__restrict__ q,
             double *__restrict__ x, double *__restrict__ r, const KState *st, SliceOut o) {
+  pdl_enter();
   if (st->done) return;
   const double alpha = st->alpha;
   SliceSums<1> ss{o.sp, o.ld, {0.0}};
@@ -396,6 +406,7 @@ __global__ void __launch_bounds__(kBlock)
 __global__ void __launch_bounds__(kBlock)
     k_bicg_p(int n, const double *__restrict__ r, const double *__restrict__ v,
              double *__restrict__ p, const KState *st) {
+  pdl_enter();
   if (st->done) return;
   const int i = blockIdx.x * kBlock + threadIdx.x;
   if (i >= n) return;
@@ -406,6 +417,7 @@ __global__ void __launch_bounds__(kBlock)
 __global__ void __launch_bounds__(kBlock)
     k_bicg_s(int n, const double *__restrict__ r, const double *__restrict__ v,
              double *__restrict__ s, const KState *st) {
+  pdl_enter();
   if (st->done) return;
   const int i = blockIdx.x * kBlock + threadIdx.x;
   if (i >= n) return;
@@ -418,6 +430,7 @@ __global__ void __launch_bounds__(kBlock)
               const double *__restrict__ s, const double *__restrict__ t,
               const double *__restrict__ rt, double *__restrict__ x,
               double *__restrict__ r, const KState *st, SliceOut o) {
+  pdl_enter();
   if (st->done) return;
   const double alpha = st->alpha, omega = st->omega;
   SliceSums<2> ss{o.sp, o.ld, {0.0, 0.0}};
@@ -449,8 +462,8 @@ struct CgSweep2Launch {
   template <int S, int P>
   void run() const {
     auto kern = k_cg_sweep2<V, T, S, P>;
-    kern<<<std::min(G, wave_grid((const void *)kern, m.n)), kBlock, 0, s>>>(
-        view<V>(m), (const T *)t, r, z, st, o);
+    launch(kern, std::min(G, wave_grid((const void *)kern, m.n)), kBlock, 0, s, view<V>(m),
+           (const T *)t, r, z, st, o);
   }
 };
 
@@ -474,8 +487,8 @@ struct StreamCgSweep2Launch {
     auto kern = k_stream_cg_sweep2<V, T, P>;
     if (!set_smem_attr((const void *)kern, smem)) return;
     const int g = occupancy_grid((const void *)kern, kStreamThreads, smem, grid);
-    kern<<<g, kStreamThreads, smem, s>>>(view<V>(m), m.stages, m.nstages, L, (const T *)t, r,
-                                            z, st, o);
+    launch(kern, g, kStreamThreads, smem, s, view<V>(m), m.stages, m.nstages, L, (const T *)t, r, z,
+           st, o);
     *launched = true;
   }
 };
@@ -512,8 +525,8 @@ struct SpmvDotsLaunch {
   template <int S, int P>
   void run() const {
     auto kern = k_spmv_dots<MODE, S, P>;
-    kern<<<std::min(G, wave_grid((const void *)kern, A.n)), kBlock, 0, s>>>(A, x, y, w1, w2, w3,
-                                                                          st, pp);
+    launch(kern, std::min(G, wave_grid((const void *)kern, A.n)), kBlock, 0, s, A, x, y, w1, w2, w3,
+           st, pp);
   }
 };
 
@@ -537,8 +550,8 @@ struct StreamDotsLaunch {
     auto kern = k_stream_dots<MODE, P>;
     if (!set_smem_attr((const void *)kern, smem)) return;
     const int g = occupancy_grid((const void *)kern, kStreamThreads, smem, grid);
-    kern<<<g, kStreamThreads, smem, s>>>(view<double>(m), m.stages, m.nstages, L, x, y, w1,
-                                            w2, w3, st, pp);
+    launch(kern, g, kStreamThreads, smem, s, view<double>(m), m.stages, m.nstages, L, x, y, w1, w2,
+           w3, st, pp);
     *launched = true;
   }
 };
@@ -597,7 +610,7 @@ struct KrylovWs {
   // Fold the slice sums of the reduction just enqueued (NV dots).
   template <int NV, class Fin>
   void fold(const Fin &fin) const {
-    k_fold<NV, Fin><<<nr, kFoldThreads, 0, s>>>(sp, ld, ns, rs, ldr, st, fin);
+    launch(k_fold<NV, Fin>, nr, kFoldThreads, 0, s, sp, ld, ns, rs, ldr, st, fin);
   }
 };
 
@@ -683,24 +696,24 @@ int enqueue_iteration(KrylovWs *w, const ainv_handle *h, const ainv_csr *a, int 
       AINV_TRY(launch_sweep_dscale(h->wt, h->d, r, h->t, s, stop, &st->timeout));
       precond_sweep2_cg(h, r, z, st, pp, G, s);
     } else {
-      k_cg_ident<<<std::min(G, wave_grid((const void *)k_cg_ident, n)), kBlock, 0, s>>>(n, r, z,
-                                                                                         st, pp);
+      launch(k_cg_ident, std::min(G, wave_grid((const void *)k_cg_ident, n)), kBlock, 0, s, n, r, z,
+             st, pp);
     }
     w->fold<1>(FinCgRho{});
-    k_cg_p<<<Gv, kBlock, 0, s>>>(n, z, p, st);
+    launch(k_cg_p, Gv, kBlock, 0, s, n, z, p, st);
     spmv_dots<kCgSigma>(A, G, s, p, q, nullptr, nullptr, nullptr, st, pp);
     w->fold<1>(FinDots<kCgSigma>{nullptr});
-    k_cg_xr<<<std::min(G, wave_grid((const void *)k_cg_xr, n)), kBlock, 0, s>>>(n, p, q, x, r,
-                                                                                 st, pp);
+    launch(k_cg_xr, std::min(G, wave_grid((const void *)k_cg_xr, n)), kBlock, 0, s, n, p, q, x, r,
+           st, pp);
     w->fold<1>(FinCgXr{});
     spmv_dots<kTrueRes>(A, G, s, x, w->v(RTRUE), w->v(BW), nullptr, r, st, pp);
     w->fold<3>(FinDots<kTrueRes>{nullptr});
-    k_replace_r<<<wave_grid((const void *)k_replace_r, n), kBlock, 0, s>>>(n, w->v(RTRUE), r,
-                                                                         st);
+    launch(k_replace_r, wave_grid((const void *)k_replace_r, n), kBlock, 0, s, n, w->v(RTRUE), r,
+           st);
   } else {
     double *r = w->v(R), *rt = w->v(RT), *p = w->v(P), *v = w->v(V), *f = w->v(F),
            *sv = w->v(S), *z = w->v(Z), *t = w->v(T), *x = w->v(XW);
-    k_bicg_p<<<Gv, kBlock, 0, s>>>(n, r, v, p, st);
+    launch(k_bicg_p, Gv, kBlock, 0, s, n, r, v, p, st);
     if (h) {
       AINV_TRY(ainv_apply_async(h, 'N', 1.0, p, 0.0, f, s, stop, &st->timeout));
     } else {
@@ -708,7 +721,7 @@ int enqueue_iteration(KrylovWs *w, const ainv_handle *h, const ainv_csr *a, int 
     }
     spmv_dots<kBicgSigma>(A, G, s, f, v, rt, nullptr, nullptr, st, pp);
     w->fold<1>(FinDots<kBicgSigma>{rt});
-    k_bicg_s<<<Gv, kBlock, 0, s>>>(n, r, v, sv, st);
+    launch(k_bicg_s, Gv, kBlock, 0, s, n, r, v, sv, st);
     if (h) {
       AINV_TRY(ainv_apply_async(h, 'N', 1.0, sv, 0.0, z, s, stop, &st->timeout));
     } else {
@@ -716,13 +729,13 @@ int enqueue_iteration(KrylovWs *w, const ainv_handle *h, const ainv_csr *a, int 
     }
     spmv_dots<kBicgOmega>(A, G, s, z, t, sv, nullptr, nullptr, st, pp);
     w->fold<2>(FinDots<kBicgOmega>{rt});
-    k_bicg_xr<<<std::min(G, wave_grid((const void *)k_bicg_xr, n)), kBlock, 0, s>>>(
-        n, f, z, sv, t, rt, x, r, st, pp);
+    launch(k_bicg_xr, std::min(G, wave_grid((const void *)k_bicg_xr, n)), kBlock, 0, s, n, f, z, sv,
+           t, rt, x, r, st, pp);
     w->fold<2>(FinBicgXr{});
     spmv_dots<kTrueRes>(A, G, s, x, w->v(RTRUE), w->v(BW), rt, r, st, pp);
     w->fold<3>(FinDots<kTrueRes>{rt});
-    k_replace_r<<<wave_grid((const void *)k_replace_r, n), kBlock, 0, s>>>(n, w->v(RTRUE), r,
-                                                                         st);
+    launch(k_replace_r, wave_grid((const void *)k_replace_r, n), kBlock, 0, s, n, w->v(RTRUE), r,
+           st);
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
@@ -792,8 +805,8 @@ int krylov_solve(const ainv_handle *h, ainv_csr *a, const double *b, double *x, 
   *w->hst = init;
   AINV_CUDA_TRY(cudaMemcpyAsync(w->st, w->hst, sizeof(KState), cudaMemcpyHostToDevice, w->s));
   const DevSell &A = a->a;
-  k_bnorm<<<std::min(w->G, wave_grid((const void *)k_bnorm, n)), kBlock, 0, w->s>>>(
-      n, w->v(BW), w->out());
+  launch(k_bnorm, std::min(w->G, wave_grid((const void *)k_bnorm, n)), kBlock, 0, w->s, n, w->v(BW),
+         w->out());
   w->fold<1>(FinBnorm{});
   double *rt0 = method == AINV_KRYLOV_BICGSTAB ? w->v(RT) : nullptr;
   spmv_dots<kInit>(A, w->G, w->s, w->v(XW), w->v(R), w->v(BW), rt0, nullptr, w->st, w->out());

@@ -5,6 +5,7 @@
 #include <cuda_bf16.h>
 
 #include <type_traits>
+#include <utility>
 
 #include "internal.h"
 
@@ -34,6 +35,20 @@ __device__ __forceinline__ float ldd(const float *p) { return __ldg(p); }
 __device__ __forceinline__ float ldd(const __nv_bfloat16 *p) {
   unsigned short u = __ldg(reinterpret_cast<const unsigned short *>(p));
   return __uint_as_float(((unsigned)u) << 16);
+}
+
+// ---- programmatic dependent launch ------------------------------------------
+// The kernels of the apply and of the Krylov loop are launched with
+// programmatic stream serialisation (launch() below): a kernel may be
+// scheduled while its predecessor in the stream drains, so the launch
+// latency and block rasterisation of one step hide behind the tail of the
+// previous one.  Each such kernel starts with pdl_enter(): griddepcontrol.
+// wait returns once the preceding grid has completed and its writes are
+// visible (at once when the kernel was launched without the attribute), and
+// launch_dependents lets the next kernel be scheduled as this one runs.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
 // c + a*b of the row accumulations.  In FP64 the product and the sum each
@@ -498,6 +513,24 @@ struct SliceSums {
     }
   }
 };
+
+// Host side of the programmatic launch: k<<<g, b, smem, s>>>(args...) with
+// the programmatic-serialisation attribute (AINV_PDL=0 launches plainly).
+bool pdl_enabled();
+template <class... P, class... A>
+inline void launch(void (*k)(P...), dim3 g, dim3 b, size_t smem, cudaStream_t s, A &&...a) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = g;
+  cfg.blockDim = b;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, k, std::forward<A>(a)...);
+}
 
 inline int grid_for(int nslices) { return (nslices + kSlicesPerBlock - 1) / kSlicesPerBlock; }
 

@@ -2,7 +2,10 @@
 against the CPU oracle on the same factors and inputs, through the C-ABI.
 
 Tolerances (norm-wise relative, ||y - y_oracle||_inf / ||y_oracle||_inf):
-  FP64 factors: 1e-12 (the north-star bound for the FP64 apply)
+  FP64 factors: 1e-12 (the north-star bound for the FP64 apply); the 'N'
+                apply is moreover bit-identical to the oracle's: both sum
+                each row in column order with every product and sum
+                rounded once, and form alpha*acc + beta*y alike
   FP32 factors: 5e-6   (float32 storage and accumulation)
   BF16 factors: 3e-2   (bfloat16 storage, float32 accumulation)
 """
@@ -60,6 +63,8 @@ def test_apply_fp64_parity(idim, kind, beta, trans):
         y = _gpu_apply(df, x, alpha, beta_, y0, trans)
         ref = O.ainv_apply(of, x, alpha, beta_, y0, trans)
         assert relerr(y, ref) <= 1e-12, (alpha, beta_)
+        if trans == "N":
+            np.testing.assert_array_equal(y, ref)
 
 
 def test_apply_full_size_convdiff_200():
@@ -73,6 +78,7 @@ def test_apply_full_size_convdiff_200():
     y = _gpu_apply(df, x, 1.0, 0.0, np.zeros(n), "N")
     ref = O.ainv_apply(oracle_factors(f), x, 1.0, 0.0, None, "N")
     assert relerr(y, ref) <= 1e-12
+    np.testing.assert_array_equal(y, ref)
     x2 = ainv.pde.rand_uniform(1, n)
     y2 = _gpu_apply(df, x2, 1.0, 0.0, np.zeros(n), "N")
     y12 = _gpu_apply(df, 2.0 * x - 3.0 * x2, 1.0, 0.0, np.zeros(n), "N")

@@ -211,3 +211,4 @@ def test_spmv_matches_oracle():
     ref = O.spmv(O.CSR(n, irp, ja, val), x, 2.0, -1.0, y0)
     y = yd.cpu().numpy()
     assert np.abs(y - ref).max() <= 1e-12 * np.abs(ref).max()
+    np.testing.assert_array_equal(y, ref)  # alpha*acc + beta*y formed as the oracle forms it
