@@ -257,7 +257,8 @@ def main():
     ap.add_argument("--serve-prec", default="FP32",
                     help="factor precision of the served operators (FP32: the workload's)")
     ap.add_argument("--serve-iters", type=int, default=4)
-    ap.add_argument("--leg", default="all", choices=["all", "block", "solve", "serve", "apply"],
+    ap.add_argument("--leg", default="all",
+                    choices=["all", "block", "solve", "serve", "apply", "served200"],
                     help="run one leg alone (profiler captures of its kernels)")
     ap.add_argument("--leg-prec", default="FP32",
                     help="factor precision of the apply / solve legs run alone")
@@ -565,7 +566,8 @@ def run_extras(ainv, torch, dev, irp, ja, val, f, sv, flush, stream, fp64_ms):
     return out
 
 
-def run_served_200(ainv, torch, dev, irp, ja, val, sv, requests=16, slots=16, iters=4):
+def run_served_200(ainv, torch, dev, irp, ja, val, sv, requests=16, slots=16, iters=4,
+                   modes=("FP32_ACC64", "BF16_ACC64", "FP32", "BF16", "FP64"), plain=True):
     """The mixed-precision, served solve on the 200^3 convection-diffusion
     case against the plain FP64 GPU solve.  `requests` right-hand sides
     b_k = A x*_k (x*_k ~ U(-1,1), seed k), BiCGSTAB to 1e-9 from x0 = 0:
@@ -587,25 +589,11 @@ def run_served_200(ainv, torch, dev, irp, ja, val, sv, requests=16, slots=16, it
         bh.append(bd.cpu().pin_memory())
     out = {"workload": "convdiff3d_200_upwind_bicgstab_1e-9_ainv_llk_drop0.1_fill20",
            "requests": requests, "slots": slots, "iters_per_launch": iters}
-    # plain FP64 solves, one after another (device b and x)
-    assert sv.cnv("FP64") == 0, ainv.last_error()
-    its, t_tot = [], 0.0
-    x = torch.zeros(n, dtype=torch.float64, device=dev)
-    A.solve(bh[0].to(dev), x, sv.device, "BICGSTAB", 1e-9, 2000)  # warm-up
-    for k in range(requests):
-        b = bh[k].to(dev)
-        x.zero_()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        r = A.solve(b, x, sv.device, "BICGSTAB", 1e-9, 2000)
-        torch.cuda.synchronize()
-        t_tot += time.perf_counter() - t0
-        its.append(r.iter)
-    plain = requests / t_tot
-    out["plain_fp64"] = {"solves_per_s": round(plain, 3), "iters_mean": round(float(np.mean(its)), 2),
-                         "iters": its}
     out["served"] = {}
-    for mode in ("FP32_ACC64", "BF16_ACC64", "FP32", "BF16", "FP64"):
+    plain_sps = None
+    if plain:
+        plain_sps, out["plain_fp64"] = plain_fp64_solves(ainv, torch, dev, A, sv, bh, requests)
+    for mode in modes:
         assert sv.cnv(mode) == 0, ainv.last_error()
         xh = [torch.zeros(n, dtype=torch.float64).pin_memory() for _ in range(requests)]
         with serve.SolveServer(max_slots=slots, iters_per_launch=iters) as srv:
@@ -619,7 +607,8 @@ def run_served_200(ainv, torch, dev, irp, ja, val, sv, requests=16, slots=16, it
         lat = np.array([q.latency for q in res]) * 1e3
         sps = requests / (t_last - t_first)
         out["served"][mode] = {
-            "solves_per_s": round(sps, 3), "vs_plain_fp64": round(sps / plain, 3),
+            "solves_per_s": round(sps, 3),
+            "vs_plain_fp64": round(sps / plain_sps, 3) if plain_sps else None,
             "converged": int(sum(q.converged for q in res)),
             "max_final_fp64_relres": float(max(q.err for q in res)),
             "max_err_vs_xstar": float(max(np.abs(xh[k].numpy() - xstar[k]).max()
@@ -632,6 +621,28 @@ def run_served_200(ainv, torch, dev, irp, ja, val, sv, requests=16, slots=16, it
     assert sv.cnv("FP64") == 0, ainv.last_error()
     A.close()
     return out
+
+
+def plain_fp64_solves(ainv, torch, dev, A, sv, bh, requests):
+    """The plain FP64 GPU solve of the same right-hand sides, one after
+    another (device b and x): (solves/s, record)."""
+    n = A.n
+    assert sv.cnv("FP64") == 0, ainv.last_error()
+    its, t_tot = [], 0.0
+    x = torch.zeros(n, dtype=torch.float64, device=dev)
+    A.solve(bh[0].to(dev), x, sv.device, "BICGSTAB", 1e-9, 2000)  # warm-up
+    for k in range(requests):
+        b = bh[k].to(dev)
+        x.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = A.solve(b, x, sv.device, "BICGSTAB", 1e-9, 2000)
+        torch.cuda.synchronize()
+        t_tot += time.perf_counter() - t0
+        its.append(r.iter)
+    sps = requests / t_tot
+    return sps, {"solves_per_s": round(sps, 3), "iters_mean": round(float(np.mean(its)), 2),
+                 "iters": its}
 
 
 def scattered_factors(f, band=40_000, seed=1):
@@ -929,12 +940,19 @@ def run_block_cg(ainv, torch, dev, idim=128, m=32, itmax=2000, reps=3, single=Tr
 def run_leg(ainv, torch, args):
     """One leg alone, e.g. under a profiler: `block` (multi-RHS CG),
     `solve` (one BiCGSTAB solve of the convection-diffusion workload with
-    `--leg-prec` factors), `apply` (applies of those factors) or `serve`
-    (the serving stream)."""
+    `--leg-prec` factors), `apply` (applies of those factors), `served200`
+    (`--leg-reps` such solves served together) or `serve` (the serving
+    stream)."""
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
     if args.leg == "block":
         out = run_block_cg(ainv, torch, dev, idim=args.leg_idim or 128, itmax=args.leg_itmax,
                            reps=1, single=False)
+    elif args.leg == "served200":
+        # `--leg-reps` requests of the 200^3 (or --leg-idim) solve served
+        # together with `--leg-prec` factors, no plain comparison
+        (irp, ja, val), sv = build_workload(args.leg_idim or IDIM)
+        out = run_served_200(ainv, torch, dev, irp, ja, val, sv, requests=args.leg_reps,
+                             slots=args.leg_reps, modes=(args.leg_prec,), plain=False)
     elif args.leg == "apply":
         # `--leg-reps` applies ('N') of the convection-diffusion factors in
         # `--leg-prec`, each after an L2 flush

@@ -3,23 +3,25 @@
 // as driven at tests/pdegen/ppde3d.f90:280-281.
 //
 // Every scalar of the recurrence (rho, alpha, omega, beta, norms, status)
-// lives in device memory and is produced by the fold kernel that completes
-// the corresponding reduction, so one iteration is a fixed sequence of
-// launches with no host round trip.  Iterations are issued in chunks
-// captured once into a CUDA graph; when the loop has converged (or broken
-// down) a device flag makes every later kernel of the chunk return at once,
-// and the host inspects the state once per chunk.
+// lives in device memory and is produced by the kernel that completes the
+// corresponding reduction, so one iteration is a fixed sequence of launches
+// with no host round trip.  Iterations are issued in chunks captured once
+// into a CUDA graph; when the loop has converged (or broken down) a device
+// flag makes every later kernel of the chunk return at once, and the host
+// inspects the state once per chunk.
 //
 // Reproducible iterates.  Every dot is summed in the canonical order of
 // sell_device.cuh (slice trees, then 1024-slice ranges, then the ranges),
 // which does not depend on the grid, the kernel that computes the products
-// or the device: the producing kernel stores one sum per 32-row slice and a
-// fold kernel (k_fold) reduces them.  The library is compiled without
-// floating-point contraction, so every FP64 product and sum of the vector
-// updates rounds once, as in the reference's Fortran on a target without
-// fused multiply-add, and the row sums of the sweeps and of A use the same
-// unfused order (madd).  With FP64 factors the iterates therefore equal,
-// bit for bit, those of the oracle's ordered-dot Krylov loop.
+// or the device: the producing kernel stores one sum per 32-row slice, the
+// warp that completes a range folds it, and the warp that completes the
+// last range folds the total and applies the scalar step.  The library is
+// compiled without floating-point contraction, so every FP64 product and
+// sum of the vector updates rounds once, as in the reference's Fortran on a
+// target without fused multiply-add, and the row sums of the sweeps and of
+// A use the same unfused order (madd).  With FP64 factors the iterates
+// therefore equal, bit for bit, those of the oracle's ordered-dot Krylov
+// loop.
 //
 // Fused steps: the A product and the dots that consume it (p.q, rt.v, t.t
 // and t.s) share one kernel; the Z sweep of the preconditioner and the CG
@@ -47,67 +49,12 @@ using namespace kstate;
 constexpr int kChunk = 8;  // iterations per captured graph launch
 constexpr int kHistCap = 8192;  // iterations whose residual is recorded
 
-// Where a reduction kernel stores its slice sums: dot k of slice s at
-// sp[k*ld + s].
-struct SliceOut {
-  double *sp;
-  int ld;
-};
-
-// ---- the fold ----------------------------------------------------------------
-// Block j reduces the slice sums of range j (kFoldRange slices) and stores
-// the range sums; the last block to finish (atomic ticket, no waiting)
-// folds the range sums and hands the totals to fin.  fin.skip(st) repeats
-// the producing kernel's early-exit test, so a reduction that did not run
-// is not folded.
-template <int NV, class Fin>
-__global__ void __launch_bounds__(kFoldThreads)
-    k_fold(const double *__restrict__ sp, int ld, int ns, double *__restrict__ rs, int ldr,
-           KState *st, Fin fin) {
-  pdl_enter();
-  if (fin.skip(st)) return;
-  __shared__ bool is_last;
-  const int nr = gridDim.x;
-  const int s0 = blockIdx.x * kFoldRange, s1 = min(ns, s0 + kFoldRange);
-  double v[NV];
-#pragma unroll
-  for (int k = 0; k < NV; k++) {
-    double a = 0.0;
-    for (int s = s0 + threadIdx.x; s < s1; s += kFoldThreads) a = __dadd_rn(a, sp[(size_t)k * ld + s]);
-    v[k] = a;
-  }
-  block_sum<NV>(v);
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int k = 0; k < NV; k++) rs[(size_t)k * ldr + blockIdx.x] = v[k];
-    __threadfence();
-    is_last = atomicAdd(&st->ticket[3], 1u) == (unsigned)nr - 1;
-  }
-  __syncthreads();
-  if (!is_last) return;
-  __threadfence();
-#pragma unroll
-  for (int k = 0; k < NV; k++) {
-    double a = 0.0;
-    for (int r = threadIdx.x; r < nr; r += kFoldThreads)
-      a = __dadd_rn(a, __ldcg(rs + (size_t)k * ldr + r));
-    v[k] = a;
-  }
-  block_sum<NV>(v);
-  if (threadIdx.x == 0) {
-    st->ticket[3] = 0u;
-    fin(st, v);
-  }
-}
-
-// Early-exit test of the reductions that stop once the loop is done.
-struct UntilDone {
-  __device__ __forceinline__ bool skip(const KState *st) const { return st->done != 0; }
-};
-
+// ---- scalar steps ------------------------------------------------------------
+// Each reduction ends in lane 0 of the warp that folds its total (SliceSums
+// in sell_device.cuh), which applies one of these to the state.
 struct FinBnorm {
-  __device__ __forceinline__ bool skip(const KState *) const { return false; }
-  __device__ __forceinline__ void operator()(KState *st, const double (&v)[1]) const {
+  KState *st;
+  __device__ __forceinline__ void operator()(const double (&v)[1]) const {
     const double bn = sqrt(v[0]);
     st->bn2 = (bn == 0.0) ? 1.0 : bn;
   }
@@ -125,36 +72,36 @@ constexpr int dots_of(int mode) {
 }
 
 // Scalar step of an SpMV-with-dots reduction (w2: rt for BiCGSTAB, else
-// null, as finish_dots expects).
+// null, as finish_dots expects; verify: the true-residual pass confirms a
+// convergence claim, decided when the kernel started).
 template <int MODE>
 struct FinDots {
+  KState *st;
   const double *w2;
-  __device__ __forceinline__ bool skip(const KState *st) const {
-    if (MODE == kTrueRes) return !true_res_verify(st) && !true_res_periodic(st);
-    return st->done != 0;
-  }
-  __device__ __forceinline__ void operator()(KState *st, const double (&v)[dots_of(MODE)]) const {
+  bool verify;
+  __device__ __forceinline__ void operator()(const double (&v)[dots_of(MODE)]) const {
     double pr[3] = {0.0, 0.0, 0.0};
 #pragma unroll
     for (int k = 0; k < dots_of(MODE); k++) pr[k] = v[k];
-    finish_dots<MODE>(st, pr, MODE == kTrueRes && true_res_verify(st), w2);
+    finish_dots<MODE>(st, pr, verify, w2);
   }
 };
 
-struct FinCgRho : UntilDone {
-  __device__ __forceinline__ void operator()(KState *st, const double (&v)[1]) const {
-    cg_take_rho(st, v[0]);
-  }
+struct FinCgRho {
+  KState *st;
+  __device__ __forceinline__ void operator()(const double (&v)[1]) const { cg_take_rho(st, v[0]); }
 };
 
-struct FinCgXr : UntilDone {
-  __device__ __forceinline__ void operator()(KState *st, const double (&v)[1]) const {
+struct FinCgXr {
+  KState *st;
+  __device__ __forceinline__ void operator()(const double (&v)[1]) const {
     finish_iteration(st, v[0]);
   }
 };
 
-struct FinBicgXr : UntilDone {
-  __device__ __forceinline__ void operator()(KState *st, const double (&v)[2]) const {
+struct FinBicgXr {
+  KState *st;
+  __device__ __forceinline__ void operator()(const double (&v)[2]) const {
     finish_iteration(st, v[0]);
     bicg_next_rho(st, v[1]);
   }
@@ -162,20 +109,42 @@ struct FinBicgXr : UntilDone {
 
 // ---- reduction kernels ---------------------------------------------------------
 // Vector-only kernels walk warp-per-slice (lane = row), so the slice trees
-// see the same lane order as in the SpMV kernels.
+// see the same lane order as in the SpMV kernels.  A warp takes kVecSlices
+// consecutive slices per step and issues all of their loads before the
+// first slice's tree.
 __device__ __forceinline__ int nslices_of(int n) { return (n + kSlice - 1) / kSlice; }
+constexpr int kVecSlices = 4;
+
+// for_slices(n, body, end): body(j, i) for row i of slice j of the step
+// (rows < n), then end(j, s) with the whole warp for each slice s < ns.
+template <class Body, class End>
+__device__ __forceinline__ void for_slices(int n, Body &&body, End &&end) {
+  const int ns = nslices_of(n), lane = threadIdx.x & 31;
+  for (int q = first_slice(); q * kVecSlices < ns; q += slice_stride()) {
+#pragma unroll
+    for (int j = 0; j < kVecSlices; j++) {
+      const int i = (q * kVecSlices + j) * kSlice + lane;
+      if (i < n) body(j, i);
+    }
+#pragma unroll
+    for (int j = 0; j < kVecSlices; j++)
+      if (q * kVecSlices + j < ns) end(j, q * kVecSlices + j);
+  }
+}
 
 // ||b||_2 (istop=2 denominator).
 __global__ void __launch_bounds__(kBlock)
-    k_bnorm(int n, const double *__restrict__ b, SliceOut o) {
+    k_bnorm(int n, const double *__restrict__ b, KState *st, FoldBuf fb) {
   pdl_enter();
-  SliceSums<1> ss{o.sp, o.ld, {0.0}};
-  const int ns = nslices_of(n), lane = threadIdx.x & 31;
-  for (int s = first_slice(); s < ns; s += slice_stride()) {
-    const int i = s * kSlice + lane;
-    if (i < n) ss.v[0] = b[i] * b[i];
-    ss.end(s);
-  }
+  SliceSums<1, FinBnorm> ss{fb, FinBnorm{st}, {0.0}};
+  double p[kVecSlices] = {};
+  for_slices(
+      n, [&](int j, int i) { p[j] = b[i] * b[i]; },
+      [&](int j, int s) {
+        ss.v[0] = p[j];
+        p[j] = 0.0;
+        ss.end(s);
+      });
 }
 
 // y = A x with the reductions each caller needs (see MODE):
@@ -188,11 +157,12 @@ __global__ void __launch_bounds__(kBlock)
 //               iterations and once when the recurrence claims convergence.
 //               Decides whether r is replaced (k_replace_r) and whether the
 //               convergence stands; w2 = rt for BiCGSTAB's rho.
-// The row products of the dots go to ss; the fold does the scalar step.
-template <int MODE>
+// The row products of the dots go to the slice sums; the fold of the last
+// range does the scalar step.
+template <int MODE, class SS>
 __device__ __forceinline__ void dots_row(int i, double acc, const double *__restrict__ x,
                                          double *__restrict__ y, const double *w1, double *w2,
-                                         const double *w3, SliceSums<dots_of(MODE)> &ss) {
+                                         const double *w3, SS &ss) {
   if constexpr (MODE == kTrueRes || MODE == kInit) {
     const double ri = w1[i] - acc;
     y[i] = ri;
@@ -224,14 +194,22 @@ __device__ __forceinline__ bool dots_skip(const KState *st) {
   return st->done != 0;
 }
 
+template <int MODE>
+using DotsSums = SliceSums<dots_of(MODE), FinDots<MODE>>;
+
+template <int MODE>
+__device__ __forceinline__ FinDots<MODE> dots_fin(KState *st, const double *w2) {
+  return FinDots<MODE>{st, w2, MODE == kTrueRes && true_res_verify(st)};
+}
+
 template <int MODE, int S, int P>
 __global__ void __launch_bounds__(kBlock)
     k_spmv_dots(SellView<double> m, const double *__restrict__ x, double *__restrict__ y,
                 const double *__restrict__ w1, double *__restrict__ w2,
-                const double *__restrict__ w3, const KState *st, SliceOut o) {
+                const double *__restrict__ w3, KState *st, FoldBuf fb) {
   pdl_enter();
   if (dots_skip<MODE>(st)) return;
-  SliceSums<dots_of(MODE)> ss{o.sp, o.ld, {}};
+  DotsSums<MODE> ss{fb, dots_fin<MODE>(st, w2), {}};
   for_each_row_sliced<S, P>(
       m, x, [&](int i, double acc) { dots_row<MODE>(i, acc, x, y, w1, w2, w3, ss); },
       [&](int s) { ss.end(s); });
@@ -256,7 +234,7 @@ struct EpiDots {
   const double *__restrict__ w1;
   double *__restrict__ w2;
   const double *__restrict__ w3;
-  SliceSums<dots_of(MODE)> ss;
+  DotsSums<MODE> ss;
   static constexpr int kRowVecs = (MODE == kTrueRes) ? 3 : 1;
   // row operands: b (init / true residual, with r and rt), p (CG sigma),
   // rt (BiCGSTAB sigma), s (BiCGSTAB omega)
@@ -298,10 +276,10 @@ __global__ void __launch_bounds__(kStreamThreads)
     k_stream_dots(SellView<double> m, const StageDesc *__restrict__ stages, int nstages,
                   StreamLayout L, const double *__restrict__ x, double *__restrict__ y,
                   const double *__restrict__ w1, double *__restrict__ w2,
-                  const double *__restrict__ w3, KState *st, SliceOut o) {
+                  const double *__restrict__ w3, KState *st, FoldBuf fb) {
   pdl_enter();
   if (dots_skip<MODE>(st)) return;
-  EpiDots<MODE> epi{y, x, w1, w2, w3, {o.sp, o.ld, {}}};
+  EpiDots<MODE> epi{y, x, w1, w2, w3, {fb, dots_fin<MODE>(st, w2), {}}};
   stream_rows<P, 1>(m, stages, nstages, x, L, epi, &st->timeout);
 }
 
@@ -310,7 +288,7 @@ template <class T>
 struct EpiCgZ {
   const double *__restrict__ r;
   double *__restrict__ z;
-  SliceSums<1> ss;
+  SliceSums<1, FinCgRho> ss;
   static constexpr int kRowVecs = 1;
   __device__ __host__ __forceinline__ RowVecs row_vecs() const {
     return RowVecs{{r, nullptr, nullptr}, {8, 0, 0}};
@@ -328,10 +306,10 @@ template <class V, class T, int P>
 __global__ void __launch_bounds__(kStreamThreads)
     k_stream_cg_sweep2(SellView<V> m, const StageDesc *__restrict__ stages, int nstages,
                        StreamLayout L, const T *__restrict__ t, const double *__restrict__ r,
-                       double *__restrict__ z, KState *st, SliceOut o) {
+                       double *__restrict__ z, KState *st, FoldBuf fb) {
   pdl_enter();
   if (st->done) return;
-  EpiCgZ<T> epi{r, z, {o.sp, o.ld, {0.0}}};
+  EpiCgZ<T> epi{r, z, {fb, FinCgRho{st}, {0.0}}};
   stream_rows<P, stream_rmax<V>()>(m, stages, nstages, t, L, epi, &st->timeout);
 }
 
@@ -339,10 +317,10 @@ __global__ void __launch_bounds__(kStreamThreads)
 template <class V, class T, int S, int P>
 __global__ void __launch_bounds__(kBlock)
     k_cg_sweep2(SellView<V> m, const T *__restrict__ t, const double *__restrict__ r,
-                double *__restrict__ z, const KState *st, SliceOut o) {
+                double *__restrict__ z, KState *st, FoldBuf fb) {
   pdl_enter();
   if (st->done) return;
-  SliceSums<1> ss{o.sp, o.ld, {0.0}};
+  SliceSums<1, FinCgRho> ss{fb, FinCgRho{st}, {0.0}};
   for_each_row_sliced<S, P>(
       m, t,
       [&](int i, auto acc) {
@@ -355,20 +333,24 @@ __global__ void __launch_bounds__(kBlock)
 
 // CG without preconditioner: z = r, rho = r.r.
 __global__ void __launch_bounds__(kBlock)
-    k_cg_ident(int n, const double *__restrict__ r, double *__restrict__ z, const KState *st,
-               SliceOut o) {
+    k_cg_ident(int n, const double *__restrict__ r, double *__restrict__ z, KState *st,
+               FoldBuf fb) {
   pdl_enter();
   if (st->done) return;
-  SliceSums<1> ss{o.sp, o.ld, {0.0}};
-  const int ns = nslices_of(n), lane = threadIdx.x & 31;
-  for (int s = first_slice(); s < ns; s += slice_stride()) {
-    const int i = s * kSlice + lane;
-    if (i < n) {
-      z[i] = r[i];
-      ss.v[0] = r[i] * r[i];
-    }
-    ss.end(s);
-  }
+  SliceSums<1, FinCgRho> ss{fb, FinCgRho{st}, {0.0}};
+  double p[kVecSlices] = {};
+  for_slices(
+      n,
+      [&](int j, int i) {
+        const double ri = r[i];
+        z[i] = ri;
+        p[j] = ri * ri;
+      },
+      [&](int j, int s) {
+        ss.v[0] = p[j];
+        p[j] = 0.0;
+        ss.end(s);
+      });
 }
 
 // CG: p = z (first iteration) or p = z + beta p.
@@ -384,22 +366,25 @@ __global__ void __launch_bounds__(kBlock)
 // CG: x += alpha p, r -= alpha q, rn2 = r.r.
 __global__ void __launch_bounds__(kBlock)
     k_cg_xr(int n, const double *__restrict__ p, const double *__restrict__ q,
-            double *__restrict__ x, double *__restrict__ r, const KState *st, SliceOut o) {
+            double *__restrict__ x, double *__restrict__ r, KState *st, FoldBuf fb) {
   pdl_enter();
   if (st->done) return;
   const double alpha = st->alpha;
-  SliceSums<1> ss{o.sp, o.ld, {0.0}};
-  const int ns = nslices_of(n), lane = threadIdx.x & 31;
-  for (int s = first_slice(); s < ns; s += slice_stride()) {
-    const int i = s * kSlice + lane;
-    if (i < n) {
-      x[i] = x[i] + alpha * p[i];
-      const double ri = r[i] - alpha * q[i];
-      r[i] = ri;
-      ss.v[0] = ri * ri;
-    }
-    ss.end(s);
-  }
+  SliceSums<1, FinCgXr> ss{fb, FinCgXr{st}, {0.0}};
+  double pr[kVecSlices] = {};
+  for_slices(
+      n,
+      [&](int j, int i) {
+        x[i] = x[i] + alpha * p[i];
+        const double ri = r[i] - alpha * q[i];
+        r[i] = ri;
+        pr[j] = ri * ri;
+      },
+      [&](int j, int s) {
+        ss.v[0] = pr[j];
+        pr[j] = 0.0;
+        ss.end(s);
+      });
 }
 
 // BiCGSTAB: p = r (first iteration) or p = r + beta (p - omega v).
@@ -429,25 +414,28 @@ __global__ void __launch_bounds__(kBlock)
     k_bicg_xr(int n, const double *__restrict__ f, const double *__restrict__ z,
               const double *__restrict__ s, const double *__restrict__ t,
               const double *__restrict__ rt, double *__restrict__ x,
-              double *__restrict__ r, const KState *st, SliceOut o) {
+              double *__restrict__ r, KState *st, FoldBuf fb) {
   pdl_enter();
   if (st->done) return;
   const double alpha = st->alpha, omega = st->omega;
-  SliceSums<2> ss{o.sp, o.ld, {0.0, 0.0}};
-  const int ns = nslices_of(n), lane = threadIdx.x & 31;
-  for (int sl = first_slice(); sl < ns; sl += slice_stride()) {
-    const int i = sl * kSlice + lane;
-    if (i < n) {
-      x[i] = (x[i] + alpha * f[i]) + omega * z[i];
-      const double ri = s[i] - omega * t[i];
-      r[i] = ri;
-      ss.v[0] = ri * ri;
-      ss.v[1] = rt[i] * ri;
-    }
-    ss.end(sl);
-  }
+  SliceSums<2, FinBicgXr> ss{fb, FinBicgXr{st}, {0.0, 0.0}};
+  double p0[kVecSlices] = {}, p1[kVecSlices] = {};
+  for_slices(
+      n,
+      [&](int j, int i) {
+        x[i] = (x[i] + alpha * f[i]) + omega * z[i];
+        const double ri = s[i] - omega * t[i];
+        r[i] = ri;
+        p0[j] = ri * ri;
+        p1[j] = rt[i] * ri;
+      },
+      [&](int j, int sl) {
+        ss.v[0] = p0[j];
+        ss.v[1] = p1[j];
+        p0[j] = p1[j] = 0.0;
+        ss.end(sl);
+      });
 }
-
 
 template <class V, class T>
 struct CgSweep2Launch {
@@ -456,7 +444,7 @@ struct CgSweep2Launch {
   const double *r;
   double *z;
   KState *st;
-  SliceOut o;
+  FoldBuf o;
   int G;
   cudaStream_t s;
   template <int S, int P>
@@ -479,7 +467,7 @@ struct StreamCgSweep2Launch {
   const double *r;
   double *z;
   KState *st;
-  SliceOut o;
+  FoldBuf o;
   cudaStream_t s;
   bool *launched;
   template <int S, int P>
@@ -495,7 +483,7 @@ struct StreamCgSweep2Launch {
 
 template <class V, class T>
 void launch_cg_sweep2(const DevSell &m, const void *t, const double *r, double *z,
-                      KState *st, SliceOut o, int G, cudaStream_t s) {
+                      KState *st, FoldBuf o, int G, cudaStream_t s) {
   if (stream_enabled(m.prec)) {
     StreamLayout L;
     size_t smem = 0;
@@ -521,7 +509,7 @@ struct SpmvDotsLaunch {
   double *w2;
   const double *w3;
   KState *st;
-  SliceOut pp;
+  FoldBuf pp;
   template <int S, int P>
   void run() const {
     auto kern = k_spmv_dots<MODE, S, P>;
@@ -543,7 +531,7 @@ struct StreamDotsLaunch {
   double *w2;
   const double *w3;
   KState *st;
-  SliceOut pp;
+  FoldBuf pp;
   bool *launched;
   template <int S, int P>
   void run() const {
@@ -559,7 +547,7 @@ struct StreamDotsLaunch {
 // y = A x with the dots of MODE (streaming when the layout allows).
 template <int MODE>
 void spmv_dots(const DevSell &Am, int G, cudaStream_t s, const double *x, double *y,
-               const double *w1, double *w2, const double *w3, KState *st, SliceOut pp) {
+               const double *w1, double *w2, const double *w3, KState *st, FoldBuf pp) {
   if (stream_enabled(Am.prec)) {
     StreamLayout L;
     size_t smem = 0;
@@ -589,10 +577,11 @@ struct KrylovWs {
   int n = 0, G = 0;
   size_t stride = 0;      // doubles between vectors (n rounded up to 32: 256 B aligned)
   double *vec = nullptr;  // 11 vectors of n
-  // canonical-order reductions: up to 3 dots' slice sums (ld per dot) and
-  // range sums (ldr per dot)
+  // canonical-order reductions: up to 3 dots' slice sums (ld per dot),
+  // range sums (ldr per dot), per-range counts and the range ticket
   int ns = 0, ld = 0, nr = 0, ldr = 0;
   double *sp = nullptr, *rs = nullptr;
+  unsigned *cnt = nullptr;  // nr counts, then the ticket
   // relative residual per iteration of the last solve (device, host copy)
   double *hist = nullptr;
   std::vector<double> hhist;
@@ -606,12 +595,7 @@ struct KrylovWs {
   int key_method = -1, key_replace = -1;
   KState last{};  // final state of the last solve (statistics)
   double *v(int i) const { return vec + (size_t)i * stride; }
-  SliceOut out() const { return SliceOut{sp, ld}; }
-  // Fold the slice sums of the reduction just enqueued (NV dots).
-  template <int NV, class Fin>
-  void fold(const Fin &fin) const {
-    launch(k_fold<NV, Fin>, nr, kFoldThreads, 0, s, sp, ld, ns, rs, ldr, st, fin);
-  }
+  FoldBuf out() const { return FoldBuf{sp, rs, cnt, cnt + nr, ld, ldr, ns, nr}; }
 };
 
 void destroy_ws(KrylovWs *w) {
@@ -620,6 +604,7 @@ void destroy_ws(KrylovWs *w) {
   if (w->vec) cudaFree(w->vec);
   if (w->hist) cudaFree(w->hist);
   if (w->sp) cudaFree(w->sp);
+  if (w->cnt) cudaFree(w->cnt);
   if (w->rs) cudaFree(w->rs);
   if (w->st) cudaFree(w->st);
   if (w->hst) cudaFreeHost(w->hst);
@@ -652,6 +637,7 @@ int get_ws(ainv_csr *a, KrylovWs **out) {
   w->ldr = (w->nr + 31) / 32 * 32;
   if (e == cudaSuccess) e = cudaMalloc(&w->sp, sizeof(double) * 3 * (size_t)w->ld);
   if (e == cudaSuccess) e = cudaMalloc(&w->rs, sizeof(double) * 3 * (size_t)w->ldr);
+  if (e == cudaSuccess) e = cudaMalloc(&w->cnt, sizeof(unsigned) * ((size_t)w->nr + 1));
   if (e == cudaSuccess) e = cudaMalloc(&w->hist, sizeof(double) * kHistCap);
   if (e == cudaSuccess) e = cudaMalloc(&w->st, sizeof(KState));
   if (e == cudaSuccess) e = cudaMallocHost(&w->hst, sizeof(KState));
@@ -669,7 +655,7 @@ int get_ws(ainv_csr *a, KrylovWs **out) {
 }
 
 void precond_sweep2_cg(const ainv_handle *h, const double *r, double *z, KState *st,
-                       SliceOut partials, int G, cudaStream_t s) {
+                       FoldBuf partials, int G, cudaStream_t s) {
   switch (h->prec) {
     case AINV_PREC_FP64: launch_cg_sweep2<double, double>(h->z, h->t, r, z, st, partials, G, s); break;
     case AINV_PREC_FP32: launch_cg_sweep2<float, float>(h->z, h->t, r, z, st, partials, G, s); break;
@@ -687,7 +673,7 @@ int enqueue_iteration(KrylovWs *w, const ainv_handle *h, const ainv_csr *a, int 
   const int Gv = (n + kBlock - 1) / kBlock;
   const DevSell &A = a->a;
   KState *st = w->st;
-  const SliceOut pp = w->out();
+  const FoldBuf pp = w->out();
   cudaStream_t s = w->s;
   const int *stop = &st->done;
   if (method == AINV_KRYLOV_CG) {
@@ -699,15 +685,11 @@ int enqueue_iteration(KrylovWs *w, const ainv_handle *h, const ainv_csr *a, int 
       launch(k_cg_ident, std::min(G, wave_grid((const void *)k_cg_ident, n)), kBlock, 0, s, n, r, z,
              st, pp);
     }
-    w->fold<1>(FinCgRho{});
     launch(k_cg_p, Gv, kBlock, 0, s, n, z, p, st);
     spmv_dots<kCgSigma>(A, G, s, p, q, nullptr, nullptr, nullptr, st, pp);
-    w->fold<1>(FinDots<kCgSigma>{nullptr});
     launch(k_cg_xr, std::min(G, wave_grid((const void *)k_cg_xr, n)), kBlock, 0, s, n, p, q, x, r,
            st, pp);
-    w->fold<1>(FinCgXr{});
     spmv_dots<kTrueRes>(A, G, s, x, w->v(RTRUE), w->v(BW), nullptr, r, st, pp);
-    w->fold<3>(FinDots<kTrueRes>{nullptr});
     launch(k_replace_r, wave_grid((const void *)k_replace_r, n), kBlock, 0, s, n, w->v(RTRUE), r,
            st);
   } else {
@@ -720,7 +702,6 @@ int enqueue_iteration(KrylovWs *w, const ainv_handle *h, const ainv_csr *a, int 
       AINV_CUDA_TRY(cudaMemcpyAsync(f, p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     }
     spmv_dots<kBicgSigma>(A, G, s, f, v, rt, nullptr, nullptr, st, pp);
-    w->fold<1>(FinDots<kBicgSigma>{rt});
     launch(k_bicg_s, Gv, kBlock, 0, s, n, r, v, sv, st);
     if (h) {
       AINV_TRY(ainv_apply_async(h, 'N', 1.0, sv, 0.0, z, s, stop, &st->timeout));
@@ -728,12 +709,9 @@ int enqueue_iteration(KrylovWs *w, const ainv_handle *h, const ainv_csr *a, int 
       AINV_CUDA_TRY(cudaMemcpyAsync(z, sv, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     }
     spmv_dots<kBicgOmega>(A, G, s, z, t, sv, nullptr, nullptr, st, pp);
-    w->fold<2>(FinDots<kBicgOmega>{rt});
     launch(k_bicg_xr, std::min(G, wave_grid((const void *)k_bicg_xr, n)), kBlock, 0, s, n, f, z, sv,
            t, rt, x, r, st, pp);
-    w->fold<2>(FinBicgXr{});
     spmv_dots<kTrueRes>(A, G, s, x, w->v(RTRUE), w->v(BW), rt, r, st, pp);
-    w->fold<3>(FinDots<kTrueRes>{rt});
     launch(k_replace_r, wave_grid((const void *)k_replace_r, n), kBlock, 0, s, n, w->v(RTRUE), r,
            st);
   }
@@ -804,13 +782,14 @@ int krylov_solve(const ainv_handle *h, ainv_csr *a, const double *b, double *x, 
   init.hist_cap = kHistCap;
   *w->hst = init;
   AINV_CUDA_TRY(cudaMemcpyAsync(w->st, w->hst, sizeof(KState), cudaMemcpyHostToDevice, w->s));
+  // range counts start at zero (a solve that stopped on a timeout may have
+  // left some behind)
+  AINV_CUDA_TRY(cudaMemsetAsync(w->cnt, 0, sizeof(unsigned) * ((size_t)w->nr + 1), w->s));
   const DevSell &A = a->a;
   launch(k_bnorm, std::min(w->G, wave_grid((const void *)k_bnorm, n)), kBlock, 0, w->s, n, w->v(BW),
-         w->out());
-  w->fold<1>(FinBnorm{});
+         w->st, w->out());
   double *rt0 = method == AINV_KRYLOV_BICGSTAB ? w->v(RT) : nullptr;
   spmv_dots<kInit>(A, w->G, w->s, w->v(XW), w->v(R), w->v(BW), rt0, nullptr, w->st, w->out());
-  w->fold<2>(FinDots<kInit>{rt0});
   AINV_CUDA_TRY(cudaGetLastError());
 
   // The first chunk always runs as plain launches (kernel attributes are

@@ -481,13 +481,15 @@ __device__ __forceinline__ void for_each_row_sliced(const SellView<V> &m,
 //   1. slice sums: the 32 products of slice s (rows 32s..32s+31, zero past
 //      n) go through the warp tree below (lane l adds lane l+16, then l+8,
 //      4, 2, 1; lane 0's value);
-//   2. range sums: slices [1024j, 1024j+1024) are folded by 256 threads,
-//      thread t adding slices t, t+256, t+512, t+768 in that order from
-//      zero, then the warp tree over each warp's 32 thread sums and the 8
-//      warp sums added from zero in warp order (block_sum);
-//   3. the total: the range sums folded the same way (thread t adds ranges
-//      t, t+256, ... in order).
-constexpr int kFoldThreads = 256;
+//   2. range sums: the slice sums of slices [1024j, 1024j+1024) are folded
+//      by one warp, lane l adding slices 1024j+l, +32, ..., +992 in that
+//      order from zero, then the warp tree;
+//   3. the total: the range sums folded the same way (lane l adds ranges
+//      l, l+32, l+64, ... in order from zero, then the warp tree).
+// The kernel that computes the products does all three: the warp that
+// stores the last slice sum of a range folds that range, and the warp that
+// stores the last range sum folds the total and runs the scalar step.  Both
+// are found by atomic counts; nothing waits.
 constexpr int kFoldRange = 1024;  // slices per range
 
 __device__ __forceinline__ double warp_tree(double v) {
@@ -496,21 +498,78 @@ __device__ __forceinline__ double warp_tree(double v) {
   return v;
 }
 
+// Device buffers of one reduction: slice sums of dot k at sp[k*ld + s],
+// range sums at rs[k*ldr + r], per-range counts (zero between reductions)
+// and the range ticket.
+struct FoldBuf {
+  double *sp, *rs;
+  unsigned *cnt, *ticket;
+  int ld, ldr, ns, nr;
+};
+
+// Steps 2 and 3 for range r, by the warp that completed it; fin(totals)
+// runs in lane 0 of the warp that completes the last range.
+template <int NV, class Fin>
+__device__ __noinline__ void fold_range(const FoldBuf b, const Fin fin, int r) {
+  const int lane = threadIdx.x & 31;
+  __threadfence();
+  double t[NV];
+#pragma unroll
+  for (int k = 0; k < NV; k++) {
+    double a = 0.0;
+    for (int q = 0; q < kFoldRange / 32; q++) {
+      const int s = r * kFoldRange + 32 * q + lane;
+      if (s < b.ns) a = __dadd_rn(a, __ldcg(b.sp + (size_t)k * b.ld + s));
+    }
+    t[k] = warp_tree(a);
+  }
+  unsigned last = 0;
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; k++) b.rs[(size_t)k * b.ldr + r] = t[k];
+    b.cnt[r] = 0u;
+    __threadfence();
+    last = atomicAdd(b.ticket, 1u) == (unsigned)b.nr - 1;
+  }
+  if (!__shfl_sync(0xffffffffu, last, 0)) return;
+  __threadfence();
+#pragma unroll
+  for (int k = 0; k < NV; k++) {
+    double a = 0.0;
+    for (int j = lane; j < b.nr; j += 32) a = __dadd_rn(a, __ldcg(b.rs + (size_t)k * b.ldr + j));
+    t[k] = warp_tree(a);
+  }
+  if (lane == 0) {
+    *b.ticket = 0u;
+    fin(t);
+  }
+}
+
 // Per-slice sums of NV dots.  Each lane sets v[k] to its row's product;
-// end(s), called by the whole warp, stores the slice's warp tree at
-// sp[k*ld + s] and clears v for the next slice (lanes past n keep zero).
-template <int NV>
+// end(s), called by the whole warp once slice s is done, stores the slice's
+// warp tree, clears v for the next slice (lanes past n keep zero) and counts
+// the slice in its range.
+template <int NV, class Fin>
 struct SliceSums {
-  double *__restrict__ sp;
-  int ld;
+  FoldBuf b;
+  Fin fin;
   double v[NV];
   __device__ __forceinline__ void end(int s) {
+    const int lane = threadIdx.x & 31;
 #pragma unroll
     for (int k = 0; k < NV; k++) {
       const double t = warp_tree(v[k]);
-      if ((threadIdx.x & 31) == 0) sp[(size_t)k * ld + s] = t;
+      if (lane == 0) b.sp[(size_t)k * b.ld + s] = t;
       v[k] = 0.0;
     }
+    const int r = s / kFoldRange;
+    unsigned last = 0;
+    if (lane == 0) {
+      const int in_range = min(kFoldRange, b.ns - r * kFoldRange);
+      __threadfence();
+      last = atomicAdd(b.cnt + r, 1u) == (unsigned)in_range - 1;
+    }
+    if (__shfl_sync(0xffffffffu, last, 0)) fold_range<NV>(b, fin, r);
   }
 };
 

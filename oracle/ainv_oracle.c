@@ -763,11 +763,10 @@ int orc_ainv_apply(int n, const int *wt_irp, const int *wt_ja,
  *   ORC_DOT_DEVICE (default): the device library's canonical order -- the
  *     32 products of each 32-row slice (zero past n) summed by the tree
  *     u[l] += u[l+16], u[l] += u[l+8], ..., u[0] += u[1]; the slice sums of
- *     each run of 1024 slices folded by 256 "threads" (thread t adds slices
- *     t, t+256, t+512, t+768 in order from zero), the 256 thread sums by
- *     the same tree per group of 32 and the 8 group sums added in order;
- *     the range sums folded the same way.  The Krylov iterates then match
- *     the device's bit for bit;
+ *     each run of 1024 slices folded by 32 "lanes" (lane l adds slices l,
+ *     l+32, ..., l+992 of the run in order from zero) and the same tree;
+ *     the range sums folded the same way (lane l adds ranges l, l+32, ...).
+ *     The Krylov iterates then match the device's bit for bit;
  *   ORC_DOT_SEQUENTIAL: one running sum in index order, the order of the
  *     reference BLAS ddot. */
 static int g_dot_order = ORC_DOT_DEVICE;
@@ -786,18 +785,15 @@ static double tree32(double *u) {
   return u[0];
 }
 
-/* 256 running sums over src[t], src[t+256], ... then the trees. */
-static double fold256(const double *src, long count) {
-  double t[256], w[8];
-  for (int j = 0; j < 256; j++) {
+/* 32 running sums over src[l], src[l+32], ... then the tree. */
+static double fold32(const double *src, long count) {
+  double t[32];
+  for (int l = 0; l < 32; l++) {
     double a = 0.0;
-    for (long s = j; s < count; s += 256) a = a + src[s];
-    t[j] = a;
+    for (long s = l; s < count; s += 32) a = a + src[s];
+    t[l] = a;
   }
-  for (int k = 0; k < 8; k++) w[k] = tree32(t + 32 * k);
-  double tot = 0.0;
-  for (int k = 0; k < 8; k++) tot = tot + w[k];
-  return tot;
+  return tree32(t);
 }
 
 double orc_dot_device_order(int n, const double *a, const double *b) {
@@ -816,9 +812,9 @@ double orc_dot_device_order(int n, const double *a, const double *b) {
 #pragma omp parallel for schedule(static)
   for (long j = 0; j < nr; j++) {
     const long c = ns - 1024 * j < 1024 ? ns - 1024 * j : 1024;
-    R[j] = fold256(S + 1024 * j, c);
+    R[j] = fold32(S + 1024 * j, c);
   }
-  const double tot = fold256(R, nr);
+  const double tot = fold32(R, nr);
   free(S);
   return tot;
 }

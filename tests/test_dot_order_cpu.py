@@ -1,7 +1,7 @@
 """The canonical summation order of the Krylov dots.
 
 The device library sums every dot in one fixed order (32-row slice trees,
-1024-slice ranges folded by 256 running sums and the same trees, then the
+1024-slice ranges folded by 32 running sums and the same tree, then the
 ranges folded alike) so that its Krylov iterates do not depend on the grid
 or the device; the oracle's ordered dot restates that order so that its
 iterates equal the device's bit for bit.  Here the oracle's C form is
@@ -23,18 +23,14 @@ def _tree32(u):
     return u[..., 0]
 
 
-def _fold256(src):
-    t = np.zeros(256)
-    for j in range(256):
+def _fold32(src):
+    t = np.zeros(32)
+    for lane in range(32):
         a = 0.0
-        for s in range(j, len(src), 256):
+        for s in range(lane, len(src), 32):
             a = a + src[s]
-        t[j] = a
-    w = _tree32(t.reshape(8, 32))
-    tot = 0.0
-    for k in range(8):
-        tot = tot + w[k]
-    return tot
+        t[lane] = a
+    return _tree32(t)
 
 
 def _canonical_dot(a, b):
@@ -43,8 +39,8 @@ def _canonical_dot(a, b):
     p = np.zeros(ns * 32)
     p[:n] = a * b
     S = _tree32(p.reshape(ns, 32))
-    R = np.array([_fold256(S[j:j + 1024]) for j in range(0, ns, 1024)])
-    return _fold256(R)
+    R = np.array([_fold32(S[j:j + 1024]) for j in range(0, ns, 1024)])
+    return _fold32(R)
 
 
 @pytest.mark.parametrize("n", [1, 31, 32, 33, 1000, 32 * 1024, 32 * 1024 + 5, 100_003])
