@@ -150,13 +150,23 @@ class ClockSampler:
                 "reasons": sorted(self.reasons), "samples": len(self.samples)}
 
 
-def build_workload(idim=IDIM):
+VARIANTS = {"INVK": {"SUB_FILLIN": 1, "INV_FILLIN": 1},
+            "INVT": {"SUB_FILLIN": 20, "SUB_ILUTHRS": 0.05, "INV_FILLIN": 20, "INV_THRESH": 0.05}}
+
+
+def build_workload(idim=IDIM, solver="AINV"):
     import ainv
     irp, ja, val = ainv.pde.gen_pde3d(idim, "convdiff", BETA)
-    sv = ainv.mld_d_ainv_solver_type()
-    sv.csetc("AINV_ALG", "LLK")
-    sv.cseti("SUB_FILLIN", FILL)
-    sv.csetr("SUB_ILUTHRS", THRESH)
+    if solver == "AINV":
+        sv = ainv.mld_d_ainv_solver_type()
+        sv.csetc("AINV_ALG", "LLK")
+        sv.cseti("SUB_FILLIN", FILL)
+        sv.csetr("SUB_ILUTHRS", THRESH)
+    else:
+        sv = (ainv.mld_d_invk_solver_type() if solver == "INVK"
+              else ainv.mld_d_invt_solver_type())
+        for k, v in VARIANTS[solver].items():
+            (sv.csetr if isinstance(v, float) else sv.cseti)(k, v)
     sv.check()
     info = sv.build(irp, ja, val)
     if info != 0:
@@ -266,6 +276,9 @@ def main():
                     help="apply leg: the stencil factors, or the same rows with scattered "
                          "columns (per-entry column layout)")
     ap.add_argument("--leg-reps", type=int, default=5, help="applies of the apply leg")
+    ap.add_argument("--leg-solver", default="AINV", choices=["AINV", "INVK", "INVT"],
+                    help="factors of the apply leg: AINV, or the INVK(1,1) / INVT(0.05,20) "
+                         "variants")
     ap.add_argument("--leg-itmax", type=int, default=2000,
                     help="iteration cap of the solve / block legs run alone")
     ap.add_argument("--leg-idim", type=int, default=0,
@@ -730,10 +743,7 @@ def run_variants(ainv, torch, dev, irp, ja, val, A, b, bn, xs, x, y, flush, stre
     factors."""
     n = len(irp) - 1
     out = {}
-    settings = {"INVK": {"SUB_FILLIN": 1, "INV_FILLIN": 1},
-                "INVT": {"SUB_FILLIN": 20, "SUB_ILUTHRS": 0.05,
-                         "INV_FILLIN": 20, "INV_THRESH": 0.05}}
-    for name, kv in settings.items():
+    for name, kv in VARIANTS.items():
         sv = (ainv.mld_d_invk_solver_type() if name == "INVK"
               else ainv.mld_d_invt_solver_type())
         for k, v in kv.items():
@@ -956,7 +966,7 @@ def run_leg(ainv, torch, args):
     elif args.leg == "apply":
         # `--leg-reps` applies ('N') of the convection-diffusion factors in
         # `--leg-prec`, each after an L2 flush
-        (irp, ja, val), sv = build_workload(args.leg_idim or IDIM)
+        (irp, ja, val), sv = build_workload(args.leg_idim or IDIM, args.leg_solver)
         n = len(irp) - 1
         f = sv.factors()
         if args.leg_pattern == "scattered":

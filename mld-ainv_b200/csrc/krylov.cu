@@ -3,25 +3,24 @@
 // as driven at tests/pdegen/ppde3d.f90:280-281.
 //
 // Every scalar of the recurrence (rho, alpha, omega, beta, norms, status)
-// lives in device memory and is produced by the kernel that completes the
-// corresponding reduction, so one iteration is a fixed sequence of launches
-// with no host round trip.  Iterations are issued in chunks captured once
-// into a CUDA graph; when the loop has converged (or broken down) a device
-// flag makes every later kernel of the chunk return at once, and the host
-// inspects the state once per chunk.
+// lives in device memory and is produced by the fold kernel that completes
+// the corresponding reduction, so one iteration is a fixed sequence of
+// launches with no host round trip.  Iterations are issued in chunks
+// captured once into a CUDA graph; when the loop has converged (or broken
+// down) a device flag makes every later kernel of the chunk return at once,
+// and the host inspects the state once per chunk.
 //
 // Reproducible iterates.  Every dot is summed in the canonical order of
 // sell_device.cuh (slice trees, then 1024-slice ranges, then the ranges),
 // which does not depend on the grid, the kernel that computes the products
-// or the device: the producing kernel stores one sum per 32-row slice, the
-// warp that completes a range folds it, and the warp that completes the
-// last range folds the total and applies the scalar step.  The library is
-// compiled without floating-point contraction, so every FP64 product and
-// sum of the vector updates rounds once, as in the reference's Fortran on a
-// target without fused multiply-add, and the row sums of the sweeps and of
-// A use the same unfused order (madd).  With FP64 factors the iterates
-// therefore equal, bit for bit, those of the oracle's ordered-dot Krylov
-// loop.
+// or the device: the producing kernel stores one sum per group of 8 slices
+// (per slice, for the streaming kernels) and a small fold kernel (k_fold)
+// reduces them.  The library is compiled without
+// floating-point contraction, so every FP64 product and sum of the vector
+// updates rounds once, as in the reference's Fortran on a target without
+// fused multiply-add, and the row sums of the sweeps and of A use the same
+// unfused order (madd).  With FP64 factors the iterates therefore equal,
+// bit for bit, those of the oracle's ordered-dot Krylov loop.
 //
 // Fused steps: the A product and the dots that consume it (p.q, rt.v, t.t
 // and t.s) share one kernel; the Z sweep of the preconditioner and the CG
@@ -49,12 +48,82 @@ using namespace kstate;
 constexpr int kChunk = 8;  // iterations per captured graph launch
 constexpr int kHistCap = 8192;  // iterations whose residual is recorded
 
-// ---- scalar steps ------------------------------------------------------------
-// Each reduction ends in lane 0 of the warp that folds its total (SliceSums
-// in sell_device.cuh), which applies one of these to the state.
+// Where a reduction kernel stores its sums: dot k of group g (or of slice
+// s, for the streaming kernels) at sp[k*ld + g].
+struct SliceOut {
+  double *sp;
+  int ld, ns;
+};
+
+// ---- the fold ----------------------------------------------------------------
+// Block j reduces the group sums of range j (kFoldRange groups; with
+// FROM_SLICES it first forms each group's sum from its 8 slice sums, in
+// slice order) and stores the range sums; the last block to finish (atomic
+// ticket, no waiting) folds the range sums and hands the totals to fin.
+// fin.skip(st) repeats the producing kernel's early-exit test, so a
+// reduction that did not run is not folded.
+template <int NV, bool FROM_SLICES, class Fin>
+__global__ void __launch_bounds__(kFoldThreads)
+    k_fold(const double *__restrict__ sp, int ld, int ns, int ng, double *__restrict__ rs,
+           int ldr, KState *st, Fin fin) {
+  pdl_enter();
+  if (fin.skip(st)) return;
+  __shared__ bool is_last;
+  const int nr = gridDim.x;
+  const int g0 = blockIdx.x * kFoldRange, g1 = min(ng, g0 + kFoldRange);
+  double v[NV];
+#pragma unroll
+  for (int k = 0; k < NV; k++) {
+    const double *src = sp + (size_t)k * ld;
+    double a = 0.0;
+    for (int g = g0 + threadIdx.x; g < g1; g += kFoldThreads) {
+      double gsum;
+      if constexpr (FROM_SLICES) {
+        gsum = 0.0;
+#pragma unroll
+        for (int j = 0; j < kGroupSlices; j++) {
+          const int sl = g * kGroupSlices + j;
+          if (sl < ns) gsum = __dadd_rn(gsum, src[sl]);
+        }
+      } else {
+        gsum = src[g];
+      }
+      a = __dadd_rn(a, gsum);
+    }
+    v[k] = a;
+  }
+  block_sum<NV>(v);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; k++) rs[(size_t)k * ldr + blockIdx.x] = v[k];
+    __threadfence();
+    is_last = atomicAdd(&st->ticket[3], 1u) == (unsigned)nr - 1;
+  }
+  __syncthreads();
+  if (!is_last) return;
+  __threadfence();
+#pragma unroll
+  for (int k = 0; k < NV; k++) {
+    double a = 0.0;
+    for (int r = threadIdx.x; r < nr; r += kFoldThreads)
+      a = __dadd_rn(a, __ldcg(rs + (size_t)k * ldr + r));
+    v[k] = a;
+  }
+  block_sum<NV>(v);
+  if (threadIdx.x == 0) {
+    st->ticket[3] = 0u;
+    fin(st, v);
+  }
+}
+
+// Early-exit test of the reductions that stop once the loop is done.
+struct UntilDone {
+  __device__ __forceinline__ bool skip(const KState *st) const { return st->done != 0; }
+};
+
 struct FinBnorm {
-  KState *st;
-  __device__ __forceinline__ void operator()(const double (&v)[1]) const {
+  __device__ __forceinline__ bool skip(const KState *) const { return false; }
+  __device__ __forceinline__ void operator()(KState *st, const double (&v)[1]) const {
     const double bn = sqrt(v[0]);
     st->bn2 = (bn == 0.0) ? 1.0 : bn;
   }
@@ -72,36 +141,36 @@ constexpr int dots_of(int mode) {
 }
 
 // Scalar step of an SpMV-with-dots reduction (w2: rt for BiCGSTAB, else
-// null, as finish_dots expects; verify: the true-residual pass confirms a
-// convergence claim, decided when the kernel started).
+// null, as finish_dots expects).
 template <int MODE>
 struct FinDots {
-  KState *st;
   const double *w2;
-  bool verify;
-  __device__ __forceinline__ void operator()(const double (&v)[dots_of(MODE)]) const {
+  __device__ __forceinline__ bool skip(const KState *st) const {
+    if (MODE == kTrueRes) return !true_res_verify(st) && !true_res_periodic(st);
+    return st->done != 0;
+  }
+  __device__ __forceinline__ void operator()(KState *st, const double (&v)[dots_of(MODE)]) const {
     double pr[3] = {0.0, 0.0, 0.0};
 #pragma unroll
     for (int k = 0; k < dots_of(MODE); k++) pr[k] = v[k];
-    finish_dots<MODE>(st, pr, verify, w2);
+    finish_dots<MODE>(st, pr, MODE == kTrueRes && true_res_verify(st), w2);
   }
 };
 
-struct FinCgRho {
-  KState *st;
-  __device__ __forceinline__ void operator()(const double (&v)[1]) const { cg_take_rho(st, v[0]); }
+struct FinCgRho : UntilDone {
+  __device__ __forceinline__ void operator()(KState *st, const double (&v)[1]) const {
+    cg_take_rho(st, v[0]);
+  }
 };
 
-struct FinCgXr {
-  KState *st;
-  __device__ __forceinline__ void operator()(const double (&v)[1]) const {
+struct FinCgXr : UntilDone {
+  __device__ __forceinline__ void operator()(KState *st, const double (&v)[1]) const {
     finish_iteration(st, v[0]);
   }
 };
 
-struct FinBicgXr {
-  KState *st;
-  __device__ __forceinline__ void operator()(const double (&v)[2]) const {
+struct FinBicgXr : UntilDone {
+  __device__ __forceinline__ void operator()(KState *st, const double (&v)[2]) const {
     finish_iteration(st, v[0]);
     bicg_next_rho(st, v[1]);
   }
@@ -109,36 +178,36 @@ struct FinBicgXr {
 
 // ---- reduction kernels ---------------------------------------------------------
 // Vector-only kernels walk warp-per-slice (lane = row), so the slice trees
-// see the same lane order as in the SpMV kernels.  A warp takes kVecSlices
-// consecutive slices per step and issues all of their loads before the
-// first slice's tree.
+// see the same lane order as in the SpMV kernels, and a warp takes a whole
+// group of 8 slices per step: all of the group's loads are issued before
+// its first tree.
 __device__ __forceinline__ int nslices_of(int n) { return (n + kSlice - 1) / kSlice; }
-constexpr int kVecSlices = 4;
 
-// for_slices(n, body, end): body(j, i) for row i of slice j of the step
-// (rows < n), then end(j, s) with the whole warp for each slice s < ns.
+// body(j, i) for row i of slice j of the warp's group (rows < n), then
+// end(j, s) with the whole warp for each slice s of the group.
 template <class Body, class End>
-__device__ __forceinline__ void for_slices(int n, Body &&body, End &&end) {
+__device__ __forceinline__ void for_groups(int n, Body &&body, End &&end) {
   const int ns = nslices_of(n), lane = threadIdx.x & 31;
-  for (int q = first_slice(); q * kVecSlices < ns; q += slice_stride()) {
+  const int ngroups = (ns + kGroupSlices - 1) / kGroupSlices;
+  for (int q = first_slice(); q < ngroups; q += slice_stride()) {
 #pragma unroll
-    for (int j = 0; j < kVecSlices; j++) {
-      const int i = (q * kVecSlices + j) * kSlice + lane;
+    for (int j = 0; j < kGroupSlices; j++) {
+      const int i = (q * kGroupSlices + j) * kSlice + lane;
       if (i < n) body(j, i);
     }
 #pragma unroll
-    for (int j = 0; j < kVecSlices; j++)
-      if (q * kVecSlices + j < ns) end(j, q * kVecSlices + j);
+    for (int j = 0; j < kGroupSlices; j++)
+      if (q * kGroupSlices + j < ns) end(j, q * kGroupSlices + j);
   }
 }
 
 // ||b||_2 (istop=2 denominator).
 __global__ void __launch_bounds__(kBlock)
-    k_bnorm(int n, const double *__restrict__ b, KState *st, FoldBuf fb) {
+    k_bnorm(int n, const double *__restrict__ b, SliceOut o) {
   pdl_enter();
-  SliceSums<1, FinBnorm> ss{fb, FinBnorm{st}, {0.0}};
-  double p[kVecSlices] = {};
-  for_slices(
+  GroupSums<1> ss{o.sp, o.ld, o.ns, {0.0}, {0.0}};
+  double p[kGroupSlices] = {};
+  for_groups(
       n, [&](int j, int i) { p[j] = b[i] * b[i]; },
       [&](int j, int s) {
         ss.v[0] = p[j];
@@ -157,8 +226,7 @@ __global__ void __launch_bounds__(kBlock)
 //               iterations and once when the recurrence claims convergence.
 //               Decides whether r is replaced (k_replace_r) and whether the
 //               convergence stands; w2 = rt for BiCGSTAB's rho.
-// The row products of the dots go to the slice sums; the fold of the last
-// range does the scalar step.
+// The row products of the dots go to ss; the fold does the scalar step.
 template <int MODE, class SS>
 __device__ __forceinline__ void dots_row(int i, double acc, const double *__restrict__ x,
                                          double *__restrict__ y, const double *w1, double *w2,
@@ -194,22 +262,14 @@ __device__ __forceinline__ bool dots_skip(const KState *st) {
   return st->done != 0;
 }
 
-template <int MODE>
-using DotsSums = SliceSums<dots_of(MODE), FinDots<MODE>>;
-
-template <int MODE>
-__device__ __forceinline__ FinDots<MODE> dots_fin(KState *st, const double *w2) {
-  return FinDots<MODE>{st, w2, MODE == kTrueRes && true_res_verify(st)};
-}
-
 template <int MODE, int S, int P>
 __global__ void __launch_bounds__(kBlock)
     k_spmv_dots(SellView<double> m, const double *__restrict__ x, double *__restrict__ y,
                 const double *__restrict__ w1, double *__restrict__ w2,
-                const double *__restrict__ w3, KState *st, FoldBuf fb) {
+                const double *__restrict__ w3, const KState *st, SliceOut o) {
   pdl_enter();
   if (dots_skip<MODE>(st)) return;
-  DotsSums<MODE> ss{fb, dots_fin<MODE>(st, w2), {}};
+  GroupSums<dots_of(MODE)> ss{o.sp, o.ld, o.ns, {}, {}};
   for_each_row_sliced<S, P>(
       m, x, [&](int i, double acc) { dots_row<MODE>(i, acc, x, y, w1, w2, w3, ss); },
       [&](int s) { ss.end(s); });
@@ -234,7 +294,7 @@ struct EpiDots {
   const double *__restrict__ w1;
   double *__restrict__ w2;
   const double *__restrict__ w3;
-  DotsSums<MODE> ss;
+  SliceSums<dots_of(MODE)> ss;
   static constexpr int kRowVecs = (MODE == kTrueRes) ? 3 : 1;
   // row operands: b (init / true residual, with r and rt), p (CG sigma),
   // rt (BiCGSTAB sigma), s (BiCGSTAB omega)
@@ -276,10 +336,10 @@ __global__ void __launch_bounds__(kStreamThreads)
     k_stream_dots(SellView<double> m, const StageDesc *__restrict__ stages, int nstages,
                   StreamLayout L, const double *__restrict__ x, double *__restrict__ y,
                   const double *__restrict__ w1, double *__restrict__ w2,
-                  const double *__restrict__ w3, KState *st, FoldBuf fb) {
+                  const double *__restrict__ w3, KState *st, SliceOut o) {
   pdl_enter();
   if (dots_skip<MODE>(st)) return;
-  EpiDots<MODE> epi{y, x, w1, w2, w3, {fb, dots_fin<MODE>(st, w2), {}}};
+  EpiDots<MODE> epi{y, x, w1, w2, w3, {o.sp, o.ld, {}}};
   stream_rows<P, 1>(m, stages, nstages, x, L, epi, &st->timeout);
 }
 
@@ -288,7 +348,7 @@ template <class T>
 struct EpiCgZ {
   const double *__restrict__ r;
   double *__restrict__ z;
-  SliceSums<1, FinCgRho> ss;
+  SliceSums<1> ss;
   static constexpr int kRowVecs = 1;
   __device__ __host__ __forceinline__ RowVecs row_vecs() const {
     return RowVecs{{r, nullptr, nullptr}, {8, 0, 0}};
@@ -306,10 +366,10 @@ template <class V, class T, int P>
 __global__ void __launch_bounds__(kStreamThreads)
     k_stream_cg_sweep2(SellView<V> m, const StageDesc *__restrict__ stages, int nstages,
                        StreamLayout L, const T *__restrict__ t, const double *__restrict__ r,
-                       double *__restrict__ z, KState *st, FoldBuf fb) {
+                       double *__restrict__ z, KState *st, SliceOut o) {
   pdl_enter();
   if (st->done) return;
-  EpiCgZ<T> epi{r, z, {fb, FinCgRho{st}, {0.0}}};
+  EpiCgZ<T> epi{r, z, {o.sp, o.ld, {0.0}}};
   stream_rows<P, stream_rmax<V>()>(m, stages, nstages, t, L, epi, &st->timeout);
 }
 
@@ -317,10 +377,10 @@ __global__ void __launch_bounds__(kStreamThreads)
 template <class V, class T, int S, int P>
 __global__ void __launch_bounds__(kBlock)
     k_cg_sweep2(SellView<V> m, const T *__restrict__ t, const double *__restrict__ r,
-                double *__restrict__ z, KState *st, FoldBuf fb) {
+                double *__restrict__ z, const KState *st, SliceOut o) {
   pdl_enter();
   if (st->done) return;
-  SliceSums<1, FinCgRho> ss{fb, FinCgRho{st}, {0.0}};
+  GroupSums<1> ss{o.sp, o.ld, o.ns, {0.0}, {0.0}};
   for_each_row_sliced<S, P>(
       m, t,
       [&](int i, auto acc) {
@@ -333,13 +393,13 @@ __global__ void __launch_bounds__(kBlock)
 
 // CG without preconditioner: z = r, rho = r.r.
 __global__ void __launch_bounds__(kBlock)
-    k_cg_ident(int n, const double *__restrict__ r, double *__restrict__ z, KState *st,
-               FoldBuf fb) {
+    k_cg_ident(int n, const double *__restrict__ r, double *__restrict__ z, const KState *st,
+               SliceOut o) {
   pdl_enter();
   if (st->done) return;
-  SliceSums<1, FinCgRho> ss{fb, FinCgRho{st}, {0.0}};
-  double p[kVecSlices] = {};
-  for_slices(
+  GroupSums<1> ss{o.sp, o.ld, o.ns, {0.0}, {0.0}};
+  double p[kGroupSlices] = {};
+  for_groups(
       n,
       [&](int j, int i) {
         const double ri = r[i];
@@ -366,13 +426,13 @@ __global__ void __launch_bounds__(kBlock)
 // CG: x += alpha p, r -= alpha q, rn2 = r.r.
 __global__ void __launch_bounds__(kBlock)
     k_cg_xr(int n, const double *__restrict__ p, const double *__restrict__ q,
-            double *__restrict__ x, double *__restrict__ r, KState *st, FoldBuf fb) {
+            double *__restrict__ x, double *__restrict__ r, const KState *st, SliceOut o) {
   pdl_enter();
   if (st->done) return;
   const double alpha = st->alpha;
-  SliceSums<1, FinCgXr> ss{fb, FinCgXr{st}, {0.0}};
-  double pr[kVecSlices] = {};
-  for_slices(
+  GroupSums<1> ss{o.sp, o.ld, o.ns, {0.0}, {0.0}};
+  double pr[kGroupSlices] = {};
+  for_groups(
       n,
       [&](int j, int i) {
         x[i] = x[i] + alpha * p[i];
@@ -414,13 +474,13 @@ __global__ void __launch_bounds__(kBlock)
     k_bicg_xr(int n, const double *__restrict__ f, const double *__restrict__ z,
               const double *__restrict__ s, const double *__restrict__ t,
               const double *__restrict__ rt, double *__restrict__ x,
-              double *__restrict__ r, KState *st, FoldBuf fb) {
+              double *__restrict__ r, const KState *st, SliceOut o) {
   pdl_enter();
   if (st->done) return;
   const double alpha = st->alpha, omega = st->omega;
-  SliceSums<2, FinBicgXr> ss{fb, FinBicgXr{st}, {0.0, 0.0}};
-  double p0[kVecSlices] = {}, p1[kVecSlices] = {};
-  for_slices(
+  GroupSums<2> ss{o.sp, o.ld, o.ns, {0.0, 0.0}, {0.0, 0.0}};
+  double p0[kGroupSlices] = {}, p1[kGroupSlices] = {};
+  for_groups(
       n,
       [&](int j, int i) {
         x[i] = (x[i] + alpha * f[i]) + omega * z[i];
@@ -437,6 +497,7 @@ __global__ void __launch_bounds__(kBlock)
       });
 }
 
+
 template <class V, class T>
 struct CgSweep2Launch {
   const DevSell &m;
@@ -444,7 +505,7 @@ struct CgSweep2Launch {
   const double *r;
   double *z;
   KState *st;
-  FoldBuf o;
+  SliceOut o;
   int G;
   cudaStream_t s;
   template <int S, int P>
@@ -467,7 +528,7 @@ struct StreamCgSweep2Launch {
   const double *r;
   double *z;
   KState *st;
-  FoldBuf o;
+  SliceOut o;
   cudaStream_t s;
   bool *launched;
   template <int S, int P>
@@ -481,9 +542,10 @@ struct StreamCgSweep2Launch {
   }
 };
 
+// Returns true when the streaming kernel ran (its sums are per slice).
 template <class V, class T>
-void launch_cg_sweep2(const DevSell &m, const void *t, const double *r, double *z,
-                      KState *st, FoldBuf o, int G, cudaStream_t s) {
+bool launch_cg_sweep2(const DevSell &m, const void *t, const double *r, double *z,
+                      KState *st, SliceOut o, int G, cudaStream_t s) {
   if (stream_enabled(m.prec)) {
     StreamLayout L;
     size_t smem = 0;
@@ -492,10 +554,11 @@ void launch_cg_sweep2(const DevSell &m, const void *t, const double *r, double *
     if (grid > 0 && grid <= G && aligned16(t) && aligned16(r))
       with_pack<V, 1>(m.pack, StreamCgSweep2Launch<V, T>{m, L, grid, smem, t, r, z, st, o,
                                                           s, &launched});
-    if (launched) return;
+    if (launched) return true;
   }
   with_group_pack<V>(group_size(m.prec), m.pack,
                      CgSweep2Launch<V, T>{m, t, r, z, st, o, G, s});
+  return false;
 }
 
 template <int MODE>
@@ -509,7 +572,7 @@ struct SpmvDotsLaunch {
   double *w2;
   const double *w3;
   KState *st;
-  FoldBuf pp;
+  SliceOut pp;
   template <int S, int P>
   void run() const {
     auto kern = k_spmv_dots<MODE, S, P>;
@@ -531,7 +594,7 @@ struct StreamDotsLaunch {
   double *w2;
   const double *w3;
   KState *st;
-  FoldBuf pp;
+  SliceOut pp;
   bool *launched;
   template <int S, int P>
   void run() const {
@@ -544,10 +607,11 @@ struct StreamDotsLaunch {
   }
 };
 
-// y = A x with the dots of MODE (streaming when the layout allows).
+// y = A x with the dots of MODE (streaming when the layout allows; then the
+// sums are per slice and the function returns true).
 template <int MODE>
-void spmv_dots(const DevSell &Am, int G, cudaStream_t s, const double *x, double *y,
-               const double *w1, double *w2, const double *w3, KState *st, FoldBuf pp) {
+bool spmv_dots(const DevSell &Am, int G, cudaStream_t s, const double *x, double *y,
+               const double *w1, double *w2, const double *w3, KState *st, SliceOut pp) {
   if (stream_enabled(Am.prec)) {
     StreamLayout L;
     size_t smem = 0;
@@ -558,11 +622,12 @@ void spmv_dots(const DevSell &Am, int G, cudaStream_t s, const double *x, double
         aligned16(rv.p[2]))
       with_pack<double, 1>(Am.pack, StreamDotsLaunch<MODE>{Am, L, grid, smem, s, x, y, w1, w2, w3,
                                                            st, pp, &launched});
-    if (launched) return;
+    if (launched) return true;
   }
   const SellView<double> A = view<double>(Am);
   with_group_pack<double>(group_size(Am.prec), Am.pack,
                           SpmvDotsLaunch<MODE>{A, G, s, x, y, w1, w2, w3, st, pp});
+  return false;
 }
 
 
@@ -577,11 +642,10 @@ struct KrylovWs {
   int n = 0, G = 0;
   size_t stride = 0;      // doubles between vectors (n rounded up to 32: 256 B aligned)
   double *vec = nullptr;  // 11 vectors of n
-  // canonical-order reductions: up to 3 dots' slice sums (ld per dot),
-  // range sums (ldr per dot), per-range counts and the range ticket
-  int ns = 0, ld = 0, nr = 0, ldr = 0;
+  // canonical-order reductions: up to 3 dots' slice sums (ld per dot) and
+  // range sums (ldr per dot)
+  int ns = 0, ng = 0, ld = 0, nr = 0, ldr = 0;
   double *sp = nullptr, *rs = nullptr;
-  unsigned *cnt = nullptr;  // nr counts, then the ticket
   // relative residual per iteration of the last solve (device, host copy)
   double *hist = nullptr;
   std::vector<double> hhist;
@@ -595,7 +659,16 @@ struct KrylovWs {
   int key_method = -1, key_replace = -1;
   KState last{};  // final state of the last solve (statistics)
   double *v(int i) const { return vec + (size_t)i * stride; }
-  FoldBuf out() const { return FoldBuf{sp, rs, cnt, cnt + nr, ld, ldr, ns, nr}; }
+  SliceOut out() const { return SliceOut{sp, ld, ns}; }
+  // Fold the sums of the reduction just enqueued (NV dots): group sums, or
+  // slice sums when a streaming kernel produced them.
+  template <int NV, class Fin>
+  void fold(const Fin &fin, bool from_slices = false) const {
+    if (from_slices)
+      launch(k_fold<NV, true, Fin>, nr, kFoldThreads, 0, s, sp, ld, ns, ng, rs, ldr, st, fin);
+    else
+      launch(k_fold<NV, false, Fin>, nr, kFoldThreads, 0, s, sp, ld, ns, ng, rs, ldr, st, fin);
+  }
 };
 
 void destroy_ws(KrylovWs *w) {
@@ -604,7 +677,6 @@ void destroy_ws(KrylovWs *w) {
   if (w->vec) cudaFree(w->vec);
   if (w->hist) cudaFree(w->hist);
   if (w->sp) cudaFree(w->sp);
-  if (w->cnt) cudaFree(w->cnt);
   if (w->rs) cudaFree(w->rs);
   if (w->st) cudaFree(w->st);
   if (w->hst) cudaFreeHost(w->hst);
@@ -633,11 +705,11 @@ int get_ws(ainv_csr *a, KrylovWs **out) {
   cudaError_t e = cudaMalloc(&w->vec, sizeof(double) * kNumVec * w->stride);
   w->ns = (a->n + kSlice - 1) / kSlice;
   w->ld = (w->ns + 31) / 32 * 32;
-  w->nr = (w->ns + kFoldRange - 1) / kFoldRange;
+  w->ng = (w->ns + kGroupSlices - 1) / kGroupSlices;
+  w->nr = (w->ng + kFoldRange - 1) / kFoldRange;
   w->ldr = (w->nr + 31) / 32 * 32;
   if (e == cudaSuccess) e = cudaMalloc(&w->sp, sizeof(double) * 3 * (size_t)w->ld);
   if (e == cudaSuccess) e = cudaMalloc(&w->rs, sizeof(double) * 3 * (size_t)w->ldr);
-  if (e == cudaSuccess) e = cudaMalloc(&w->cnt, sizeof(unsigned) * ((size_t)w->nr + 1));
   if (e == cudaSuccess) e = cudaMalloc(&w->hist, sizeof(double) * kHistCap);
   if (e == cudaSuccess) e = cudaMalloc(&w->st, sizeof(KState));
   if (e == cudaSuccess) e = cudaMallocHost(&w->hst, sizeof(KState));
@@ -654,14 +726,14 @@ int get_ws(ainv_csr *a, KrylovWs **out) {
   return AINV_SUCCESS;
 }
 
-void precond_sweep2_cg(const ainv_handle *h, const double *r, double *z, KState *st,
-                       FoldBuf partials, int G, cudaStream_t s) {
+bool precond_sweep2_cg(const ainv_handle *h, const double *r, double *z, KState *st,
+                       SliceOut o, int G, cudaStream_t s) {
   switch (h->prec) {
-    case AINV_PREC_FP64: launch_cg_sweep2<double, double>(h->z, h->t, r, z, st, partials, G, s); break;
-    case AINV_PREC_FP32: launch_cg_sweep2<float, float>(h->z, h->t, r, z, st, partials, G, s); break;
-    case AINV_PREC_FP32_ACC64: launch_cg_sweep2<f32w, double>(h->z, h->t, r, z, st, partials, G, s); break;
-    case AINV_PREC_BF16_ACC64: launch_cg_sweep2<b16w, double>(h->z, h->t, r, z, st, partials, G, s); break;
-    default: launch_cg_sweep2<__nv_bfloat16, float>(h->z, h->t, r, z, st, partials, G, s); break;
+    case AINV_PREC_FP64: return launch_cg_sweep2<double, double>(h->z, h->t, r, z, st, o, G, s);
+    case AINV_PREC_FP32: return launch_cg_sweep2<float, float>(h->z, h->t, r, z, st, o, G, s);
+    case AINV_PREC_FP32_ACC64: return launch_cg_sweep2<f32w, double>(h->z, h->t, r, z, st, o, G, s);
+    case AINV_PREC_BF16_ACC64: return launch_cg_sweep2<b16w, double>(h->z, h->t, r, z, st, o, G, s);
+    default: return launch_cg_sweep2<__nv_bfloat16, float>(h->z, h->t, r, z, st, o, G, s);
   }
 }
 
@@ -673,23 +745,28 @@ int enqueue_iteration(KrylovWs *w, const ainv_handle *h, const ainv_csr *a, int 
   const int Gv = (n + kBlock - 1) / kBlock;
   const DevSell &A = a->a;
   KState *st = w->st;
-  const FoldBuf pp = w->out();
+  const SliceOut pp = w->out();
   cudaStream_t s = w->s;
   const int *stop = &st->done;
   if (method == AINV_KRYLOV_CG) {
     double *r = w->v(R), *z = w->v(Z), *p = w->v(P), *q = w->v(V), *x = w->v(XW);
+    bool sl = false;
     if (h) {
       AINV_TRY(launch_sweep_dscale(h->wt, h->d, r, h->t, s, stop, &st->timeout));
-      precond_sweep2_cg(h, r, z, st, pp, G, s);
+      sl = precond_sweep2_cg(h, r, z, st, pp, G, s);
     } else {
       launch(k_cg_ident, std::min(G, wave_grid((const void *)k_cg_ident, n)), kBlock, 0, s, n, r, z,
              st, pp);
     }
+    w->fold<1>(FinCgRho{}, sl);
     launch(k_cg_p, Gv, kBlock, 0, s, n, z, p, st);
-    spmv_dots<kCgSigma>(A, G, s, p, q, nullptr, nullptr, nullptr, st, pp);
+    sl = spmv_dots<kCgSigma>(A, G, s, p, q, nullptr, nullptr, nullptr, st, pp);
+    w->fold<1>(FinDots<kCgSigma>{nullptr}, sl);
     launch(k_cg_xr, std::min(G, wave_grid((const void *)k_cg_xr, n)), kBlock, 0, s, n, p, q, x, r,
            st, pp);
-    spmv_dots<kTrueRes>(A, G, s, x, w->v(RTRUE), w->v(BW), nullptr, r, st, pp);
+    w->fold<1>(FinCgXr{});
+    sl = spmv_dots<kTrueRes>(A, G, s, x, w->v(RTRUE), w->v(BW), nullptr, r, st, pp);
+    w->fold<3>(FinDots<kTrueRes>{nullptr}, sl);
     launch(k_replace_r, wave_grid((const void *)k_replace_r, n), kBlock, 0, s, n, w->v(RTRUE), r,
            st);
   } else {
@@ -701,17 +778,21 @@ int enqueue_iteration(KrylovWs *w, const ainv_handle *h, const ainv_csr *a, int 
     } else {
       AINV_CUDA_TRY(cudaMemcpyAsync(f, p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     }
-    spmv_dots<kBicgSigma>(A, G, s, f, v, rt, nullptr, nullptr, st, pp);
+    bool sl = spmv_dots<kBicgSigma>(A, G, s, f, v, rt, nullptr, nullptr, st, pp);
+    w->fold<1>(FinDots<kBicgSigma>{rt}, sl);
     launch(k_bicg_s, Gv, kBlock, 0, s, n, r, v, sv, st);
     if (h) {
       AINV_TRY(ainv_apply_async(h, 'N', 1.0, sv, 0.0, z, s, stop, &st->timeout));
     } else {
       AINV_CUDA_TRY(cudaMemcpyAsync(z, sv, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     }
-    spmv_dots<kBicgOmega>(A, G, s, z, t, sv, nullptr, nullptr, st, pp);
+    sl = spmv_dots<kBicgOmega>(A, G, s, z, t, sv, nullptr, nullptr, st, pp);
+    w->fold<2>(FinDots<kBicgOmega>{rt}, sl);
     launch(k_bicg_xr, std::min(G, wave_grid((const void *)k_bicg_xr, n)), kBlock, 0, s, n, f, z, sv,
            t, rt, x, r, st, pp);
-    spmv_dots<kTrueRes>(A, G, s, x, w->v(RTRUE), w->v(BW), rt, r, st, pp);
+    w->fold<2>(FinBicgXr{});
+    sl = spmv_dots<kTrueRes>(A, G, s, x, w->v(RTRUE), w->v(BW), rt, r, st, pp);
+    w->fold<3>(FinDots<kTrueRes>{rt}, sl);
     launch(k_replace_r, wave_grid((const void *)k_replace_r, n), kBlock, 0, s, n, w->v(RTRUE), r,
            st);
   }
@@ -782,14 +863,14 @@ int krylov_solve(const ainv_handle *h, ainv_csr *a, const double *b, double *x, 
   init.hist_cap = kHistCap;
   *w->hst = init;
   AINV_CUDA_TRY(cudaMemcpyAsync(w->st, w->hst, sizeof(KState), cudaMemcpyHostToDevice, w->s));
-  // range counts start at zero (a solve that stopped on a timeout may have
-  // left some behind)
-  AINV_CUDA_TRY(cudaMemsetAsync(w->cnt, 0, sizeof(unsigned) * ((size_t)w->nr + 1), w->s));
   const DevSell &A = a->a;
   launch(k_bnorm, std::min(w->G, wave_grid((const void *)k_bnorm, n)), kBlock, 0, w->s, n, w->v(BW),
-         w->st, w->out());
+         w->out());
+  w->fold<1>(FinBnorm{});
   double *rt0 = method == AINV_KRYLOV_BICGSTAB ? w->v(RT) : nullptr;
-  spmv_dots<kInit>(A, w->G, w->s, w->v(XW), w->v(R), w->v(BW), rt0, nullptr, w->st, w->out());
+  const bool sl = spmv_dots<kInit>(A, w->G, w->s, w->v(XW), w->v(R), w->v(BW), rt0, nullptr,
+                                   w->st, w->out());
+  w->fold<2>(FinDots<kInit>{rt0}, sl);
   AINV_CUDA_TRY(cudaGetLastError());
 
   // The first chunk always runs as plain launches (kernel attributes are

@@ -450,47 +450,27 @@ __device__ __forceinline__ void for_each_row(const SellView<V> &m, const X *__re
   }
 }
 
-// Visit every slice: epi(row, acc) for each lane whose row is < n, then,
-// with the whole warp, end(slice) once the slice's rows are done.
-template <int S, int P, int K = 4, class V, class X, class Epi, class End>
-__device__ __forceinline__ void for_each_row_sliced(const SellView<V> &m,
-                                                    const X *__restrict__ x, Epi &&epi,
-                                                    End &&end) {
-  const int ngroups = (m.nslices + S - 1) / S;
-  const int lane = threadIdx.x & 31;
-  for (int g = first_slice(); g < ngroups; g += slice_stride()) {
-    GroupCtx<S> c;
-    group_ctx(m, g, c);
-    typename Acc<V>::type acc[S];
-    group_dot<P, K>(m, c, g, x, acc);
-#pragma unroll
-    for (int q = 0; q < S; q++) {
-      const int s = g * S + q;
-      if (s < m.nslices) {
-        const int row = s * kSlice + lane;
-        if (row < m.n) epi(row, acc[q]);
-        end(s);
-      }
-    }
-  }
-}
-
 // ---- canonical reduction order of the Krylov dots ---------------------------
 // A dot of two n-vectors is summed in one fixed order whatever the grid, the
 // kernel or the device, and the oracle's ordered dot restates that order:
 //   1. slice sums: the 32 products of slice s (rows 32s..32s+31, zero past
 //      n) go through the warp tree below (lane l adds lane l+16, then l+8,
 //      4, 2, 1; lane 0's value);
-//   2. range sums: the slice sums of slices [1024j, 1024j+1024) are folded
-//      by one warp, lane l adding slices 1024j+l, +32, ..., +992 in that
-//      order from zero, then the warp tree;
-//   3. the total: the range sums folded the same way (lane l adds ranges
-//      l, l+32, l+64, ... in order from zero, then the warp tree).
-// The kernel that computes the products does all three: the warp that
-// stores the last slice sum of a range folds that range, and the warp that
-// stores the last range sum folds the total and runs the scalar step.  Both
-// are found by atomic counts; nothing waits.
-constexpr int kFoldRange = 1024;  // slices per range
+//   2. group sums: the slice sums of slices [8g, 8g+8) added in slice order
+//      from zero;
+//   3. range sums: groups [1024j, 1024j+1024) folded by 256 threads, thread
+//      t adding groups t, t+256, t+512, t+768 in that order from zero, then
+//      the warp tree over each warp's 32 thread sums and the 8 warp sums
+//      added from zero in warp order (block_sum);
+//   4. the total: the range sums folded the same way (thread t adds ranges
+//      t, t+256, ... in order).
+// Kernels whose warps walk whole groups (the register SpMV and the vector
+// kernels) form steps 1-2 themselves (GroupSums) and store one sum per
+// group; the streaming kernels store slice sums (SliceSums).  A small fold
+// kernel does the rest.
+constexpr int kGroupSlices = 8;   // slices per group
+constexpr int kFoldThreads = 256;
+constexpr int kFoldRange = 1024;  // groups per range
 
 __device__ __forceinline__ double warp_tree(double v) {
 #pragma unroll
@@ -498,80 +478,79 @@ __device__ __forceinline__ double warp_tree(double v) {
   return v;
 }
 
-// Device buffers of one reduction: slice sums of dot k at sp[k*ld + s],
-// range sums at rs[k*ldr + r], per-range counts (zero between reductions)
-// and the range ticket.
-struct FoldBuf {
-  double *sp, *rs;
-  unsigned *cnt, *ticket;
-  int ld, ldr, ns, nr;
-};
-
-// Steps 2 and 3 for range r, by the warp that completed it; fin(totals)
-// runs in lane 0 of the warp that completes the last range.
-template <int NV, class Fin>
-__device__ __noinline__ void fold_range(const FoldBuf b, const Fin fin, int r) {
-  const int lane = threadIdx.x & 31;
-  __threadfence();
-  double t[NV];
-#pragma unroll
-  for (int k = 0; k < NV; k++) {
-    double a = 0.0;
-    for (int q = 0; q < kFoldRange / 32; q++) {
-      const int s = r * kFoldRange + 32 * q + lane;
-      if (s < b.ns) a = __dadd_rn(a, __ldcg(b.sp + (size_t)k * b.ld + s));
-    }
-    t[k] = warp_tree(a);
-  }
-  unsigned last = 0;
-  if (lane == 0) {
-#pragma unroll
-    for (int k = 0; k < NV; k++) b.rs[(size_t)k * b.ldr + r] = t[k];
-    b.cnt[r] = 0u;
-    __threadfence();
-    last = atomicAdd(b.ticket, 1u) == (unsigned)b.nr - 1;
-  }
-  if (!__shfl_sync(0xffffffffu, last, 0)) return;
-  __threadfence();
-#pragma unroll
-  for (int k = 0; k < NV; k++) {
-    double a = 0.0;
-    for (int j = lane; j < b.nr; j += 32) a = __dadd_rn(a, __ldcg(b.rs + (size_t)k * b.ldr + j));
-    t[k] = warp_tree(a);
-  }
-  if (lane == 0) {
-    *b.ticket = 0u;
-    fin(t);
-  }
-}
-
-// Per-slice sums of NV dots.  Each lane sets v[k] to its row's product;
-// end(s), called by the whole warp once slice s is done, stores the slice's
-// warp tree, clears v for the next slice (lanes past n keep zero) and counts
-// the slice in its range.
-template <int NV, class Fin>
+// Per-slice sums of NV dots (streaming kernels).  Each lane sets v[k] to its
+// row's product; end(s), called by the whole warp, stores the slice's warp
+// tree at sp[k*ld + s] and clears v for the next slice (lanes past n keep
+// zero).
+template <int NV>
 struct SliceSums {
-  FoldBuf b;
-  Fin fin;
+  double *__restrict__ sp;
+  int ld;
   double v[NV];
   __device__ __forceinline__ void end(int s) {
-    const int lane = threadIdx.x & 31;
 #pragma unroll
     for (int k = 0; k < NV; k++) {
       const double t = warp_tree(v[k]);
-      if (lane == 0) b.sp[(size_t)k * b.ld + s] = t;
+      if ((threadIdx.x & 31) == 0) sp[(size_t)k * ld + s] = t;
       v[k] = 0.0;
     }
-    const int r = s / kFoldRange;
-    unsigned last = 0;
-    if (lane == 0) {
-      const int in_range = min(kFoldRange, b.ns - r * kFoldRange);
-      __threadfence();
-      last = atomicAdd(b.cnt + r, 1u) == (unsigned)in_range - 1;
-    }
-    if (__shfl_sync(0xffffffffu, last, 0)) fold_range<NV>(b, fin, r);
   }
 };
+
+// Per-group sums of NV dots, for warps that walk each group's slices in
+// order: end(s) adds slice s's warp tree to the group's running sum (lane
+// 0) and stores it at gs[k*ld + s/8] after the group's last slice.
+template <int NV>
+struct GroupSums {
+  double *__restrict__ gs;
+  int ld, ns;
+  double v[NV];
+  double g[NV];
+  __device__ __forceinline__ void end(int s) {
+    const bool last = (s % kGroupSlices) == kGroupSlices - 1 || s == ns - 1;
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+      const double t = warp_tree(v[k]);
+      v[k] = 0.0;
+      g[k] = __dadd_rn(g[k], t);
+      if (last) {
+        if ((threadIdx.x & 31) == 0) gs[(size_t)k * ld + s / kGroupSlices] = g[k];
+        g[k] = 0.0;
+      }
+    }
+  }
+};
+
+// Visit every slice, warps taking whole groups of 8 slices (warp w: groups
+// w, w + W, ...) and each group's slices in order: epi(row, acc) for each
+// lane whose row is < n, then, with the whole warp, end(slice).
+template <int S, int P, int K = 4, class V, class X, class Epi, class End>
+__device__ __forceinline__ void for_each_row_sliced(const SellView<V> &m,
+                                                    const X *__restrict__ x, Epi &&epi,
+                                                    End &&end) {
+  static_assert(kGroupSlices % S == 0, "a group holds whole steps");
+  const int ngroups = (m.nslices + kGroupSlices - 1) / kGroupSlices;
+  const int lane = threadIdx.x & 31;
+  for (int q = first_slice(); q < ngroups; q += slice_stride()) {
+    for (int j = 0; j < kGroupSlices / S; j++) {
+      const int g = q * (kGroupSlices / S) + j;
+      if (g * S >= m.nslices) break;  // warp-uniform
+      GroupCtx<S> c;
+      group_ctx(m, g, c);
+      typename Acc<V>::type acc[S];
+      group_dot<P, K>(m, c, g, x, acc);
+#pragma unroll
+      for (int qq = 0; qq < S; qq++) {
+        const int s = g * S + qq;
+        if (s < m.nslices) {
+          const int row = s * kSlice + lane;
+          if (row < m.n) epi(row, acc[qq]);
+          end(s);
+        }
+      }
+    }
+  }
+}
 
 // Host side of the programmatic launch: k<<<g, b, smem, s>>>(args...) with
 // the programmatic-serialisation attribute (AINV_PDL=0 launches plainly).

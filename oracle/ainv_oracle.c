@@ -763,10 +763,12 @@ int orc_ainv_apply(int n, const int *wt_irp, const int *wt_ja,
  *   ORC_DOT_DEVICE (default): the device library's canonical order -- the
  *     32 products of each 32-row slice (zero past n) summed by the tree
  *     u[l] += u[l+16], u[l] += u[l+8], ..., u[0] += u[1]; the slice sums of
- *     each run of 1024 slices folded by 32 "lanes" (lane l adds slices l,
- *     l+32, ..., l+992 of the run in order from zero) and the same tree;
- *     the range sums folded the same way (lane l adds ranges l, l+32, ...).
- *     The Krylov iterates then match the device's bit for bit;
+ *     each group of 8 slices added in order from zero; the group sums of
+ *     each run of 1024 groups folded by 256 "threads" (thread t adds groups
+ *     t, t+256, t+512, t+768 in order from zero), the 256 thread sums by
+ *     the same tree per group of 32 threads and the 8 tree sums added in
+ *     order; the range sums folded the same way.  The Krylov iterates then
+ *     match the device's bit for bit;
  *   ORC_DOT_SEQUENTIAL: one running sum in index order, the order of the
  *     reference BLAS ddot. */
 static int g_dot_order = ORC_DOT_DEVICE;
@@ -785,21 +787,24 @@ static double tree32(double *u) {
   return u[0];
 }
 
-/* 32 running sums over src[l], src[l+32], ... then the tree. */
-static double fold32(const double *src, long count) {
-  double t[32];
-  for (int l = 0; l < 32; l++) {
+/* 256 running sums over src[t], src[t+256], ... then the trees. */
+static double fold256(const double *src, long count) {
+  double t[256], w[8];
+  for (int j = 0; j < 256; j++) {
     double a = 0.0;
-    for (long s = l; s < count; s += 32) a = a + src[s];
-    t[l] = a;
+    for (long s = j; s < count; s += 256) a = a + src[s];
+    t[j] = a;
   }
-  return tree32(t);
+  for (int k = 0; k < 8; k++) w[k] = tree32(t + 32 * k);
+  double tot = 0.0;
+  for (int k = 0; k < 8; k++) tot = tot + w[k];
+  return tot;
 }
 
 double orc_dot_device_order(int n, const double *a, const double *b) {
-  const long ns = ((long)n + 31) / 32, nr = (ns + 1023) / 1024;
-  double *S = (double *)malloc(sizeof(double) * (size_t)(ns + nr + 1));
-  double *R = S + ns;
+  const long ns = ((long)n + 31) / 32, ng = (ns + 7) / 8, nr = (ng + 1023) / 1024;
+  double *S = (double *)malloc(sizeof(double) * (size_t)(ns + ng + nr + 1));
+  double *G = S + ns, *R = G + ng;
 #pragma omp parallel for schedule(static)
   for (long s = 0; s < ns; s++) {
     double u[32];
@@ -809,12 +814,17 @@ double orc_dot_device_order(int n, const double *a, const double *b) {
     }
     S[s] = tree32(u);
   }
+  for (long g = 0; g < ng; g++) {
+    double t = 0.0;
+    for (long s = 8 * g; s < 8 * g + 8 && s < ns; s++) t = t + S[s];
+    G[g] = t;
+  }
 #pragma omp parallel for schedule(static)
   for (long j = 0; j < nr; j++) {
-    const long c = ns - 1024 * j < 1024 ? ns - 1024 * j : 1024;
-    R[j] = fold32(S + 1024 * j, c);
+    const long c = ng - 1024 * j < 1024 ? ng - 1024 * j : 1024;
+    R[j] = fold256(G + 1024 * j, c);
   }
-  const double tot = fold32(R, nr);
+  const double tot = fold256(R, nr);
   free(S);
   return tot;
 }

@@ -1,8 +1,8 @@
 """The canonical summation order of the Krylov dots.
 
 The device library sums every dot in one fixed order (32-row slice trees,
-1024-slice ranges folded by 32 running sums and the same tree, then the
-ranges folded alike) so that its Krylov iterates do not depend on the grid
+groups of 8 slices added in order, 1024-group ranges folded by 256 running
+sums and the same trees, then the ranges folded alike) so that its Krylov iterates do not depend on the grid
 or the device; the oracle's ordered dot restates that order so that its
 iterates equal the device's bit for bit.  Here the oracle's C form is
 checked against a second, independent numpy restatement, and the two
@@ -23,14 +23,18 @@ def _tree32(u):
     return u[..., 0]
 
 
-def _fold32(src):
-    t = np.zeros(32)
-    for lane in range(32):
+def _fold256(src):
+    t = np.zeros(256)
+    for j in range(256):
         a = 0.0
-        for s in range(lane, len(src), 32):
+        for s in range(j, len(src), 256):
             a = a + src[s]
-        t[lane] = a
-    return _tree32(t)
+        t[j] = a
+    w = _tree32(t.reshape(8, 32))
+    tot = 0.0
+    for k in range(8):
+        tot = tot + w[k]
+    return tot
 
 
 def _canonical_dot(a, b):
@@ -39,11 +43,18 @@ def _canonical_dot(a, b):
     p = np.zeros(ns * 32)
     p[:n] = a * b
     S = _tree32(p.reshape(ns, 32))
-    R = np.array([_fold32(S[j:j + 1024]) for j in range(0, ns, 1024)])
-    return _fold32(R)
+    G = []
+    for g in range(0, ns, 8):
+        t = 0.0
+        for v in S[g:g + 8]:
+            t = t + v
+        G.append(t)
+    G = np.array(G)
+    R = np.array([_fold256(G[j:j + 1024]) for j in range(0, len(G), 1024)])
+    return _fold256(R)
 
 
-@pytest.mark.parametrize("n", [1, 31, 32, 33, 1000, 32 * 1024, 32 * 1024 + 5, 100_003])
+@pytest.mark.parametrize("n", [1, 31, 32, 33, 1000, 256 * 1024, 256 * 1024 + 5, 300_003])
 def test_device_order_dot_matches_numpy_restatement(n):
     rng = np.random.default_rng(n)
     a = rng.standard_normal(n) * np.exp(rng.uniform(-20, 20, n))
