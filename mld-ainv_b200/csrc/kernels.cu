@@ -34,7 +34,6 @@ template <class V, class T, int S, int P>
 __global__ void __launch_bounds__(kBlock)
     k_sweep_dscale(SellView<V> m, const double *__restrict__ x, const V *__restrict__ d,
                    T *__restrict__ t, const int *__restrict__ stop) {
-  pdl_enter();
   if (stop && *stop) return;
   for_each_row<S, P>(m, x, [&](int row, auto acc) { t[row] = (T)(ldd(d + row) * acc); });
 }
@@ -45,7 +44,6 @@ template <class V, class T, int S, int P>
 __global__ void __launch_bounds__(kBlock)
     k_sweep_axpby(SellView<V> m, const T *__restrict__ t, double alpha, double beta,
                   double *__restrict__ y, const int *__restrict__ stop) {
-  pdl_enter();
   if (stop && *stop) return;
   for_each_row<S, P>(m, t, [&](int row, auto acc) {
     y[row] = axpby_row(alpha, (double)acc, beta, beta == 0.0 ? 0.0 : y[row]);
@@ -121,7 +119,6 @@ __global__ void __launch_bounds__(kStreamThreads)
     k_stream(SellView<V> m, const StageDesc *__restrict__ stages, int nstages,
              const X *__restrict__ x, StreamLayout L, Epi epi, int *status,
              const int *__restrict__ stop) {
-  pdl_enter();
   if (stop && *stop) return;
   stream_rows<P, stream_rmax<V>()>(m, stages, nstages, x, L, epi, status);
 }
@@ -163,13 +160,6 @@ int stream_forced() {
   return forced;
 }
 }  // namespace
-bool pdl_enabled() {
-  static const bool on = [] {
-    const char *e = std::getenv("AINV_PDL");
-    return !(e && std::atoi(e) == 0);
-  }();
-  return on;
-}
 bool stream_enabled(int prec) {
   if (stream_forced() >= 0) return stream_forced() == 1;
   return prec != AINV_PREC_FP64;

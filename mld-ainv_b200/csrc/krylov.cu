@@ -13,9 +13,8 @@
 // Reproducible iterates.  Every dot is summed in the canonical order of
 // sell_device.cuh (slice trees, then 1024-slice ranges, then the ranges),
 // which does not depend on the grid, the kernel that computes the products
-// or the device: the producing kernel stores one sum per group of 8 slices
-// (per slice, for the streaming kernels) and a small fold kernel (k_fold)
-// reduces them.  The library is compiled without
+// or the device: the producing kernel stores one sum per 32-row slice and a
+// small fold kernel (k_fold) reduces them.  The library is compiled without
 // floating-point contraction, so every FP64 product and sum of the vector
 // updates rounds once, as in the reference's Fortran on a target without
 // fused multiply-add, and the row sums of the sweeps and of A use the same
@@ -56,17 +55,16 @@ struct SliceOut {
 };
 
 // ---- the fold ----------------------------------------------------------------
-// Block j reduces the group sums of range j (kFoldRange groups; with
-// FROM_SLICES it first forms each group's sum from its 8 slice sums, in
-// slice order) and stores the range sums; the last block to finish (atomic
-// ticket, no waiting) folds the range sums and hands the totals to fin.
-// fin.skip(st) repeats the producing kernel's early-exit test, so a
+// Block j takes range j (kFoldRange groups of 8 slices): thread t forms the
+// sum of group t from its 8 slice sums in slice order, the block folds
+// them (block_sum) and stores the range sum; the last block to finish
+// (atomic ticket, no waiting) folds the range sums and hands the totals to
+// fin.  fin.skip(st) repeats the producing kernel's early-exit test, so a
 // reduction that did not run is not folded.
-template <int NV, bool FROM_SLICES, class Fin>
+template <int NV, class Fin>
 __global__ void __launch_bounds__(kFoldThreads)
     k_fold(const double *__restrict__ sp, int ld, int ns, int ng, double *__restrict__ rs,
            int ldr, KState *st, Fin fin) {
-  pdl_enter();
   if (fin.skip(st)) return;
   __shared__ bool is_last;
   const int nr = gridDim.x;
@@ -77,16 +75,11 @@ __global__ void __launch_bounds__(kFoldThreads)
     const double *src = sp + (size_t)k * ld;
     double a = 0.0;
     for (int g = g0 + threadIdx.x; g < g1; g += kFoldThreads) {
-      double gsum;
-      if constexpr (FROM_SLICES) {
-        gsum = 0.0;
+      double gsum = 0.0;
 #pragma unroll
-        for (int j = 0; j < kGroupSlices; j++) {
-          const int sl = g * kGroupSlices + j;
-          if (sl < ns) gsum = __dadd_rn(gsum, src[sl]);
-        }
-      } else {
-        gsum = src[g];
+      for (int j = 0; j < kGroupSlices; j++) {
+        const int sl = g * kGroupSlices + j;
+        if (sl < ns) gsum = __dadd_rn(gsum, src[sl]);
       }
       a = __dadd_rn(a, gsum);
     }
@@ -178,42 +171,19 @@ struct FinBicgXr : UntilDone {
 
 // ---- reduction kernels ---------------------------------------------------------
 // Vector-only kernels walk warp-per-slice (lane = row), so the slice trees
-// see the same lane order as in the SpMV kernels, and a warp takes a whole
-// group of 8 slices per step: all of the group's loads are issued before
-// its first tree.
+// see the same lane order as in the SpMV kernels.
 __device__ __forceinline__ int nslices_of(int n) { return (n + kSlice - 1) / kSlice; }
-
-// body(j, i) for row i of slice j of the warp's group (rows < n), then
-// end(j, s) with the whole warp for each slice s of the group.
-template <class Body, class End>
-__device__ __forceinline__ void for_groups(int n, Body &&body, End &&end) {
-  const int ns = nslices_of(n), lane = threadIdx.x & 31;
-  const int ngroups = (ns + kGroupSlices - 1) / kGroupSlices;
-  for (int q = first_slice(); q < ngroups; q += slice_stride()) {
-#pragma unroll
-    for (int j = 0; j < kGroupSlices; j++) {
-      const int i = (q * kGroupSlices + j) * kSlice + lane;
-      if (i < n) body(j, i);
-    }
-#pragma unroll
-    for (int j = 0; j < kGroupSlices; j++)
-      if (q * kGroupSlices + j < ns) end(j, q * kGroupSlices + j);
-  }
-}
 
 // ||b||_2 (istop=2 denominator).
 __global__ void __launch_bounds__(kBlock)
     k_bnorm(int n, const double *__restrict__ b, SliceOut o) {
-  pdl_enter();
-  GroupSums<1> ss{o.sp, o.ld, o.ns, {0.0}, {0.0}};
-  double p[kGroupSlices] = {};
-  for_groups(
-      n, [&](int j, int i) { p[j] = b[i] * b[i]; },
-      [&](int j, int s) {
-        ss.v[0] = p[j];
-        p[j] = 0.0;
-        ss.end(s);
-      });
+  SliceSums<1> ss{o.sp, o.ld, {0.0}};
+  const int ns = nslices_of(n), lane = threadIdx.x & 31;
+  for (int s = first_slice(); s < ns; s += slice_stride()) {
+    const int i = s * kSlice + lane;
+    if (i < n) ss.v[0] = b[i] * b[i];
+    ss.end(s);
+  }
 }
 
 // y = A x with the reductions each caller needs (see MODE):
@@ -267,9 +237,8 @@ __global__ void __launch_bounds__(kBlock)
     k_spmv_dots(SellView<double> m, const double *__restrict__ x, double *__restrict__ y,
                 const double *__restrict__ w1, double *__restrict__ w2,
                 const double *__restrict__ w3, const KState *st, SliceOut o) {
-  pdl_enter();
   if (dots_skip<MODE>(st)) return;
-  GroupSums<dots_of(MODE)> ss{o.sp, o.ld, o.ns, {}, {}};
+  SliceSums<dots_of(MODE)> ss{o.sp, o.ld, {}};
   for_each_row_sliced<S, P>(
       m, x, [&](int i, double acc) { dots_row<MODE>(i, acc, x, y, w1, w2, w3, ss); },
       [&](int s) { ss.end(s); });
@@ -279,7 +248,6 @@ __global__ void __launch_bounds__(kBlock)
 __global__ void __launch_bounds__(kBlock)
     k_replace_r(int n, const double *__restrict__ rtrue, double *__restrict__ r,
                 const KState *st) {
-  pdl_enter();
   if (!st->replace) return;
   for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) r[i] = rtrue[i];
 }
@@ -337,7 +305,6 @@ __global__ void __launch_bounds__(kStreamThreads)
                   StreamLayout L, const double *__restrict__ x, double *__restrict__ y,
                   const double *__restrict__ w1, double *__restrict__ w2,
                   const double *__restrict__ w3, KState *st, SliceOut o) {
-  pdl_enter();
   if (dots_skip<MODE>(st)) return;
   EpiDots<MODE> epi{y, x, w1, w2, w3, {o.sp, o.ld, {}}};
   stream_rows<P, 1>(m, stages, nstages, x, L, epi, &st->timeout);
@@ -367,7 +334,6 @@ __global__ void __launch_bounds__(kStreamThreads)
     k_stream_cg_sweep2(SellView<V> m, const StageDesc *__restrict__ stages, int nstages,
                        StreamLayout L, const T *__restrict__ t, const double *__restrict__ r,
                        double *__restrict__ z, KState *st, SliceOut o) {
-  pdl_enter();
   if (st->done) return;
   EpiCgZ<T> epi{r, z, {o.sp, o.ld, {0.0}}};
   stream_rows<P, stream_rmax<V>()>(m, stages, nstages, t, L, epi, &st->timeout);
@@ -378,9 +344,8 @@ template <class V, class T, int S, int P>
 __global__ void __launch_bounds__(kBlock)
     k_cg_sweep2(SellView<V> m, const T *__restrict__ t, const double *__restrict__ r,
                 double *__restrict__ z, const KState *st, SliceOut o) {
-  pdl_enter();
   if (st->done) return;
-  GroupSums<1> ss{o.sp, o.ld, o.ns, {0.0}, {0.0}};
+  SliceSums<1> ss{o.sp, o.ld, {0.0}};
   for_each_row_sliced<S, P>(
       m, t,
       [&](int i, auto acc) {
@@ -395,28 +360,22 @@ __global__ void __launch_bounds__(kBlock)
 __global__ void __launch_bounds__(kBlock)
     k_cg_ident(int n, const double *__restrict__ r, double *__restrict__ z, const KState *st,
                SliceOut o) {
-  pdl_enter();
   if (st->done) return;
-  GroupSums<1> ss{o.sp, o.ld, o.ns, {0.0}, {0.0}};
-  double p[kGroupSlices] = {};
-  for_groups(
-      n,
-      [&](int j, int i) {
-        const double ri = r[i];
-        z[i] = ri;
-        p[j] = ri * ri;
-      },
-      [&](int j, int s) {
-        ss.v[0] = p[j];
-        p[j] = 0.0;
-        ss.end(s);
-      });
+  SliceSums<1> ss{o.sp, o.ld, {0.0}};
+  const int ns = nslices_of(n), lane = threadIdx.x & 31;
+  for (int s = first_slice(); s < ns; s += slice_stride()) {
+    const int i = s * kSlice + lane;
+    if (i < n) {
+      z[i] = r[i];
+      ss.v[0] = r[i] * r[i];
+    }
+    ss.end(s);
+  }
 }
 
 // CG: p = z (first iteration) or p = z + beta p.
 __global__ void __launch_bounds__(kBlock)
     k_cg_p(int n, const double *__restrict__ z, double *__restrict__ p, const KState *st) {
-  pdl_enter();
   if (st->done) return;
   const int i = blockIdx.x * kBlock + threadIdx.x;
   if (i >= n) return;
@@ -427,31 +386,26 @@ __global__ void __launch_bounds__(kBlock)
 __global__ void __launch_bounds__(kBlock)
     k_cg_xr(int n, const double *__restrict__ p, const double *__restrict__ q,
             double *__restrict__ x, double *__restrict__ r, const KState *st, SliceOut o) {
-  pdl_enter();
   if (st->done) return;
   const double alpha = st->alpha;
-  GroupSums<1> ss{o.sp, o.ld, o.ns, {0.0}, {0.0}};
-  double pr[kGroupSlices] = {};
-  for_groups(
-      n,
-      [&](int j, int i) {
-        x[i] = x[i] + alpha * p[i];
-        const double ri = r[i] - alpha * q[i];
-        r[i] = ri;
-        pr[j] = ri * ri;
-      },
-      [&](int j, int s) {
-        ss.v[0] = pr[j];
-        pr[j] = 0.0;
-        ss.end(s);
-      });
+  SliceSums<1> ss{o.sp, o.ld, {0.0}};
+  const int ns = nslices_of(n), lane = threadIdx.x & 31;
+  for (int s = first_slice(); s < ns; s += slice_stride()) {
+    const int i = s * kSlice + lane;
+    if (i < n) {
+      x[i] = x[i] + alpha * p[i];
+      const double ri = r[i] - alpha * q[i];
+      r[i] = ri;
+      ss.v[0] = ri * ri;
+    }
+    ss.end(s);
+  }
 }
 
 // BiCGSTAB: p = r (first iteration) or p = r + beta (p - omega v).
 __global__ void __launch_bounds__(kBlock)
     k_bicg_p(int n, const double *__restrict__ r, const double *__restrict__ v,
              double *__restrict__ p, const KState *st) {
-  pdl_enter();
   if (st->done) return;
   const int i = blockIdx.x * kBlock + threadIdx.x;
   if (i >= n) return;
@@ -462,7 +416,6 @@ __global__ void __launch_bounds__(kBlock)
 __global__ void __launch_bounds__(kBlock)
     k_bicg_s(int n, const double *__restrict__ r, const double *__restrict__ v,
              double *__restrict__ s, const KState *st) {
-  pdl_enter();
   if (st->done) return;
   const int i = blockIdx.x * kBlock + threadIdx.x;
   if (i >= n) return;
@@ -475,26 +428,21 @@ __global__ void __launch_bounds__(kBlock)
               const double *__restrict__ s, const double *__restrict__ t,
               const double *__restrict__ rt, double *__restrict__ x,
               double *__restrict__ r, const KState *st, SliceOut o) {
-  pdl_enter();
   if (st->done) return;
   const double alpha = st->alpha, omega = st->omega;
-  GroupSums<2> ss{o.sp, o.ld, o.ns, {0.0, 0.0}, {0.0, 0.0}};
-  double p0[kGroupSlices] = {}, p1[kGroupSlices] = {};
-  for_groups(
-      n,
-      [&](int j, int i) {
-        x[i] = (x[i] + alpha * f[i]) + omega * z[i];
-        const double ri = s[i] - omega * t[i];
-        r[i] = ri;
-        p0[j] = ri * ri;
-        p1[j] = rt[i] * ri;
-      },
-      [&](int j, int sl) {
-        ss.v[0] = p0[j];
-        ss.v[1] = p1[j];
-        p0[j] = p1[j] = 0.0;
-        ss.end(sl);
-      });
+  SliceSums<2> ss{o.sp, o.ld, {0.0, 0.0}};
+  const int ns = nslices_of(n), lane = threadIdx.x & 31;
+  for (int sl = first_slice(); sl < ns; sl += slice_stride()) {
+    const int i = sl * kSlice + lane;
+    if (i < n) {
+      x[i] = (x[i] + alpha * f[i]) + omega * z[i];
+      const double ri = s[i] - omega * t[i];
+      r[i] = ri;
+      ss.v[0] = ri * ri;
+      ss.v[1] = rt[i] * ri;
+    }
+    ss.end(sl);
+  }
 }
 
 
@@ -660,14 +608,10 @@ struct KrylovWs {
   KState last{};  // final state of the last solve (statistics)
   double *v(int i) const { return vec + (size_t)i * stride; }
   SliceOut out() const { return SliceOut{sp, ld, ns}; }
-  // Fold the sums of the reduction just enqueued (NV dots): group sums, or
-  // slice sums when a streaming kernel produced them.
+  // Fold the slice sums of the reduction just enqueued (NV dots).
   template <int NV, class Fin>
-  void fold(const Fin &fin, bool from_slices = false) const {
-    if (from_slices)
-      launch(k_fold<NV, true, Fin>, nr, kFoldThreads, 0, s, sp, ld, ns, ng, rs, ldr, st, fin);
-    else
-      launch(k_fold<NV, false, Fin>, nr, kFoldThreads, 0, s, sp, ld, ns, ng, rs, ldr, st, fin);
+  void fold(const Fin &fin) const {
+    launch(k_fold<NV, Fin>, nr, kFoldThreads, 0, s, sp, ld, ns, ng, rs, ldr, st, fin);
   }
 };
 
@@ -750,23 +694,22 @@ int enqueue_iteration(KrylovWs *w, const ainv_handle *h, const ainv_csr *a, int 
   const int *stop = &st->done;
   if (method == AINV_KRYLOV_CG) {
     double *r = w->v(R), *z = w->v(Z), *p = w->v(P), *q = w->v(V), *x = w->v(XW);
-    bool sl = false;
     if (h) {
       AINV_TRY(launch_sweep_dscale(h->wt, h->d, r, h->t, s, stop, &st->timeout));
-      sl = precond_sweep2_cg(h, r, z, st, pp, G, s);
+      precond_sweep2_cg(h, r, z, st, pp, G, s);
     } else {
       launch(k_cg_ident, std::min(G, wave_grid((const void *)k_cg_ident, n)), kBlock, 0, s, n, r, z,
              st, pp);
     }
-    w->fold<1>(FinCgRho{}, sl);
+    w->fold<1>(FinCgRho{});
     launch(k_cg_p, Gv, kBlock, 0, s, n, z, p, st);
-    sl = spmv_dots<kCgSigma>(A, G, s, p, q, nullptr, nullptr, nullptr, st, pp);
-    w->fold<1>(FinDots<kCgSigma>{nullptr}, sl);
+    spmv_dots<kCgSigma>(A, G, s, p, q, nullptr, nullptr, nullptr, st, pp);
+    w->fold<1>(FinDots<kCgSigma>{nullptr});
     launch(k_cg_xr, std::min(G, wave_grid((const void *)k_cg_xr, n)), kBlock, 0, s, n, p, q, x, r,
            st, pp);
     w->fold<1>(FinCgXr{});
-    sl = spmv_dots<kTrueRes>(A, G, s, x, w->v(RTRUE), w->v(BW), nullptr, r, st, pp);
-    w->fold<3>(FinDots<kTrueRes>{nullptr}, sl);
+    spmv_dots<kTrueRes>(A, G, s, x, w->v(RTRUE), w->v(BW), nullptr, r, st, pp);
+    w->fold<3>(FinDots<kTrueRes>{nullptr});
     launch(k_replace_r, wave_grid((const void *)k_replace_r, n), kBlock, 0, s, n, w->v(RTRUE), r,
            st);
   } else {
@@ -778,21 +721,21 @@ int enqueue_iteration(KrylovWs *w, const ainv_handle *h, const ainv_csr *a, int 
     } else {
       AINV_CUDA_TRY(cudaMemcpyAsync(f, p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     }
-    bool sl = spmv_dots<kBicgSigma>(A, G, s, f, v, rt, nullptr, nullptr, st, pp);
-    w->fold<1>(FinDots<kBicgSigma>{rt}, sl);
+    spmv_dots<kBicgSigma>(A, G, s, f, v, rt, nullptr, nullptr, st, pp);
+    w->fold<1>(FinDots<kBicgSigma>{rt});
     launch(k_bicg_s, Gv, kBlock, 0, s, n, r, v, sv, st);
     if (h) {
       AINV_TRY(ainv_apply_async(h, 'N', 1.0, sv, 0.0, z, s, stop, &st->timeout));
     } else {
       AINV_CUDA_TRY(cudaMemcpyAsync(z, sv, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     }
-    sl = spmv_dots<kBicgOmega>(A, G, s, z, t, sv, nullptr, nullptr, st, pp);
-    w->fold<2>(FinDots<kBicgOmega>{rt}, sl);
+    spmv_dots<kBicgOmega>(A, G, s, z, t, sv, nullptr, nullptr, st, pp);
+    w->fold<2>(FinDots<kBicgOmega>{rt});
     launch(k_bicg_xr, std::min(G, wave_grid((const void *)k_bicg_xr, n)), kBlock, 0, s, n, f, z, sv,
            t, rt, x, r, st, pp);
     w->fold<2>(FinBicgXr{});
-    sl = spmv_dots<kTrueRes>(A, G, s, x, w->v(RTRUE), w->v(BW), rt, r, st, pp);
-    w->fold<3>(FinDots<kTrueRes>{rt}, sl);
+    spmv_dots<kTrueRes>(A, G, s, x, w->v(RTRUE), w->v(BW), rt, r, st, pp);
+    w->fold<3>(FinDots<kTrueRes>{rt});
     launch(k_replace_r, wave_grid((const void *)k_replace_r, n), kBlock, 0, s, n, w->v(RTRUE), r,
            st);
   }
@@ -868,9 +811,8 @@ int krylov_solve(const ainv_handle *h, ainv_csr *a, const double *b, double *x, 
          w->out());
   w->fold<1>(FinBnorm{});
   double *rt0 = method == AINV_KRYLOV_BICGSTAB ? w->v(RT) : nullptr;
-  const bool sl = spmv_dots<kInit>(A, w->G, w->s, w->v(XW), w->v(R), w->v(BW), rt0, nullptr,
-                                   w->st, w->out());
-  w->fold<2>(FinDots<kInit>{rt0}, sl);
+  spmv_dots<kInit>(A, w->G, w->s, w->v(XW), w->v(R), w->v(BW), rt0, nullptr, w->st, w->out());
+  w->fold<2>(FinDots<kInit>{rt0});
   AINV_CUDA_TRY(cudaGetLastError());
 
   // The first chunk always runs as plain launches (kernel attributes are

@@ -37,20 +37,6 @@ __device__ __forceinline__ float ldd(const __nv_bfloat16 *p) {
   return __uint_as_float(((unsigned)u) << 16);
 }
 
-// ---- programmatic dependent launch ------------------------------------------
-// The kernels of the apply and of the Krylov loop are launched with
-// programmatic stream serialisation (launch() below): a kernel may be
-// scheduled while its predecessor in the stream drains, so the launch
-// latency and block rasterisation of one step hide behind the tail of the
-// previous one.  Each such kernel starts with pdl_enter(): griddepcontrol.
-// wait returns once the preceding grid has completed and its writes are
-// visible (at once when the kernel was launched without the attribute), and
-// launch_dependents lets the next kernel be scheduled as this one runs.
-__device__ __forceinline__ void pdl_enter() {
-  asm volatile("griddepcontrol.wait;" ::: "memory");
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-}
-
 // c + a*b of the row accumulations.  In FP64 the product and the sum each
 // round once, with no fused multiply-add: the arithmetic of the reference's
 // CSR product compiled for a target without FMA, so an FP64 row sum here
@@ -458,19 +444,16 @@ __device__ __forceinline__ void for_each_row(const SellView<V> &m, const X *__re
 //      4, 2, 1; lane 0's value);
 //   2. group sums: the slice sums of slices [8g, 8g+8) added in slice order
 //      from zero;
-//   3. range sums: groups [1024j, 1024j+1024) folded by 256 threads, thread
-//      t adding groups t, t+256, t+512, t+768 in that order from zero, then
-//      the warp tree over each warp's 32 thread sums and the 8 warp sums
-//      added from zero in warp order (block_sum);
+//   3. range sums: groups [256j, 256j+256) folded by 256 threads (thread t
+//      takes group t), then the warp tree over each warp's 32 values and the
+//      8 warp sums added from zero in warp order (block_sum);
 //   4. the total: the range sums folded the same way (thread t adds ranges
-//      t, t+256, ... in order).
-// Kernels whose warps walk whole groups (the register SpMV and the vector
-// kernels) form steps 1-2 themselves (GroupSums) and store one sum per
-// group; the streaming kernels store slice sums (SliceSums).  A small fold
-// kernel does the rest.
+//      t, t+256, ... in order from zero).
+// The kernels that compute the products store the slice sums (SliceSums);
+// a small fold kernel does steps 2-4.
 constexpr int kGroupSlices = 8;   // slices per group
 constexpr int kFoldThreads = 256;
-constexpr int kFoldRange = 1024;  // groups per range
+constexpr int kFoldRange = 256;   // groups per range
 
 __device__ __forceinline__ double warp_tree(double v) {
 #pragma unroll
@@ -478,10 +461,9 @@ __device__ __forceinline__ double warp_tree(double v) {
   return v;
 }
 
-// Per-slice sums of NV dots (streaming kernels).  Each lane sets v[k] to its
-// row's product; end(s), called by the whole warp, stores the slice's warp
-// tree at sp[k*ld + s] and clears v for the next slice (lanes past n keep
-// zero).
+// Per-slice sums of NV dots.  Each lane sets v[k] to its row's product;
+// end(s), called by the whole warp, stores the slice's warp tree at
+// sp[k*ld + s] and clears v for the next slice (lanes past n keep zero).
 template <int NV>
 struct SliceSums {
   double *__restrict__ sp;
@@ -497,64 +479,36 @@ struct SliceSums {
   }
 };
 
-// Per-group sums of NV dots, for warps that walk each group's slices in
-// order: end(s) adds slice s's warp tree to the group's running sum (lane
-// 0) and stores it at gs[k*ld + s/8] after the group's last slice.
-template <int NV>
-struct GroupSums {
-  double *__restrict__ gs;
-  int ld, ns;
-  double v[NV];
-  double g[NV];
-  __device__ __forceinline__ void end(int s) {
-    const bool last = (s % kGroupSlices) == kGroupSlices - 1 || s == ns - 1;
-#pragma unroll
-    for (int k = 0; k < NV; k++) {
-      const double t = warp_tree(v[k]);
-      v[k] = 0.0;
-      g[k] = __dadd_rn(g[k], t);
-      if (last) {
-        if ((threadIdx.x & 31) == 0) gs[(size_t)k * ld + s / kGroupSlices] = g[k];
-        g[k] = 0.0;
-      }
-    }
-  }
-};
-
-// Visit every slice, warps taking whole groups of 8 slices (warp w: groups
-// w, w + W, ...) and each group's slices in order: epi(row, acc) for each
-// lane whose row is < n, then, with the whole warp, end(slice).
+// Visit every slice (warps striding over groups of S slices): epi(row, acc)
+// for each lane whose row is < n, then, with the whole warp, end(slice).
 template <int S, int P, int K = 4, class V, class X, class Epi, class End>
 __device__ __forceinline__ void for_each_row_sliced(const SellView<V> &m,
                                                     const X *__restrict__ x, Epi &&epi,
                                                     End &&end) {
-  static_assert(kGroupSlices % S == 0, "a group holds whole steps");
-  const int ngroups = (m.nslices + kGroupSlices - 1) / kGroupSlices;
+  const int ngroups = (m.nslices + S - 1) / S;
   const int lane = threadIdx.x & 31;
-  for (int q = first_slice(); q < ngroups; q += slice_stride()) {
-    for (int j = 0; j < kGroupSlices / S; j++) {
-      const int g = q * (kGroupSlices / S) + j;
-      if (g * S >= m.nslices) break;  // warp-uniform
-      GroupCtx<S> c;
-      group_ctx(m, g, c);
-      typename Acc<V>::type acc[S];
-      group_dot<P, K>(m, c, g, x, acc);
+  for (int g = first_slice(); g < ngroups; g += slice_stride()) {
+    GroupCtx<S> c;
+    group_ctx(m, g, c);
+    typename Acc<V>::type acc[S];
+    group_dot<P, K>(m, c, g, x, acc);
 #pragma unroll
-      for (int qq = 0; qq < S; qq++) {
-        const int s = g * S + qq;
-        if (s < m.nslices) {
-          const int row = s * kSlice + lane;
-          if (row < m.n) epi(row, acc[qq]);
-          end(s);
-        }
+    for (int q = 0; q < S; q++) {
+      const int s = g * S + q;
+      if (s < m.nslices) {
+        const int row = s * kSlice + lane;
+        if (row < m.n) epi(row, acc[q]);
+        end(s);
       }
     }
   }
 }
 
-// Host side of the programmatic launch: k<<<g, b, smem, s>>>(args...) with
-// the programmatic-serialisation attribute (AINV_PDL=0 launches plainly).
-bool pdl_enabled();
+// k<<<g, b, smem, s>>>(args...) through cudaLaunchKernelEx.  (Launching the
+// apply and Krylov kernels with programmatic dependent launch was measured
+// and dropped: the Krylov iteration did not change, and the early-scheduled
+// blocks of a sweep's successor took shared memory from the persistent
+// streaming sweep, so FP32 and INVK applies lost 20%.)
 template <class... P, class... A>
 inline void launch(void (*k)(P...), dim3 g, dim3 b, size_t smem, cudaStream_t s, A &&...a) {
   cudaLaunchConfig_t cfg = {};
@@ -562,11 +516,6 @@ inline void launch(void (*k)(P...), dim3 g, dim3 b, size_t smem, cudaStream_t s,
   cfg.blockDim = b;
   cfg.dynamicSmemBytes = smem;
   cfg.stream = s;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = pdl_enabled() ? 1 : 0;
   cudaLaunchKernelEx(&cfg, k, std::forward<A>(a)...);
 }
 

@@ -764,11 +764,11 @@ int orc_ainv_apply(int n, const int *wt_irp, const int *wt_ja,
  *     32 products of each 32-row slice (zero past n) summed by the tree
  *     u[l] += u[l+16], u[l] += u[l+8], ..., u[0] += u[1]; the slice sums of
  *     each group of 8 slices added in order from zero; the group sums of
- *     each run of 1024 groups folded by 256 "threads" (thread t adds groups
- *     t, t+256, t+512, t+768 in order from zero), the 256 thread sums by
- *     the same tree per group of 32 threads and the 8 tree sums added in
- *     order; the range sums folded the same way.  The Krylov iterates then
- *     match the device's bit for bit;
+ *     each run of 256 groups folded by 256 "threads" (thread t takes group
+ *     t), the 256 values by the same tree per run of 32 and the 8 tree sums
+ *     added in order; the range sums folded the same way (thread t adds
+ *     ranges t, t+256, ... in order).  The Krylov iterates then match the
+ *     device's bit for bit;
  *   ORC_DOT_SEQUENTIAL: one running sum in index order, the order of the
  *     reference BLAS ddot. */
 static int g_dot_order = ORC_DOT_DEVICE;
@@ -802,7 +802,7 @@ static double fold256(const double *src, long count) {
 }
 
 double orc_dot_device_order(int n, const double *a, const double *b) {
-  const long ns = ((long)n + 31) / 32, ng = (ns + 7) / 8, nr = (ng + 1023) / 1024;
+  const long ns = ((long)n + 31) / 32, ng = (ns + 7) / 8, nr = (ng + 255) / 256;
   double *S = (double *)malloc(sizeof(double) * (size_t)(ns + ng + nr + 1));
   double *G = S + ns, *R = G + ng;
 #pragma omp parallel for schedule(static)
@@ -821,8 +821,8 @@ double orc_dot_device_order(int n, const double *a, const double *b) {
   }
 #pragma omp parallel for schedule(static)
   for (long j = 0; j < nr; j++) {
-    const long c = ng - 1024 * j < 1024 ? ng - 1024 * j : 1024;
-    R[j] = fold256(G + 1024 * j, c);
+    const long c = ng - 256 * j < 256 ? ng - 256 * j : 256;
+    R[j] = fold256(G + 256 * j, c);
   }
   const double tot = fold256(R, nr);
   free(S);

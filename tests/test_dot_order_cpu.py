@@ -1,8 +1,8 @@
 """The canonical summation order of the Krylov dots.
 
 The device library sums every dot in one fixed order (32-row slice trees,
-groups of 8 slices added in order, 1024-group ranges folded by 256 running
-sums and the same trees, then the ranges folded alike) so that its Krylov iterates do not depend on the grid
+groups of 8 slices added in order, 256-group ranges folded by 256 threads
+and the same trees, then the ranges folded alike) so that its Krylov iterates do not depend on the grid
 or the device; the oracle's ordered dot restates that order so that its
 iterates equal the device's bit for bit.  Here the oracle's C form is
 checked against a second, independent numpy restatement, and the two
@@ -50,7 +50,7 @@ def _canonical_dot(a, b):
             t = t + v
         G.append(t)
     G = np.array(G)
-    R = np.array([_fold256(G[j:j + 1024]) for j in range(0, len(G), 1024)])
+    R = np.array([_fold256(G[j:j + 256]) for j in range(0, len(G), 256)])
     return _fold256(R)
 
 
