@@ -69,21 +69,28 @@ __global__ void __launch_bounds__(kFoldThreads)
   __shared__ bool is_last;
   const int nr = gridDim.x;
   const int g0 = blockIdx.x * kFoldRange, g1 = min(ng, g0 + kFoldRange);
+  // one group per thread (kFoldRange == kFoldThreads): all of the thread's
+  // slice sums are loaded before the first add
+  static_assert(kFoldRange == kFoldThreads, "one group per thread");
   double v[NV];
+  double raw[NV][kGroupSlices];
+  const int g = g0 + threadIdx.x;
+#pragma unroll
+  for (int k = 0; k < NV; k++)
+#pragma unroll
+    for (int j = 0; j < kGroupSlices; j++) {
+      const int sl = g * kGroupSlices + j;
+      raw[k][j] = (g < g1 && sl < ns) ? __ldg(sp + (size_t)k * ld + sl) : 0.0;
+    }
 #pragma unroll
   for (int k = 0; k < NV; k++) {
-    const double *src = sp + (size_t)k * ld;
-    double a = 0.0;
-    for (int g = g0 + threadIdx.x; g < g1; g += kFoldThreads) {
-      double gsum = 0.0;
+    double gsum = 0.0;
 #pragma unroll
-      for (int j = 0; j < kGroupSlices; j++) {
-        const int sl = g * kGroupSlices + j;
-        if (sl < ns) gsum = __dadd_rn(gsum, src[sl]);
-      }
-      a = __dadd_rn(a, gsum);
+    for (int j = 0; j < kGroupSlices; j++) {
+      const int sl = g * kGroupSlices + j;
+      if (g < g1 && sl < ns) gsum = __dadd_rn(gsum, raw[k][j]);
     }
-    v[k] = a;
+    v[k] = __dadd_rn(0.0, gsum);  // the thread's running sum, from zero
   }
   block_sum<NV>(v);
   if (threadIdx.x == 0) {

@@ -203,6 +203,9 @@ template <int NV, class Body>
 __device__ __forceinline__ void for_chunks_group(const Table *tab, const GroupDesc &gd,
                                                  unsigned act, int lb, Body &&body) {
   __shared__ double sh[kChunkBatch][kMaxMembers][NV][kWarps];
+  __shared__ double *part[kMaxMembers];
+  if ((int)threadIdx.x < gd.nmem) part[threadIdx.x] = tab->slot[gd.mem[threadIdx.x]].partials;
+  __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nb = gd.nb, nchunks = gd.nchunks;
   for (int c0 = lb; c0 < nchunks; c0 += kChunkBatch * nb) {
@@ -232,7 +235,7 @@ __device__ __forceinline__ void for_chunks_group(const Table *tab, const GroupDe
       if (c < nchunks && i < gd.nmem && ((act >> i) & 1u)) {
         double sum = 0.0;
         for (int w = 0; w < kWarps; w++) sum += sh[q][i][k][w];
-        tab->slot[gd.mem[i]].partials[k * nchunks + c] = sum;
+        part[i][k * nchunks + c] = sum;
       }
     }
     __syncthreads();
@@ -280,12 +283,28 @@ __device__ __forceinline__ bool slot_fold(double (&v)[NV], const double *partial
 
 #define SRV_RUNNING (ss->phase == kRun && !st->done)
 
-// Prologue of the operator kernels: the block's group, or return.
+// Prologue of the operator kernels: the block's group (copied out of the
+// table, so that the stores of the inner loops cannot force reloads), or
+// return.
 #define SRV_GROUP_PROLOGUE                                         \
   const int grp = tab->block_group[blockIdx.x];                   \
   if (grp < 0) return;                                            \
-  const GroupDesc &gd = tab->group[grp];                          \
+  const GroupDesc gd = tab->group[grp];                           \
   const int lb = blockIdx.x - gd.b0;
+
+// The members' vector pointers an operator kernel needs (up to 5 each),
+// staged once per block in shared memory; the operator (A, W^T, Z, D^-1)
+// is the same for every member and is read from member 0.
+constexpr int kMemberVecs = 5;
+struct MemberVecs {
+  void *p[kMaxMembers][kMemberVecs];
+};
+template <class F>
+__device__ __forceinline__ void stage_members(const Table *tab, const GroupDesc &gd,
+                                              MemberVecs &mv, F &&pick) {
+  if ((int)threadIdx.x < gd.nmem) pick(tab->slot[gd.mem[threadIdx.x]], mv.p[threadIdx.x]);
+  __syncthreads();
+}
 
 __device__ __forceinline__ bool slot_running(const SlotState *ss) {
   return ss->phase == kRun && !ss->k.done;
@@ -344,16 +363,16 @@ __global__ void __launch_bounds__(kBlock) k_srv_s(const Table *tab, SlotState *s
 // Sweep 1 of the apply for the active members of a group:
 // t = D^-1 .* (W^T src), chunk by chunk, every member in turn.
 template <class V, class T>
-__device__ __forceinline__ void sweep1_group(const Table *tab, const GroupDesc &gd, unsigned act,
-                                             int src, int lb) {
+__device__ __forceinline__ void sweep1_group(const Mat &wt, const V *__restrict__ d,
+                                             const GroupDesc &gd, const MemberVecs &mv,
+                                             unsigned act, int lb) {
   for (int c = lb; c < gd.nchunks; c += gd.nb)
     for (int i = 0; i < gd.nmem; i++) {
       if (!((act >> i) & 1u)) continue;
-      const SlotDesc &sd = tab->slot[gd.mem[i]];
-      const V *__restrict__ d = (const V *)sd.d;
-      T *__restrict__ t = (T *)sd.t;
+      const double *src = (const double *)mv.p[i][0];
+      T *__restrict__ t = (T *)mv.p[i][1];
       auto epi = [&](int row, auto acc) { t[row] = (T)(ldd(d + row) * acc); };
-      chunk_rows<V>(sd.wt, c, sd.vec[src], epi);
+      chunk_rows<V>(wt, c, src, epi);
     }
 }
 
@@ -380,34 +399,42 @@ template <bool ACC>
 __global__ void __launch_bounds__(kBlock) k_srv_sweep1(const Table *tab, SlotState *sts,
                                                        int src) {
   SRV_GROUP_PROLOGUE
-  const int prec = tab->slot[gd.mem[0]].wt.prec;
-  const unsigned act = sweep_members<ACC>(tab, sts, gd, prec);
+  const Mat wt = tab->slot[gd.mem[0]].wt;
+  const void *d = tab->slot[gd.mem[0]].d;
+  const unsigned act = sweep_members<ACC>(tab, sts, gd, wt.prec);
   if (!act) return;
+  __shared__ MemberVecs mv;
+  stage_members(tab, gd, mv, [&](const SlotDesc &sd, void *(&p)[kMemberVecs]) {
+    p[0] = sd.vec[src];
+    p[1] = sd.t;
+  });
   if constexpr (ACC) {
-    if (prec == AINV_PREC_FP32_ACC64)
-      sweep1_group<f32w, double>(tab, gd, act, src, lb);
+    if (wt.prec == AINV_PREC_FP32_ACC64)
+      sweep1_group<f32w, double>(wt, (const f32w *)d, gd, mv, act, lb);
     else
-      sweep1_group<b16w, double>(tab, gd, act, src, lb);
+      sweep1_group<b16w, double>(wt, (const b16w *)d, gd, mv, act, lb);
   } else {
-    switch (prec) {
-      case AINV_PREC_FP64: sweep1_group<double, double>(tab, gd, act, src, lb); break;
-      case AINV_PREC_FP32: sweep1_group<float, float>(tab, gd, act, src, lb); break;
-      default: sweep1_group<__nv_bfloat16, float>(tab, gd, act, src, lb); break;
+    switch (wt.prec) {
+      case AINV_PREC_FP64: sweep1_group<double, double>(wt, (const double *)d, gd, mv, act, lb); break;
+      case AINV_PREC_FP32: sweep1_group<float, float>(wt, (const float *)d, gd, mv, act, lb); break;
+      default:
+        sweep1_group<__nv_bfloat16, float>(wt, (const __nv_bfloat16 *)d, gd, mv, act, lb);
+        break;
     }
   }
 }
 
 // Sweep 2 of the apply for the active members: dst = Z t.
 template <class V, class T>
-__device__ __forceinline__ void sweep2_group(const Table *tab, const GroupDesc &gd, unsigned act,
-                                             int dst, int lb) {
+__device__ __forceinline__ void sweep2_group(const Mat &z, const GroupDesc &gd,
+                                             const MemberVecs &mv, unsigned act, int lb) {
   for (int c = lb; c < gd.nchunks; c += gd.nb)
     for (int i = 0; i < gd.nmem; i++) {
       if (!((act >> i) & 1u)) continue;
-      const SlotDesc &sd = tab->slot[gd.mem[i]];
-      double *__restrict__ y = sd.vec[dst];
+      const T *t = (const T *)mv.p[i][0];
+      double *__restrict__ y = (double *)mv.p[i][1];
       auto epi = [&](int row, auto acc) { y[row] = 1.0 * (double)acc; };
-      chunk_rows<V>(sd.z, c, (const T *)sd.t, epi);
+      chunk_rows<V>(z, c, t, epi);
     }
 }
 
@@ -415,19 +442,24 @@ template <bool ACC>
 __global__ void __launch_bounds__(kBlock) k_srv_sweep2(const Table *tab, SlotState *sts,
                                                        int dst) {
   SRV_GROUP_PROLOGUE
-  const int prec = tab->slot[gd.mem[0]].z.prec;
-  const unsigned act = sweep_members<ACC>(tab, sts, gd, prec);
+  const Mat z = tab->slot[gd.mem[0]].z;
+  const unsigned act = sweep_members<ACC>(tab, sts, gd, z.prec);
   if (!act) return;
+  __shared__ MemberVecs mv;
+  stage_members(tab, gd, mv, [&](const SlotDesc &sd, void *(&p)[kMemberVecs]) {
+    p[0] = sd.t;
+    p[1] = sd.vec[dst];
+  });
   if constexpr (ACC) {
-    if (prec == AINV_PREC_FP32_ACC64)
-      sweep2_group<f32w, double>(tab, gd, act, dst, lb);
+    if (z.prec == AINV_PREC_FP32_ACC64)
+      sweep2_group<f32w, double>(z, gd, mv, act, lb);
     else
-      sweep2_group<b16w, double>(tab, gd, act, dst, lb);
+      sweep2_group<b16w, double>(z, gd, mv, act, lb);
   } else {
-    switch (prec) {
-      case AINV_PREC_FP64: sweep2_group<double, double>(tab, gd, act, dst, lb); break;
-      case AINV_PREC_FP32: sweep2_group<float, float>(tab, gd, act, dst, lb); break;
-      default: sweep2_group<__nv_bfloat16, float>(tab, gd, act, dst, lb); break;
+    switch (z.prec) {
+      case AINV_PREC_FP64: sweep2_group<double, double>(z, gd, mv, act, lb); break;
+      case AINV_PREC_FP32: sweep2_group<float, float>(z, gd, mv, act, lb); break;
+      default: sweep2_group<__nv_bfloat16, float>(z, gd, mv, act, lb); break;
     }
   }
 }
@@ -462,25 +494,31 @@ __global__ void __launch_bounds__(kBlock, 4) k_srv_spmv(const Table *tab, SlotSt
     }
   }
   if (!act) return;
-  for_chunks_group<3>(tab, gd, act, lb, [&](int c, int m, double (&pr)[3]) {
-    const SlotDesc &sd = tab->slot[gd.mem[m]];
-    const double *x, *w1, *w3 = nullptr;
-    double *y, *w2 = nullptr;
+  const Mat A = tab->slot[gd.mem[0]].A;
+  __shared__ MemberVecs mv;
+  stage_members(tab, gd, mv, [&](const SlotDesc &sd, void *(&p)[kMemberVecs]) {
     if (MODE == kBicgSigma) {
-      x = sd.vec[VF];
-      y = sd.vec[VV];
-      w1 = sd.vec[VRT];
+      p[0] = sd.vec[VF];
+      p[1] = sd.vec[VV];
+      p[2] = sd.vec[VRT];
     } else if (MODE == kBicgOmega) {
-      x = sd.vec[VZ];
-      y = sd.vec[VT];
-      w1 = sd.vec[VS];
+      p[0] = sd.vec[VZ];
+      p[1] = sd.vec[VT];
+      p[2] = sd.vec[VS];
     } else {
-      x = sd.vec[VX];
-      y = sd.vec[VRTRUE];
-      w1 = sd.vec[VB];
-      w2 = sd.vec[VRT];
-      w3 = sd.vec[VR];
+      p[0] = sd.vec[VX];
+      p[1] = sd.vec[VRTRUE];
+      p[2] = sd.vec[VB];
+      p[3] = sd.vec[VRT];
+      p[4] = sd.vec[VR];
     }
+  });
+  for_chunks_group<3>(tab, gd, act, lb, [&](int c, int m, double (&pr)[3]) {
+    const double *x = (const double *)mv.p[m][0];
+    double *y = (double *)mv.p[m][1];
+    const double *w1 = (const double *)mv.p[m][2];
+    const double *w2 = (const double *)mv.p[m][3];
+    const double *w3 = (const double *)mv.p[m][4];
     auto epi = [&](int i, double acc) {
       if (MODE == kTrueRes) {
         const double ri = w1[i] - acc;
@@ -498,7 +536,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_srv_spmv(const Table *tab, SlotSt
         }
       }
     };
-    chunk_rows<double>(sd.A, c, x, epi);
+    chunk_rows<double>(A, c, x, epi);
   });
   for (int m = 0; m < gd.nmem; m++) {
     if (!((act >> m) & 1u)) continue;
