@@ -240,8 +240,15 @@ int upload_sell_t(const HostCsr &a, int prec, DevSell &out) {
   m.slice_maxcol = std::move(maxcol);
   // streaming stages: kConsumerSlices warps, each with 8/sizeof(V) slices,
   // so a warp's share of a stage is about 1 KB of values at every precision
+  // (AINV_STAGE_R = 1 or 2 caps the slices per warp, for tuning)
   std::vector<StageDesc> stages;
-  const int stage_slices = kConsumerSlices * (int)std::max<size_t>(1, 8 / sizeof(V));
+  static const int rcap = [] {
+    const char *e = std::getenv("AINV_STAGE_R");
+    const int v = e ? std::atoi(e) : 0;
+    return (v == 1 || v == 2) ? v : 8;
+  }();
+  const int stage_slices =
+      kConsumerSlices * std::min(rcap, (int)std::max<size_t>(1, 8 / sizeof(V)));
   {
     const int nst = (ns + stage_slices - 1) / stage_slices;
     stages.resize((size_t)nst);
