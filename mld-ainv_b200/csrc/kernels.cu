@@ -115,7 +115,7 @@ struct EpiAxpby {
 };
 
 template <class V, class X, int P, class Epi>
-__global__ void __launch_bounds__(kStreamThreads)
+__global__ void __launch_bounds__(kStreamThreads, kStreamMinBlocks)
     k_stream(SellView<V> m, const StageDesc *__restrict__ stages, int nstages,
              const X *__restrict__ x, StreamLayout L, Epi epi, int *status,
              const int *__restrict__ stop) {

@@ -307,7 +307,7 @@ struct EpiDots {
 };
 
 template <int MODE, int P>
-__global__ void __launch_bounds__(kStreamThreads)
+__global__ void __launch_bounds__(kStreamThreads, kStreamMinBlocks)
     k_stream_dots(SellView<double> m, const StageDesc *__restrict__ stages, int nstages,
                   StreamLayout L, const double *__restrict__ x, double *__restrict__ y,
                   const double *__restrict__ w1, double *__restrict__ w2,
@@ -337,7 +337,7 @@ struct EpiCgZ {
 };
 
 template <class V, class T, int P>
-__global__ void __launch_bounds__(kStreamThreads)
+__global__ void __launch_bounds__(kStreamThreads, kStreamMinBlocks)
     k_stream_cg_sweep2(SellView<V> m, const StageDesc *__restrict__ stages, int nstages,
                        StreamLayout L, const T *__restrict__ t, const double *__restrict__ r,
                        double *__restrict__ z, KState *st, SliceOut o) {

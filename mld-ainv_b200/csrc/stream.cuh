@@ -29,11 +29,18 @@ namespace dev {
 
 constexpr int kConsumerWarps = kConsumerSlices;
 constexpr int kStreamThreads = (kConsumerWarps + 1) * 32;  // + the producer warp
+// Blocks a streaming kernel must fit per SM: the register budget of a
+// thread is capped at 65536 / (4 * kStreamThreads) = 56, so that four
+// producers per SM keep their copies in flight.
+constexpr int kStreamMinBlocks = 4;
 // Stage-buffer header: descriptor, then the sptr and iptr chunks (the
-// stage's slice pointers, copied from 16-byte-aligned starts).
+// stage's slice pointers, copied from 16-byte-aligned starts), then the
+// stage's derived words (StageDerived), written by the producer warp.
 constexpr int kDescBytes = 64;
 constexpr int kPtrChunkBytes = ((kMaxStageSlices + 1) * 4 + 24 + 15) / 16 * 16;
-constexpr int kHeaderBytes = kDescBytes + 2 * kPtrChunkBytes;
+constexpr int kDerivedOfs = kDescBytes + 2 * kPtrChunkBytes;
+constexpr int kDerivedBytes = 64;
+constexpr int kHeaderBytes = kDerivedOfs + kDerivedBytes;
 constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s
 
 __device__ __forceinline__ unsigned smem_u32(const void *p) {
@@ -126,6 +133,19 @@ struct RowVecs {
   int es[kMaxRowVecs];
 };
 static_assert(kMaxRowVecs == 3, "RowVecs initialisers list three vectors");
+
+// Per-stage words the producer derives from the descriptor while it issues
+// the copies, so that no consumer warp recomputes them: element k of a row
+// of a uniform stage sits at window-area index row + wofs[k] (for k past the
+// stage's offsets, an index inside window 0, never read: those slots hold
+// zeros), and the stage's first nrows[i] rows of row operand i are staged.
+struct __align__(16) StageDerived {
+  int wofs[kStageMaxOffsets];
+  int nrows[kMaxRowVecs];
+  int pad;
+};
+static_assert(sizeof(StageDerived) <= kDerivedBytes, "derived words overflow the header");
+static_assert(kDerivedOfs % 16 == 0, "derived words are read as 16-byte words");
 
 // Rows [r0, ce) of a row vector with es-byte elements are copied: r1
 // rounded up to a whole 16-byte granule if that stays inside the n-element
@@ -272,6 +292,7 @@ __device__ __forceinline__ void issue_stage(const SellView<V> &m,
   const unsigned char *src = nullptr;
   unsigned char *dst = nullptr;
   int bytes = 0;
+  StageDerived *dv = reinterpret_cast<StageDerived *>(buf + kDerivedOfs);
   if (lane == 0) {
     src = reinterpret_cast<const unsigned char *>(stages + st);
     dst = buf;
@@ -291,28 +312,38 @@ __device__ __forceinline__ void issue_stage(const SellView<V> &m,
     bytes = d.ibytes;
   } else if (lane < 5 + kStageMaxOffsets) {
     const int k = lane - 5;
+    int wofs = -r0;
     if (k < d.noff) {
       int a, e;
-      window_range<X>(r0, r1, pick(d.off, k), m.n, a, e);
+      const int o = pick(d.off, k);
+      window_range<X>(r0, r1, o, m.n, a, e);
       src = reinterpret_cast<const unsigned char *>(x + a);
       dst = buf + kHeaderBytes + L.vb + L.ib + k * L.xw;
       bytes = (e - a) * (int)sizeof(X);
+      wofs = k * (L.xw / (int)sizeof(X)) + o - a;
     }
+    dv->wofs[k] = wofs;
   } else if (lane < 5 + kStageMaxOffsets + kMaxRowVecs) {
     const int i = lane - 5 - kStageMaxOffsets;
     const void *p = pick(rv.p, i);
     const int es = pick(rv.es, i);
+    int nrows = 0;
     if (i < L.nrv && p) {
       const int ce = row_copy_end(r0, r1, m.n, es);
       src = reinterpret_cast<const unsigned char *>(p) + (size_t)r0 * es;
       dst = buf + kHeaderBytes + L.vb + L.ib + L.noff * L.xw + i * L.rw;
       bytes = (ce - r0) * es;
+      nrows = ce - r0;
     }
+    dv->nrows[i] = nrows;
   }
   if (bytes > 0) {
     mbar_add_tx(bar, (unsigned)bytes);
     bulk_g2s(dst, src, (unsigned)bytes, bar);
   }
+  // the derived words are plain shared-memory stores: the warp barrier
+  // orders them before lane 0's arrive, whose release the consumers'
+  // acquiring wait on the full barrier pairs with
   __syncwarp();
   if (lane == 0) mbar_arrive(bar);
 }
@@ -344,25 +375,26 @@ __device__ __forceinline__ StageDesc desc_from(const int4 &a, const int4 &b, con
   return d;
 }
 
-// Per-stage constants of a uniform stage, hoisted out of the row loop:
-// element k of a row lives at window-area index row + wofs[k].
+// Per-stage constants of a uniform stage, held in registers for the row
+// loop: element k of a row lives at window-area index row + wofs[k].
 struct UniformStage {
   int noff;
   int wofs[kStageMaxOffsets];
 };
-template <class X>
-__device__ __forceinline__ void uniform_stage(const StageDesc &d, const StreamLayout &L, int n,
+__device__ __forceinline__ void uniform_stage(const StageDesc &d, const StageDerived &dv,
                                               UniformStage &u) {
   u.noff = d.noff;
-  const int r0 = d.s0 * kSlice, r1 = min(n, d.s1 * kSlice);
-  const int xwe = L.xw / (int)sizeof(X);
-#pragma unroll
-  for (int k = 0; k < kStageMaxOffsets; k++) {
-    const int o = k < u.noff ? d.off[k] : 0;
-    int a, e;
-    window_range<X>(r0, r1, o, n, a, e);
-    u.wofs[k] = k * xwe + o - a;
-  }
+  static_assert(kStageMaxOffsets == 8, "the offsets' shifts are read as two 16-byte words");
+  const int4 a = *reinterpret_cast<const int4 *>(dv.wofs);
+  const int4 b = *reinterpret_cast<const int4 *>(dv.wofs + 4);
+  u.wofs[0] = a.x;
+  u.wofs[1] = a.y;
+  u.wofs[2] = a.z;
+  u.wofs[3] = a.w;
+  u.wofs[4] = b.x;
+  u.wofs[5] = b.y;
+  u.wofs[6] = b.z;
+  u.wofs[7] = b.w;
 }
 
 // Dot of the lane's row of slice s with x, everything read from the stage
@@ -394,8 +426,9 @@ __device__ __forceinline__ typename Acc<V>::type stream_row_dot(const SellView<V
         SPack<V, P>::load(sv + (k0 / P) * (kSlice * P), v);
 #pragma unroll
         for (int e = 0; e < P; e++) {
+          // slots past the stage's offsets hold zeros and are skipped
           const int k = k0 + e;
-          if (k < kStageMaxOffsets && k < u.noff && v[e] != A(0))
+          if (k < kStageMaxOffsets && v[e] != A(0))
             acc = madd(v[e], (A)win[u.wofs[k < kStageMaxOffsets ? k : 0]], acc);
         }
       }
@@ -527,19 +560,21 @@ __device__ __forceinline__ bool stream_rows(const SellView<V> &m,
       }
       const unsigned char *buf = base + (size_t)b * L.stage;
       const StageDesc &d = *reinterpret_cast<const StageDesc *>(buf);
+      const StageDerived &dv = *reinterpret_cast<const StageDerived *>(buf + kDerivedOfs);
       UniformStage u;
-      uniform_stage<X>(d, L, m.n, u);
+      uniform_stage(d, dv, u);
       StagedRows sr;
       sr.area = buf + kHeaderBytes + L.vb + L.ib + L.noff * L.xw;
       sr.rw = L.rw;
       sr.r0 = d.s0 * kSlice;
       {
-        const int r1 = min(m.n, d.s1 * kSlice);
+        static_assert(kMaxRowVecs == 3, "staged row counts are read as one 16-byte word");
+        const int4 c = *reinterpret_cast<const int4 *>(dv.nrows);
+        sr.nrows[0] = c.x;
+        sr.nrows[1] = c.y;
+        sr.nrows[2] = c.z;
 #pragma unroll
-        for (int i = 0; i < kMaxRowVecs; i++) {
-          sr.p[i] = rv.p[i];
-          sr.nrows[i] = (i < L.nrv && rv.p[i]) ? row_copy_end(sr.r0, r1, m.n, rv.es[i]) - sr.r0 : 0;
-        }
+        for (int i = 0; i < kMaxRowVecs; i++) sr.p[i] = rv.p[i];
       }
       const int sfirst = d.s0 + warp * L.R;
 #pragma unroll
