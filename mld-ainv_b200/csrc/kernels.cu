@@ -72,48 +72,6 @@ __global__ void __launch_bounds__(kBlock)
 }
 
 // ---- streaming variants (stream.cuh) ----------------------------------------
-template <class V>
-__device__ __forceinline__ typename Acc<V>::type to_acc(V v) { return v; }
-template <>
-__device__ __forceinline__ double to_acc<f32w>(f32w v) {
-  return (double)v.v;
-}
-template <>
-__device__ __forceinline__ double to_acc<b16w>(b16w v) {
-  return (double)__uint_as_float(((unsigned)v.v) << 16);
-}
-template <>
-__device__ __forceinline__ float to_acc<__nv_bfloat16>(__nv_bfloat16 v) {
-  return __uint_as_float(((unsigned)__bfloat16_as_ushort(v)) << 16);
-}
-
-template <class V, class T>
-struct EpiDscale {
-  const V *__restrict__ d;
-  T *__restrict__ t;
-  static constexpr int kRowVecs = 1;
-  __device__ __forceinline__ RowVecs row_vecs() const {
-    return RowVecs{{d, nullptr, nullptr}, {(int)sizeof(V), 0, 0}};
-  }
-  template <class A>
-  __device__ __forceinline__ void post(int row, A acc, const StagedRows &r) const {
-    t[row] = (T)(to_acc(r.get<V>(0, row)) * acc);
-  }
-};
-
-struct EpiAxpby {
-  double alpha, beta;
-  double *__restrict__ y;
-  static constexpr int kRowVecs = 1;
-  __device__ __forceinline__ RowVecs row_vecs() const {
-    return RowVecs{{beta == 0.0 ? nullptr : y, nullptr, nullptr}, {8, 0, 0}};
-  }
-  template <class A>
-  __device__ __forceinline__ void post(int row, A acc, const StagedRows &r) const {
-    y[row] = axpby_row(alpha, (double)acc, beta, beta == 0.0 ? 0.0 : r.get<double>(0, row));
-  }
-};
-
 template <class V, class X, int P, class Epi>
 __global__ void __launch_bounds__(kStreamThreads, kStreamMinBlocks)
     k_stream(SellView<V> m, const StageDesc *__restrict__ stages, int nstages,

@@ -35,7 +35,7 @@
 #include <vector>
 
 #include "kstate.cuh"
-#include "stream.cuh"
+#include "krylov_epi.cuh"
 
 namespace ainv {
 
@@ -68,31 +68,8 @@ __global__ void __launch_bounds__(kFoldThreads)
   if (fin.skip(st)) return;
   __shared__ bool is_last;
   const int nr = gridDim.x;
-  const int g0 = blockIdx.x * kFoldRange, g1 = min(ng, g0 + kFoldRange);
-  // one group per thread (kFoldRange == kFoldThreads): all of the thread's
-  // slice sums are loaded before the first add
-  static_assert(kFoldRange == kFoldThreads, "one group per thread");
   double v[NV];
-  double raw[NV][kGroupSlices];
-  const int g = g0 + threadIdx.x;
-#pragma unroll
-  for (int k = 0; k < NV; k++)
-#pragma unroll
-    for (int j = 0; j < kGroupSlices; j++) {
-      const int sl = g * kGroupSlices + j;
-      raw[k][j] = (g < g1 && sl < ns) ? __ldg(sp + (size_t)k * ld + sl) : 0.0;
-    }
-#pragma unroll
-  for (int k = 0; k < NV; k++) {
-    double gsum = 0.0;
-#pragma unroll
-    for (int j = 0; j < kGroupSlices; j++) {
-      const int sl = g * kGroupSlices + j;
-      if (g < g1 && sl < ns) gsum = __dadd_rn(gsum, raw[k][j]);
-    }
-    v[k] = __dadd_rn(0.0, gsum);  // the thread's running sum, from zero
-  }
-  block_sum<NV>(v);
+  fold_range<NV>(sp, ld, ns, ng, blockIdx.x, v);
   if (threadIdx.x == 0) {
 #pragma unroll
     for (int k = 0; k < NV; k++) rs[(size_t)k * ldr + blockIdx.x] = v[k];
@@ -102,14 +79,7 @@ __global__ void __launch_bounds__(kFoldThreads)
   __syncthreads();
   if (!is_last) return;
   __threadfence();
-#pragma unroll
-  for (int k = 0; k < NV; k++) {
-    double a = 0.0;
-    for (int r = threadIdx.x; r < nr; r += kFoldThreads)
-      a = __dadd_rn(a, __ldcg(rs + (size_t)k * ldr + r));
-    v[k] = a;
-  }
-  block_sum<NV>(v);
+  fold_total<NV>(rs, ldr, nr, v);
   if (threadIdx.x == 0) {
     st->ticket[3] = 0u;
     fin(st, v);
@@ -134,10 +104,6 @@ __device__ __forceinline__ bool true_res_verify(const KState *st) {
 }
 __device__ __forceinline__ bool true_res_periodic(const KState *st) {
   return !st->done && st->check_every > 0 && st->iter > 0 && st->iter % st->check_every == 0;
-}
-
-constexpr int dots_of(int mode) {
-  return mode == kTrueRes ? 3 : (mode == kInit || mode == kBicgOmega) ? 2 : 1;
 }
 
 // Scalar step of an SpMV-with-dots reduction (w2: rt for BiCGSTAB, else
@@ -193,46 +159,6 @@ __global__ void __launch_bounds__(kBlock)
   }
 }
 
-// y = A x with the reductions each caller needs (see MODE):
-//   kCgSigma:   sigma = x.y, alpha = rho/sigma               (q = A p)
-//   kBicgSigma: sigma = w1.y, alpha = rho/sigma              (v = A f, w1 = rt)
-//   kBicgOmega: omega = (y.w1)/(y.y)                         (t = A z, w1 = s)
-//   kInit:      y = w1 - A x, optional copy into w2 (rt), initial norm/rho
-//   kTrueRes:   y = w1 - A x (true residual, w1 = b) compared with the
-//               recurrence residual w3 = r; runs every check_every
-//               iterations and once when the recurrence claims convergence.
-//               Decides whether r is replaced (k_replace_r) and whether the
-//               convergence stands; w2 = rt for BiCGSTAB's rho.
-// The row products of the dots go to ss; the fold does the scalar step.
-template <int MODE, class SS>
-__device__ __forceinline__ void dots_row(int i, double acc, const double *__restrict__ x,
-                                         double *__restrict__ y, const double *w1, double *w2,
-                                         const double *w3, SS &ss) {
-  if constexpr (MODE == kTrueRes || MODE == kInit) {
-    const double ri = w1[i] - acc;
-    y[i] = ri;
-    ss.v[0] = ri * ri;
-    if constexpr (MODE == kInit) {
-      if (w2) {
-        w2[i] = ri;
-        ss.v[1] = ri * ri;
-      }
-    } else {
-      const double g = ri - w3[i];
-      ss.v[1] = g * g;
-      if (w2) ss.v[2] = w2[i] * ri;
-    }
-  } else {
-    y[i] = acc;
-    if constexpr (MODE == kCgSigma) ss.v[0] = x[i] * acc;
-    if constexpr (MODE == kBicgSigma) ss.v[0] = w1[i] * acc;
-    if constexpr (MODE == kBicgOmega) {
-      ss.v[0] = acc * acc;
-      ss.v[1] = acc * w1[i];
-    }
-  }
-}
-
 template <int MODE>
 __device__ __forceinline__ bool dots_skip(const KState *st) {
   if (MODE == kTrueRes) return !true_res_verify(st) && !true_res_periodic(st);
@@ -260,52 +186,6 @@ __global__ void __launch_bounds__(kBlock)
 }
 
 // ---- streaming variants (stream.cuh) ----------------------------------------
-// Epilogue of the SpMV-with-dots kernels: the per-row operands are loaded
-// while the stage's copies land, the row products go to the slice sums.
-template <int MODE>
-struct EpiDots {
-  double *__restrict__ y;
-  const double *__restrict__ x;
-  const double *__restrict__ w1;
-  double *__restrict__ w2;
-  const double *__restrict__ w3;
-  SliceSums<dots_of(MODE)> ss;
-  static constexpr int kRowVecs = (MODE == kTrueRes) ? 3 : 1;
-  // row operands: b (init / true residual, with r and rt), p (CG sigma),
-  // rt (BiCGSTAB sigma), s (BiCGSTAB omega)
-  __device__ __host__ __forceinline__ RowVecs row_vecs() const {
-    if (MODE == kTrueRes) return RowVecs{{w1, w3, w2}, {8, 8, w2 ? 8 : 0}};
-    if (MODE == kCgSigma) return RowVecs{{x, nullptr, nullptr}, {8, 0, 0}};
-    return RowVecs{{w1, nullptr, nullptr}, {8, 0, 0}};
-  }
-  __device__ __forceinline__ void post(int i, double acc, const StagedRows &r) {
-    if constexpr (MODE == kTrueRes || MODE == kInit) {
-      const double ri = r.get<double>(0, i) - acc;
-      y[i] = ri;
-      ss.v[0] = ri * ri;
-      if constexpr (MODE == kInit) {
-        if (w2) {
-          w2[i] = ri;
-          ss.v[1] = ri * ri;
-        }
-      } else {
-        const double g = ri - r.get<double>(1, i);
-        ss.v[1] = g * g;
-        if (w2) ss.v[2] = r.get<double>(2, i) * ri;
-      }
-    } else {
-      y[i] = acc;
-      const double a = r.get<double>(0, i);
-      if constexpr (MODE == kCgSigma || MODE == kBicgSigma) ss.v[0] = a * acc;
-      if constexpr (MODE == kBicgOmega) {
-        ss.v[0] = acc * acc;
-        ss.v[1] = acc * a;
-      }
-    }
-  }
-  __device__ __forceinline__ void end_slice(int s) { ss.end(s); }
-};
-
 template <int MODE, int P>
 __global__ void __launch_bounds__(kStreamThreads, kStreamMinBlocks)
     k_stream_dots(SellView<double> m, const StageDesc *__restrict__ stages, int nstages,

@@ -568,6 +568,51 @@ __device__ __forceinline__ void block_sum(double (&v)[NV]) {
   __syncthreads();
 }
 
+// Steps 2-3 of the canonical order for range r (a block of kFoldThreads
+// threads): thread t forms group 256r + t's sum from its 8 slice sums (all
+// loaded before the first add), then block_sum folds the block's groups.
+// The range sums are valid in thread 0.
+template <int NV>
+__device__ __forceinline__ void fold_range(const double *__restrict__ sp, int ld, int ns, int ng,
+                                           int r, double (&v)[NV]) {
+  static_assert(kFoldRange == kFoldThreads, "one group per thread");
+  const int g0 = r * kFoldRange, g1 = min(ng, g0 + kFoldRange);
+  double raw[NV][kGroupSlices];
+  const int g = g0 + (int)threadIdx.x;
+#pragma unroll
+  for (int k = 0; k < NV; k++)
+#pragma unroll
+    for (int j = 0; j < kGroupSlices; j++) {
+      const int sl = g * kGroupSlices + j;
+      raw[k][j] = (g < g1 && sl < ns) ? __ldg(sp + (size_t)k * ld + sl) : 0.0;
+    }
+#pragma unroll
+  for (int k = 0; k < NV; k++) {
+    double gsum = 0.0;
+#pragma unroll
+    for (int j = 0; j < kGroupSlices; j++) {
+      const int sl = g * kGroupSlices + j;
+      if (g < g1 && sl < ns) gsum = __dadd_rn(gsum, raw[k][j]);
+    }
+    v[k] = __dadd_rn(0.0, gsum);  // the thread's running sum, from zero
+  }
+  block_sum<NV>(v);
+}
+
+// Step 4: the nr range sums (rs[k*ldr + r]) folded the same way; totals in
+// thread 0.
+template <int NV>
+__device__ __forceinline__ void fold_total(const double *rs, int ldr, int nr, double (&v)[NV]) {
+#pragma unroll
+  for (int k = 0; k < NV; k++) {
+    double a = 0.0;
+    for (int r = threadIdx.x; r < nr; r += kFoldThreads)
+      a = __dadd_rn(a, __ldcg(rs + (size_t)k * ldr + r));
+    v[k] = a;
+  }
+  block_sum<NV>(v);
+}
+
 // Grid-wide deterministic sum: every block stores its partials, the last
 // block to arrive (atomic ticket, no waiting) folds all partials in block
 // order.  Returns true in the last block, where thread 0 holds the totals in

@@ -12,18 +12,23 @@
 // (psb_dbicgstab with istop=2; true-residual replacement every 50
 // iterations for FP32/BF16 factors; convergence confirmed on b - A x).
 //
-// Results do not depend on the mix: every reduction is computed over fixed
-// 512-row chunks, each chunk summed by one block in a fixed order, and the
-// chunk sums folded in chunk order; which block handles which chunk, and how
-// many blocks a slot gets, changes nothing.  A request's iterates are thus
-// bit-identical whether it runs alone or beside others.
+// Results do not depend on the mix, and they are the single-solve results:
+// every dot is summed in the canonical order of the single-solve loop (the
+// reducing kernels store one sum per 32-row slice, a fold kernel reduces
+// them in fixed groups and ranges, the slot's last block doing the scalar
+// step), and every kernel computes a member's rows with the single-solve
+// arithmetic.  A request's iterates are thus bit-identical whether it runs
+// alone, beside others, or through ainv_gpu_solve.
 //
 // Requests on the same operator share its reads.  Active slots are grouped
-// by operator (up to kMaxMembers per group); the kernels that read A or the
-// factors (the two sweeps and the three A products) walk the group's
-// chunks, and for each chunk compute the rows of every member in turn, so a
-// chunk's values and indices come from HBM once and from the cache for the
-// other members.  The per-member arithmetic is that of a slot alone.
+// by operator (up to kMaxMembers per group).  The kernels that read A or
+// the factors (the two sweeps and the three A products) run streamed where
+// the layout allows: the stream.cuh pipeline (a producer warp feeding
+// stages by bulk copies), with each of the group's blocks working for one
+// member and the members' blocks walking the same stages side by side, so
+// a stage's values come from HBM once and from L2 for the other members.
+// Otherwise the group's blocks walk its chunks of 512 rows and compute
+// each chunk for every member in turn.
 //
 // The host side is an engine thread: requests queue on submit, are admitted
 // first-come first-served while a slot is free and their vectors fit in the
@@ -33,6 +38,7 @@
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -40,11 +46,11 @@
 #include <new>
 #include <string>
 #include <thread>
+#include <type_traits>
 #include <unordered_map>
 #include <vector>
 
-#include "kstate.cuh"
-#include "sell_device.cuh"
+#include "krylov_epi.cuh"
 
 namespace ainv {
 namespace srv {
@@ -58,29 +64,52 @@ constexpr int kMaxGrid = 4096;
 constexpr int kGroupS = 2;                    // slices per warp in one chunk
 constexpr int kChunkRows = kBlock * kGroupS;  // 512 rows: 8 warps x 2 slices
 constexpr int kRecheck = 50;                  // true-residual period for FP32/BF16 factors
+static_assert(kBlock == kFoldThreads, "the fold runs on the server's blocks");
+// Resident blocks per SM of the streamed operator kernels (their register
+// cap: 72 at 3 blocks) and the streamed grid's blocks per SM.  Their
+// operator and member pointers come from the table, not from kernel
+// parameters; at 4 blocks (56 registers) they spilled, and the served 200^3
+// solve ran 17% slower.
+#ifndef AINV_SRV_STREAM_BLOCKS
+#define AINV_SRV_STREAM_BLOCKS 3
+#endif
+constexpr int kSrvStreamBlocks = AINV_SRV_STREAM_BLOCKS;
 
 enum Vec { VX = 0, VB, VR, VRT, VP, VV, VF, VS, VZ, VT, VRTRUE, kNumVec };
 enum Phase { kIdle = 0, kInitPhase = 1, kRun = 2 };
+// Operator kernels that can run streamed: sweep 1 (W^T, D^-1 staged), sweep
+// 2 (Z), the A products with one staged operand (sigma, omega) and the true
+// residual (three staged operands).
+enum StreamKind { kSkSweep1 = 0, kSkSweep2, kSkSpmv, kSkTrue, kNumSk };
 
 struct Mat {
   int n, nslices, pack, prec;
   const int *sptr, *iptr, *idx;
   const void *val;
+  const StageDesc *stages;
+  int nstages;
 };
 
 struct SlotDesc {
-  int b0, nb;  // launch blocks [b0, b0 + nb)
+  int b0, nb;  // launch blocks [b0, b0 + nb) of the vector kernels and the fold
   int n, nchunks;
   Mat A, wt, z;
   const void *d;  // D^-1 in the factors' precision
   void *t;        // apply intermediate: double (FP64 factors) or float
   double *vec[kNumVec];
-  double *partials;  // 3 * nchunks
+  // canonical-order reductions: slice sums of up to 3 dots (ld apart) and
+  // range sums (ldr apart)
+  double *sp, *rs;
+  int ns, ng, nr, ld, ldr;
+  // streamed operator kernels: layouts, and which kinds stream (bit k)
+  StreamLayout L[kNumSk];
+  unsigned smask;
 };
 
 // Slots on one operator, served together by the operator kernels.
 struct GroupDesc {
-  int b0, nb;  // launch blocks [b0, b0 + nb)
+  int b0, nb;    // chunk-walking operator kernels: blocks [b0, b0 + nb)
+  int bs0, nbs;  // streamed operator kernels: blocks [bs0, bs0 + nbs) (nbs >= nmem)
   int nchunks, nmem;
   short mem[kMaxMembers];
 };
@@ -88,8 +117,9 @@ struct GroupDesc {
 struct Table {
   SlotDesc slot[kMaxSlots];
   GroupDesc group[kMaxSlots];
-  short block_slot[kMaxGrid];   // vector kernels: the block's slot, -1 idle
-  short block_group[kMaxGrid];  // operator kernels: the block's group, -1 idle
+  short block_slot[kMaxGrid];     // vector kernels and folds: the block's slot, -1 idle
+  short block_group[kMaxGrid];    // chunk-walking operator kernels: the block's group
+  short block_group_s[kMaxGrid];  // streamed operator kernels: the block's group
 };
 
 struct SlotState {
@@ -99,7 +129,7 @@ struct SlotState {
 };
 
 inline Mat mat_of(const DevSell &m) {
-  return Mat{m.n, m.nslices, m.pack, m.prec, m.sptr, m.iptr, m.idx, m.val};
+  return Mat{m.n, m.nslices, m.pack, m.prec, m.sptr, m.iptr, m.idx, m.val, m.stages, m.nstages};
 }
 
 // ---------------------------------------------------------------- device --
@@ -108,11 +138,12 @@ __device__ __forceinline__ SellView<V> sview(const Mat &m) {
   return SellView<V>{m.n, m.nslices, m.sptr, m.iptr, m.idx, (const V *)m.val};
 }
 
-// Rows of chunk c of M (warp w takes slice group 8c + w), epi(row, acc).
-// Values and indices stay cached (a group's members read them in turn).
-template <class V, int P, class X, class Epi>
+// Rows of chunk c of M (warp w takes slice group 8c + w): epi(row, acc) for
+// its rows, then end(s) (whole warp) for each of its slices.  Values and
+// indices stay cached (a group's members read them in turn).
+template <class V, int P, class X, class Epi, class End>
 __device__ __forceinline__ void chunk_rows_p(const Mat &mm, int c, const X *__restrict__ x,
-                                             Epi &epi) {
+                                             Epi &epi, End &end) {
   const SellView<V> m = sview<V>(mm);
   const int g = c * kWarps + (threadIdx.x >> 5);
   const int ngroups = (m.nslices + kGroupS - 1) / kGroupS;
@@ -124,152 +155,38 @@ __device__ __forceinline__ void chunk_rows_p(const Mat &mm, int c, const X *__re
   const int lane = threadIdx.x & 31;
 #pragma unroll
   for (int q = 0; q < kGroupS; q++) {
-    const int row = (g * kGroupS + q) * kSlice + lane;
-    if (row < m.n) epi(row, acc[q]);
+    const int s = g * kGroupS + q;
+    if (s < m.nslices) {
+      const int row = s * kSlice + lane;
+      if (row < m.n) epi(row, acc[q]);
+      end(s);
+    }
   }
 }
 
-template <class V, class X, class Epi>
-__device__ __forceinline__ void chunk_rows(const Mat &m, int c, const X *__restrict__ x,
-                                           Epi &epi) {
+template <class V, class X, class Epi, class End>
+__device__ __forceinline__ void chunk_rows(const Mat &m, int c, const X *__restrict__ x, Epi &epi,
+                                           End &end) {
   if constexpr (pack_ok<V, 2>()) {
-    if (m.pack == 2) return chunk_rows_p<V, 2>(m, c, x, epi);
+    if (m.pack == 2) return chunk_rows_p<V, 2>(m, c, x, epi, end);
   }
   if constexpr (pack_ok<V, 4>()) {
-    if (m.pack == 4) return chunk_rows_p<V, 4>(m, c, x, epi);
+    if (m.pack == 4) return chunk_rows_p<V, 4>(m, c, x, epi, end);
   }
   if constexpr (pack_ok<V, 8>()) {
-    if (m.pack == 8) return chunk_rows_p<V, 8>(m, c, x, epi);
+    if (m.pack == 8) return chunk_rows_p<V, 8>(m, c, x, epi, end);
   }
-  chunk_rows_p<V, 1>(m, c, x, epi);
+  chunk_rows_p<V, 1>(m, c, x, epi, end);
 }
 
-// Per-chunk sums: the block's fixed tree, stored at partials[i*nchunks + c].
-template <int NV>
-__device__ __forceinline__ void chunk_store(double (&v)[NV], double *__restrict__ partials,
-                                            int nchunks, int c) {
-  block_sum<NV>(v);
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int i = 0; i < NV; i++) partials[i * nchunks + c] = v[i];
-  }
-}
-
-// The block's chunks lb, lb+nb, ... in batches of kChunkBatch: body(c, pr)
-// accumulates chunk c's NV sums in pr; each warp folds its lanes (fixed
-// shuffle tree) into a shared slot without waiting, and one barrier per
-// batch lets the block fold its warps in order and store the chunk sums at
-// partials[i*nchunks + c] -- the same values chunk_store gives.
-constexpr int kChunkBatch = 4;
-template <int NV, class Body>
-__device__ __forceinline__ void for_chunks(int lb, int nb, int nchunks,
-                                           double *__restrict__ partials, Body &&body) {
-  __shared__ double sh[kChunkBatch][NV][kWarps];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int c0 = lb; c0 < nchunks; c0 += kChunkBatch * nb) {
-#pragma unroll
-    for (int q = 0; q < kChunkBatch; q++) {
-      const int c = c0 + q * nb;
-      if (c >= nchunks) break;  // block-uniform
-      double pr[NV];
-#pragma unroll
-      for (int i = 0; i < NV; i++) pr[i] = 0.0;
-      body(c, pr);
-#pragma unroll
-      for (int i = 0; i < NV; i++) {
-        double v = pr[i];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-        if (lane == 0) sh[q][i][warp] = v;
-      }
-    }
-    __syncthreads();
-    if (threadIdx.x < kChunkBatch * NV) {
-      const int q = threadIdx.x / NV, i = threadIdx.x % NV, c = c0 + q * nb;
-      if (c < nchunks) {
-        double s = 0.0;
-        for (int w = 0; w < kWarps; w++) s += sh[q][i][w];
-        partials[i * nchunks + c] = s;
-      }
-    }
-    __syncthreads();
-  }
-}
-
-// for_chunks for the members of a group: body(c, i, pr) accumulates member
-// i's NV sums of chunk c; the chunk sums of member i go to its slot's
-// partials, folded exactly as for_chunks folds them.
-template <int NV, class Body>
-__device__ __forceinline__ void for_chunks_group(const Table *tab, const GroupDesc &gd,
-                                                 unsigned act, int lb, Body &&body) {
-  __shared__ double sh[kChunkBatch][kMaxMembers][NV][kWarps];
-  __shared__ double *part[kMaxMembers];
-  if ((int)threadIdx.x < gd.nmem) part[threadIdx.x] = tab->slot[gd.mem[threadIdx.x]].partials;
-  __syncthreads();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int nb = gd.nb, nchunks = gd.nchunks;
-  for (int c0 = lb; c0 < nchunks; c0 += kChunkBatch * nb) {
-#pragma unroll
-    for (int q = 0; q < kChunkBatch; q++) {
-      const int c = c0 + q * nb;
-      if (c >= nchunks) break;  // block-uniform
-      for (int i = 0; i < gd.nmem; i++) {
-        if (!((act >> i) & 1u)) continue;
-        double pr[NV];
-#pragma unroll
-        for (int k = 0; k < NV; k++) pr[k] = 0.0;
-        body(c, i, pr);
-#pragma unroll
-        for (int k = 0; k < NV; k++) {
-          double v = pr[k];
-#pragma unroll
-          for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-          if (lane == 0) sh[q][i][k][warp] = v;
-        }
-      }
-    }
-    __syncthreads();
-    for (int e = threadIdx.x; e < kChunkBatch * kMaxMembers * NV; e += blockDim.x) {
-      const int q = e / (kMaxMembers * NV), i = (e / NV) % kMaxMembers, k = e % NV;
-      const int c = c0 + q * nb;
-      if (c < nchunks && i < gd.nmem && ((act >> i) & 1u)) {
-        double sum = 0.0;
-        for (int w = 0; w < kWarps; w++) sum += sh[q][i][k][w];
-        part[i][k * nchunks + c] = sum;
-      }
-    }
-    __syncthreads();
-  }
-}
-
-// The slot's last block (atomic ticket, no waiting) folds the chunk sums in
-// chunk order; true in that block, totals in thread 0.
-template <int NV>
-__device__ __forceinline__ bool slot_fold(double (&v)[NV], const double *partials, int nchunks,
-                                          int nb, unsigned *ticket) {
-  __shared__ bool is_last;
-  if (threadIdx.x == 0) {
-    __threadfence();
-    is_last = atomicAdd(ticket, 1u) == (unsigned)nb - 1;
-  }
-  __syncthreads();
-  if (!is_last) return false;
-  __threadfence();
-#pragma unroll
-  for (int i = 0; i < NV; i++) {
-    double s = 0.0;
-    for (int c = threadIdx.x; c < nchunks; c += blockDim.x) s += __ldcg(partials + i * nchunks + c);
-    v[i] = s;
-  }
-  block_sum<NV>(v);
-  if (threadIdx.x == 0) *ticket = 0u;
-  return true;
-}
+struct NoEnd {
+  __device__ __forceinline__ void operator()(int) const {}
+};
 
 // Block prologue: the block's slot, or -1.  `need` decides from the slot's
 // state whether this kernel acts on it; it is evaluated identically by
-// every block of the slot (the state changes only in the slot's last block,
-// after all blocks have passed this point).
+// every block of the slot (the state changes only in the last block of the
+// slot's fold, after all blocks have passed this point).
 #define SRV_PROLOGUE(need)                                        \
   const int slot = tab->block_slot[blockIdx.x];                   \
   if (slot < 0) return;                                           \
@@ -283,9 +200,9 @@ __device__ __forceinline__ bool slot_fold(double (&v)[NV], const double *partial
 
 #define SRV_RUNNING (ss->phase == kRun && !st->done)
 
-// Prologue of the operator kernels: the block's group (copied out of the
-// table, so that the stores of the inner loops cannot force reloads), or
-// return.
+// Prologue of the chunk-walking operator kernels: the block's group (copied
+// out of the table, so that the stores of the inner loops cannot force
+// reloads), or return.
 #define SRV_GROUP_PROLOGUE                                         \
   const int grp = tab->block_group[blockIdx.x];                   \
   if (grp < 0) return;                                            \
@@ -310,33 +227,32 @@ __device__ __forceinline__ bool slot_running(const SlotState *ss) {
   return ss->phase == kRun && !ss->k.done;
 }
 
-// r = rt = b, x = p = v = 0, ||b||; the first rho = r.r (x0 = 0).
+// The slot's slices, warp by warp over its blocks (lane = row): the walk of
+// the vector kernels that reduce, so their slice sums see the lane order of
+// the operator kernels.
+#define SRV_SLICES(sl) \
+  for (int sl = lb * kWarps + (int)(threadIdx.x >> 5); sl < sd.ns; sl += nb * kWarps)
+
+// r = rt = b, x = p = v = 0; slice sums of b.b (the fold sets ||b|| and the
+// first rho = r.r, x0 = 0).
 __global__ void __launch_bounds__(kBlock) k_srv_init(const Table *tab, SlotState *sts) {
   SRV_PROLOGUE(ss->phase == kInitPhase)
   double *x = sd.vec[VX], *r = sd.vec[VR], *rt = sd.vec[VRT], *p = sd.vec[VP], *v = sd.vec[VV];
   const double *b = sd.vec[VB];
-  for_chunks<1>(lb, nb, sd.nchunks, sd.partials, [&](int c, double (&pr)[1]) {
-#pragma unroll
-    for (int h = 0; h < kGroupS; h++) {
-      const int i = c * kChunkRows + h * kBlock + threadIdx.x;
-      if (i < n) {
-        const double bi = b[i];
-        x[i] = 0.0;
-        r[i] = bi;
-        rt[i] = bi;
-        p[i] = 0.0;
-        v[i] = 0.0;
-        pr[0] += bi * bi;
-      }
+  SliceSums<1> sums{sd.sp, sd.ld, {0.0}};
+  const int lane = threadIdx.x & 31;
+  SRV_SLICES(sl) {
+    const int i = sl * kSlice + lane;
+    if (i < n) {
+      const double bi = b[i];
+      x[i] = 0.0;
+      r[i] = bi;
+      rt[i] = bi;
+      p[i] = 0.0;
+      v[i] = 0.0;
+      sums.v[0] = bi * bi;
     }
-  });
-  double tot[1] = {0.0};
-  if (slot_fold<1>(tot, sd.partials, sd.nchunks, nb, &st->ticket[0]) && threadIdx.x == 0) {
-    const double bn = sqrt(tot[0]);
-    st->bn2 = (bn == 0.0) ? 1.0 : bn;
-    const double pr3[3] = {tot[0], tot[0], 0.0};
-    finish_dots<kInit>(st, pr3, false, nullptr);
-    ss->phase = kRun;
+    sums.end(sl);
   }
 }
 
@@ -360,48 +276,179 @@ __global__ void __launch_bounds__(kBlock) k_srv_s(const Table *tab, SlotState *s
   for (int i = lb * kBlock + threadIdx.x; i < n; i += nb * kBlock) s[i] = r[i] - alpha * v[i];
 }
 
-// Sweep 1 of the apply for the active members of a group:
-// t = D^-1 .* (W^T src), chunk by chunk, every member in turn.
-template <class V, class T>
-__device__ __forceinline__ void sweep1_group(const Mat &wt, const V *__restrict__ d,
-                                             const GroupDesc &gd, const MemberVecs &mv,
-                                             unsigned act, int lb) {
-  for (int c = lb; c < gd.nchunks; c += gd.nb)
-    for (int i = 0; i < gd.nmem; i++) {
-      if (!((act >> i) & 1u)) continue;
-      const double *src = (const double *)mv.p[i][0];
-      T *__restrict__ t = (T *)mv.p[i][1];
-      auto epi = [&](int row, auto acc) { t[row] = (T)(ldd(d + row) * acc); };
-      chunk_rows<V>(wt, c, src, epi);
+// x += alpha f + omega z, r = s - omega t; slice sums of r.r and rt.r.
+__global__ void __launch_bounds__(kBlock) k_srv_xr(const Table *tab, SlotState *sts) {
+  SRV_PROLOGUE(SRV_RUNNING)
+  const double *f = sd.vec[VF], *z = sd.vec[VZ], *s = sd.vec[VS], *t = sd.vec[VT],
+               *rt = sd.vec[VRT];
+  double *x = sd.vec[VX], *r = sd.vec[VR];
+  const double alpha = st->alpha, omega = st->omega;
+  SliceSums<2> sums{sd.sp, sd.ld, {0.0, 0.0}};
+  const int lane = threadIdx.x & 31;
+  SRV_SLICES(sl) {
+    const int i = sl * kSlice + lane;
+    if (i < n) {
+      x[i] = (x[i] + alpha * f[i]) + omega * z[i];
+      const double ri = s[i] - omega * t[i];
+      r[i] = ri;
+      sums.v[0] = ri * ri;
+      sums.v[1] = rt[i] * ri;
     }
+    sums.end(sl);
+  }
 }
 
-// Factor precisions come in two kernel families, so each kernel's register
-// budget is that of its own value types: FP64 / FP32 / BF16 (ACC = false)
-// and the FP64-accumulating FP32 / BF16 storage (ACC = true).
-__host__ __device__ inline bool acc64_prec(int prec) {
+// r := b - A x when the last true-residual check asked for it.
+__global__ void __launch_bounds__(kBlock) k_srv_replace(const Table *tab, SlotState *sts) {
+  SRV_PROLOGUE(ss->phase == kRun && st->replace)
+  const double *rtrue = sd.vec[VRTRUE];
+  double *r = sd.vec[VR];
+  for (int i = lb * kBlock + threadIdx.x; i < n; i += nb * kBlock) r[i] = rtrue[i];
+}
+
+// ---- the fold ------------------------------------------------------------------
+// The slot's blocks fold its slice sums in the canonical order (the single-
+// solve fold's steps): block lb takes ranges lb, lb + np, ... (np = the
+// slot's blocks, at most one per range); the last block to finish (atomic
+// ticket, no waiting) folds the range sums and runs fin.  fin.need(ss) is
+// the producing kernel's test, so a reduction that did not run is not
+// folded.
+template <int NV, class Fin>
+__global__ void __launch_bounds__(kBlock) k_srv_fold(const Table *tab, SlotState *sts, Fin fin) {
+  const int slot = tab->block_slot[blockIdx.x];
+  if (slot < 0) return;
+  SlotState *ss = sts + slot;
+  if (!fin.need(ss)) return;
+  const SlotDesc &sd = tab->slot[slot];
+  const int lb = blockIdx.x - sd.b0, np = min(sd.nb, sd.nr);
+  if (lb >= np) return;
+  __shared__ bool is_last;
+  double v[NV];
+  for (int r = lb; r < sd.nr; r += np) {
+    fold_range<NV>(sd.sp, sd.ld, sd.ns, sd.ng, r, v);
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int k = 0; k < NV; k++) sd.rs[(size_t)k * sd.ldr + r] = v[k];
+    }
+  }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    is_last = atomicAdd(&ss->k.ticket[3], 1u) == (unsigned)np - 1;
+  }
+  __syncthreads();
+  if (!is_last) return;
+  __threadfence();
+  fold_total<NV>(sd.rs, sd.ldr, sd.nr, v);
+  if (threadIdx.x == 0) {
+    ss->k.ticket[3] = 0u;
+    fin(ss, sd, v);
+  }
+}
+
+struct FinInit {
+  __device__ __forceinline__ bool need(const SlotState *ss) const { return ss->phase == kInitPhase; }
+  __device__ __forceinline__ void operator()(SlotState *ss, const SlotDesc &,
+                                             const double (&v)[1]) const {
+    KState *st = &ss->k;
+    const double bn = sqrt(v[0]);
+    st->bn2 = (bn == 0.0) ? 1.0 : bn;
+    const double pr[3] = {v[0], v[0], 0.0};
+    finish_dots<kInit>(st, pr, false, nullptr);
+    ss->phase = kRun;
+  }
+};
+
+// y = A x with the dots of MODE, as the single-solve SpMV kernels:
+//   kBicgSigma: v = A f, sigma = rt.v, alpha = rho/sigma
+//   kBicgOmega: t = A z, omega = (t.s)/(t.t)
+//   kTrueRes:   rtrue = b - A x against r (periodic, and on a convergence claim)
+template <int MODE>
+__device__ __forceinline__ bool srv_spmv_active(const SlotState *ss, bool *verify) {
+  const KState *st = &ss->k;
+  *verify = false;
+  if (ss->phase != kRun) return false;
+  if (MODE == kTrueRes) {
+    *verify = st->done && st->status == AINV_SUCCESS && !st->verified;
+    const bool periodic = !st->done && st->check_every > 0 && st->iter > 0 &&
+                          st->iter % st->check_every == 0;
+    return *verify || periodic;
+  }
+  return !st->done;
+}
+
+template <int MODE>
+struct FinDotsSrv {
+  __device__ __forceinline__ bool need(const SlotState *ss) const {
+    bool v;
+    return srv_spmv_active<MODE>(ss, &v);
+  }
+  __device__ __forceinline__ void operator()(SlotState *ss, const SlotDesc &sd,
+                                             const double (&v)[dots_of(MODE)]) const {
+    bool verify;
+    srv_spmv_active<MODE>(ss, &verify);
+    double pr[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < dots_of(MODE); k++) pr[k] = v[k];
+    finish_dots<MODE>(&ss->k, pr, verify, sd.vec[VRT]);
+  }
+};
+
+struct FinXr {
+  __device__ __forceinline__ bool need(const SlotState *ss) const { return slot_running(ss); }
+  __device__ __forceinline__ void operator()(SlotState *ss, const SlotDesc &,
+                                             const double (&v)[2]) const {
+    finish_iteration(&ss->k, v[0]);
+    bicg_next_rho(&ss->k, v[1]);
+  }
+};
+
+// ---- chunk-walking operator kernels ------------------------------------------
+// For groups whose operator kind does not stream (smask bit clear): the
+// group's blocks walk its 512-row chunks and compute each chunk for every
+// active member in turn.
+__host__ __device__ constexpr bool acc64_prec(int prec) {
   return prec == AINV_PREC_FP32_ACC64 || prec == AINV_PREC_BF16_ACC64;
 }
 
-// Members of the group that run the sweeps of family ACC (all members share
-// the operator, hence its precision).
+// Members of the group (bit i: member i) that run the sweeps: running
+// slots, when the group's operator belongs to family ACC and the sweep
+// `kind` is chunk-walked (streamed == false) or streamed (true).
 template <bool ACC>
-__device__ __forceinline__ unsigned sweep_members(const Table *tab, const SlotState *sts,
-                                                  const GroupDesc &gd, int prec) {
-  if (acc64_prec(prec) != ACC) return 0u;
+__device__ __forceinline__ unsigned sweep_members(const SlotState *sts, const GroupDesc &gd,
+                                                  int prec, unsigned smask, int kind,
+                                                  bool streamed) {
+  if (acc64_prec(prec) != ACC || (((smask >> kind) & 1u) != 0) != streamed) return 0u;
   unsigned act = 0u;
   for (int i = 0; i < gd.nmem; i++)
     if (slot_running(sts + gd.mem[i])) act |= 1u << i;
   return act;
 }
 
+// Sweep 1 of the apply: t = D^-1 .* (W^T src), chunk by chunk, every
+// member in turn.
+template <class V, class T>
+__device__ __forceinline__ void sweep1_group(const Mat &wt, const V *__restrict__ d,
+                                             const GroupDesc &gd, const MemberVecs &mv,
+                                             unsigned act, int lb) {
+  NoEnd end;
+  for (int c = lb; c < gd.nchunks; c += gd.nb)
+    for (int i = 0; i < gd.nmem; i++) {
+      if (!((act >> i) & 1u)) continue;
+      const double *src = (const double *)mv.p[i][0];
+      T *__restrict__ t = (T *)mv.p[i][1];
+      auto epi = [&](int row, auto acc) { t[row] = (T)(ldd(d + row) * acc); };
+      chunk_rows<V>(wt, c, src, epi, end);
+    }
+}
+
 template <bool ACC>
 __global__ void __launch_bounds__(kBlock) k_srv_sweep1(const Table *tab, SlotState *sts,
                                                        int src) {
   SRV_GROUP_PROLOGUE
-  const Mat wt = tab->slot[gd.mem[0]].wt;
-  const void *d = tab->slot[gd.mem[0]].d;
-  const unsigned act = sweep_members<ACC>(tab, sts, gd, wt.prec);
+  const SlotDesc &s0 = tab->slot[gd.mem[0]];
+  const Mat wt = s0.wt;
+  const void *d = s0.d;
+  const unsigned act = sweep_members<ACC>(sts, gd, wt.prec, s0.smask, kSkSweep1, false);
   if (!act) return;
   __shared__ MemberVecs mv;
   stage_members(tab, gd, mv, [&](const SlotDesc &sd, void *(&p)[kMemberVecs]) {
@@ -424,17 +471,18 @@ __global__ void __launch_bounds__(kBlock) k_srv_sweep1(const Table *tab, SlotSta
   }
 }
 
-// Sweep 2 of the apply for the active members: dst = Z t.
+// Sweep 2 of the apply: dst = Z t (alpha = 1, beta = 0).
 template <class V, class T>
 __device__ __forceinline__ void sweep2_group(const Mat &z, const GroupDesc &gd,
                                              const MemberVecs &mv, unsigned act, int lb) {
+  NoEnd end;
   for (int c = lb; c < gd.nchunks; c += gd.nb)
     for (int i = 0; i < gd.nmem; i++) {
       if (!((act >> i) & 1u)) continue;
       const T *t = (const T *)mv.p[i][0];
       double *__restrict__ y = (double *)mv.p[i][1];
-      auto epi = [&](int row, auto acc) { y[row] = 1.0 * (double)acc; };
-      chunk_rows<V>(z, c, t, epi);
+      auto epi = [&](int row, auto acc) { y[row] = axpby_row(1.0, (double)acc, 0.0, 0.0); };
+      chunk_rows<V>(z, c, t, epi, end);
     }
 }
 
@@ -442,8 +490,9 @@ template <bool ACC>
 __global__ void __launch_bounds__(kBlock) k_srv_sweep2(const Table *tab, SlotState *sts,
                                                        int dst) {
   SRV_GROUP_PROLOGUE
-  const Mat z = tab->slot[gd.mem[0]].z;
-  const unsigned act = sweep_members<ACC>(tab, sts, gd, z.prec);
+  const SlotDesc &s0 = tab->slot[gd.mem[0]];
+  const Mat z = s0.z;
+  const unsigned act = sweep_members<ACC>(sts, gd, z.prec, s0.smask, kSkSweep2, false);
   if (!act) return;
   __shared__ MemberVecs mv;
   stage_members(tab, gd, mv, [&](const SlotDesc &sd, void *(&p)[kMemberVecs]) {
@@ -464,165 +513,390 @@ __global__ void __launch_bounds__(kBlock) k_srv_sweep2(const Table *tab, SlotSta
   }
 }
 
-// y = A x with the dots of MODE, as the single-solve SpMV kernels:
-//   kBicgSigma: v = A f, sigma = rt.v, alpha = rho/sigma
-//   kBicgOmega: t = A z, omega = (t.s)/(t.t)
-//   kTrueRes:   rtrue = b - A x against r (periodic, and on a convergence claim)
+// The vectors of an A product of MODE for one member: x, y, w1, w2, w3 of
+// dots_row.
 template <int MODE>
-__device__ __forceinline__ bool srv_spmv_active(const SlotState *ss, bool *verify) {
-  const KState *st = &ss->k;
-  *verify = false;
-  if (ss->phase != kRun) return false;
-  if (MODE == kTrueRes) {
-    *verify = st->done && st->status == AINV_SUCCESS && !st->verified;
-    const bool periodic = !st->done && st->check_every > 0 && st->iter > 0 &&
-                          st->iter % st->check_every == 0;
-    return *verify || periodic;
+__device__ __forceinline__ void spmv_vectors(const SlotDesc &sd, void *(&p)[kMemberVecs]) {
+  if (MODE == kBicgSigma) {
+    p[0] = sd.vec[VF];
+    p[1] = sd.vec[VV];
+    p[2] = sd.vec[VRT];
+    p[3] = nullptr;
+    p[4] = nullptr;
+  } else if (MODE == kBicgOmega) {
+    p[0] = sd.vec[VZ];
+    p[1] = sd.vec[VT];
+    p[2] = sd.vec[VS];
+    p[3] = nullptr;
+    p[4] = nullptr;
+  } else {
+    p[0] = sd.vec[VX];
+    p[1] = sd.vec[VRTRUE];
+    p[2] = sd.vec[VB];
+    p[3] = sd.vec[VRT];
+    p[4] = sd.vec[VR];
   }
-  return !st->done;
+}
+
+constexpr int spmv_kind(int mode) { return mode == kTrueRes ? kSkTrue : kSkSpmv; }
+
+// Members that run the A product of MODE (streamed or chunk-walked).
+template <int MODE>
+__device__ __forceinline__ unsigned spmv_members(const SlotState *sts, const GroupDesc &gd,
+                                                 unsigned smask, bool streamed) {
+  if ((((smask >> spmv_kind(MODE)) & 1u) != 0) != streamed) return 0u;
+  unsigned act = 0u;
+  for (int i = 0; i < gd.nmem; i++) {
+    bool v;
+    if (srv_spmv_active<MODE>(sts + gd.mem[i], &v)) act |= 1u << i;
+  }
+  return act;
 }
 
 template <int MODE>
 __global__ void __launch_bounds__(kBlock, 4) k_srv_spmv(const Table *tab, SlotState *sts) {
   SRV_GROUP_PROLOGUE
-  unsigned act = 0u, ver = 0u;
-  for (int i = 0; i < gd.nmem; i++) {
-    bool v;
-    if (srv_spmv_active<MODE>(sts + gd.mem[i], &v)) {
-      act |= 1u << i;
-      if (v) ver |= 1u << i;
-    }
-  }
+  const SlotDesc &s0 = tab->slot[gd.mem[0]];
+  const unsigned act = spmv_members<MODE>(sts, gd, s0.smask, false);
   if (!act) return;
-  const Mat A = tab->slot[gd.mem[0]].A;
+  const Mat A = s0.A;
   __shared__ MemberVecs mv;
+  __shared__ double *msp[kMaxMembers];
+  __shared__ int mld[kMaxMembers];
   stage_members(tab, gd, mv, [&](const SlotDesc &sd, void *(&p)[kMemberVecs]) {
-    if (MODE == kBicgSigma) {
-      p[0] = sd.vec[VF];
-      p[1] = sd.vec[VV];
-      p[2] = sd.vec[VRT];
-    } else if (MODE == kBicgOmega) {
-      p[0] = sd.vec[VZ];
-      p[1] = sd.vec[VT];
-      p[2] = sd.vec[VS];
-    } else {
-      p[0] = sd.vec[VX];
-      p[1] = sd.vec[VRTRUE];
-      p[2] = sd.vec[VB];
-      p[3] = sd.vec[VRT];
-      p[4] = sd.vec[VR];
+    spmv_vectors<MODE>(sd, p);
+    msp[threadIdx.x] = sd.sp;
+    mld[threadIdx.x] = sd.ld;
+  });
+  for (int c = lb; c < gd.nchunks; c += gd.nb)
+    for (int m = 0; m < gd.nmem; m++) {
+      if (!((act >> m) & 1u)) continue;
+      const double *x = (const double *)mv.p[m][0];
+      double *y = (double *)mv.p[m][1];
+      const double *w1 = (const double *)mv.p[m][2];
+      double *w2 = (double *)mv.p[m][3];
+      const double *w3 = (const double *)mv.p[m][4];
+      SliceSums<dots_of(MODE)> sums{msp[m], mld[m], {}};
+      auto epi = [&](int i, double acc) { dots_row<MODE>(i, acc, x, y, w1, w2, w3, sums); };
+      auto end = [&](int s) { sums.end(s); };
+      chunk_rows<double>(A, c, x, epi, end);
     }
-  });
-  for_chunks_group<3>(tab, gd, act, lb, [&](int c, int m, double (&pr)[3]) {
-    const double *x = (const double *)mv.p[m][0];
-    double *y = (double *)mv.p[m][1];
-    const double *w1 = (const double *)mv.p[m][2];
-    const double *w2 = (const double *)mv.p[m][3];
-    const double *w3 = (const double *)mv.p[m][4];
-    auto epi = [&](int i, double acc) {
-      if (MODE == kTrueRes) {
-        const double ri = w1[i] - acc;
-        y[i] = ri;
-        pr[0] += ri * ri;
-        const double g = ri - w3[i];
-        pr[1] += g * g;
-        pr[2] += w2[i] * ri;
-      } else {
-        y[i] = acc;
-        if (MODE == kBicgSigma) pr[0] += w1[i] * acc;
-        if (MODE == kBicgOmega) {
-          pr[0] += acc * acc;
-          pr[1] += acc * w1[i];
-        }
-      }
-    };
-    chunk_rows<double>(A, c, x, epi);
-  });
-  for (int m = 0; m < gd.nmem; m++) {
-    if (!((act >> m) & 1u)) continue;
-    const int sl = gd.mem[m];
-    const SlotDesc &sd = tab->slot[sl];
-    KState *st = &sts[sl].k;
-    double tot[3] = {0.0, 0.0, 0.0};
-    if (slot_fold<3>(tot, sd.partials, gd.nchunks, gd.nb, &st->ticket[0]) && threadIdx.x == 0)
-      finish_dots<MODE>(st, tot, (ver >> m) & 1u, MODE == kTrueRes ? sd.vec[VRT] : nullptr);
-    __syncthreads();  // slot_fold's shared flag is reused by the next member
-  }
 }
 
-// x += alpha f + omega z, r = s - omega t, rn2 = r.r, rho' = rt.r.
-__global__ void __launch_bounds__(kBlock) k_srv_xr(const Table *tab, SlotState *sts) {
-  SRV_PROLOGUE(SRV_RUNNING)
-  const double *f = sd.vec[VF], *z = sd.vec[VZ], *s = sd.vec[VS], *t = sd.vec[VT],
-               *rt = sd.vec[VRT];
-  double *x = sd.vec[VX], *r = sd.vec[VR];
-  const double alpha = st->alpha, omega = st->omega;
-  for_chunks<2>(lb, nb, sd.nchunks, sd.partials, [&](int c, double (&pr)[2]) {
+// ---- streamed operator kernels -----------------------------------------------
+// The stream.cuh pipeline applied to a group: each of the group's blocks
+// works for one active member (block lb: member lb % M of the M active
+// ones, stages lb / M, lb / M + nbs / M, ...), so the members' blocks walk
+// the same stages side by side and a stage's values come from HBM once and
+// from L2 for the other members.  The member's vectors are its own; the
+// arithmetic is that of the single-solve streaming kernels.
+struct MemberWalk {
+  int slot, j0, jstride;
+};
+__device__ __forceinline__ bool member_walk(const GroupDesc &gd, unsigned act, int lb,
+                                            SlotState *sts, MemberWalk &w) {
+  const int M = __popc(act);
+  if (M == 0) return false;
+  const int per = gd.nbs / M;
+  if (per == 0) {  // the plan gives every group at least nmem blocks
+    if (lb == 0 && threadIdx.x == 0) atomicExch(&sts[gd.mem[0]].k.timeout, 1);
+    return false;
+  }
+  if (lb >= per * M) return false;
+  const int k = lb % M;  // k-th active member
+  int i = 0, seen = 0;
+  for (; i < gd.nmem; i++)
+    if ((act >> i) & 1u) {
+      if (seen == k) break;
+      seen++;
+    }
+  w.slot = gd.mem[i];
+  w.j0 = lb / M;
+  w.jstride = per;
+  return true;
+}
+
+#define SRV_STREAM_PROLOGUE                                        \
+  const int grp = tab->block_group_s[blockIdx.x];                 \
+  if (grp < 0) return;                                            \
+  const GroupDesc &gd = tab->group[grp];                          \
+  const SlotDesc &s0 = tab->slot[gd.mem[0]];                      \
+  const int lb = blockIdx.x - gd.bs0;
+
+template <class V>
+constexpr int prec_of() {
+  return std::is_same<V, double>::value   ? AINV_PREC_FP64
+         : std::is_same<V, float>::value  ? AINV_PREC_FP32
+         : std::is_same<V, f32w>::value   ? AINV_PREC_FP32_ACC64
+         : std::is_same<V, b16w>::value   ? AINV_PREC_BF16_ACC64
+                                          : AINV_PREC_BF16;
+}
+
+// Epilogues whose pointers live in shared memory (staged once per block):
+// each call rebuilds the epilogue from the shared copy, so the pointers are
+// loaded where they are used and hold no registers across the stage loop
+// (the single-solve kernels take them as kernel parameters instead).
+template <class E>
+struct SharedEpi {
+  const E *sh;
+  __device__ __forceinline__ RowVecs row_vecs() const { return sh->row_vecs(); }
+  template <class A>
+  __device__ __forceinline__ void post(int row, A acc, const StagedRows &r) const {
+    E e = *sh;
+    e.post(row, acc, r);
+  }
+};
+template <int MODE>
+struct SharedEpiDots {
+  static constexpr int NV = dots_of(MODE);
+  const EpiDots<MODE> *sh;
+  double v[NV];  // the lane's row products of the current slice
+  __device__ __forceinline__ RowVecs row_vecs() const { return sh->row_vecs(); }
+  __device__ __forceinline__ void post(int i, double acc, const StagedRows &r) {
+    EpiDots<MODE> e = *sh;
 #pragma unroll
-    for (int h = 0; h < kGroupS; h++) {
-      const int i = c * kChunkRows + h * kBlock + threadIdx.x;
-      if (i < n) {
-        x[i] = (x[i] + alpha * f[i]) + omega * z[i];
-        const double ri = s[i] - omega * t[i];
-        r[i] = ri;
-        pr[0] += ri * ri;
-        pr[1] += rt[i] * ri;
-      }
-    }
-  });
-  double tot[2] = {0.0, 0.0};
-  if (slot_fold<2>(tot, sd.partials, sd.nchunks, nb, &st->ticket[0]) && threadIdx.x == 0) {
-    finish_iteration(st, tot[0]);
-    bicg_next_rho(st, tot[1]);
+    for (int k = 0; k < NV; k++) e.ss.v[k] = v[k];
+    e.post(i, acc, r);
+#pragma unroll
+    for (int k = 0; k < NV; k++) v[k] = e.ss.v[k];
   }
+  __device__ __forceinline__ void end_slice(int s) {
+    SliceSums<NV> ss{sh->ss.sp, sh->ss.ld, {}};
+#pragma unroll
+    for (int k = 0; k < NV; k++) ss.v[k] = v[k];
+    ss.end(s);
+#pragma unroll
+    for (int k = 0; k < NV; k++) v[k] = 0.0;
+  }
+};
+
+// stream_rows over the member's walk, with the operator's view and layout
+// staged in shared memory.
+template <int P, int RMAX, class V, class X, class Epi>
+__device__ __forceinline__ void srv_stream(const Mat &mat, const StreamLayout &Lg,
+                                           const X *__restrict__ x, Epi &epi, int *status,
+                                           const MemberWalk &w) {
+  __shared__ SellView<V> m;
+  __shared__ StreamLayout L;
+  __shared__ const StageDesc *stages;
+  __shared__ int nstages;
+  if (threadIdx.x == 0) {
+    m = sview<V>(mat);
+    L = Lg;
+    stages = mat.stages;
+    nstages = mat.nstages;
+  }
+  __syncthreads();
+  stream_rows<P, RMAX>(m, stages, nstages, x, L, epi, status, w.j0, w.jstride);
 }
 
-// r := b - A x when the last true-residual check asked for it.
-__global__ void __launch_bounds__(kBlock) k_srv_replace(const Table *tab, SlotState *sts) {
-  SRV_PROLOGUE(ss->phase == kRun && st->replace)
-  const double *rtrue = sd.vec[VRTRUE];
-  double *r = sd.vec[VR];
-  for (int i = lb * kBlock + threadIdx.x; i < n; i += nb * kBlock) r[i] = rtrue[i];
+template <class V, class T, int P>
+__global__ void __launch_bounds__(kStreamThreads, kSrvStreamBlocks)
+    k_srv_stream_sweep1(const Table *tab, SlotState *sts, int src) {
+  SRV_STREAM_PROLOGUE
+  const Mat &wt = s0.wt;
+  if (wt.prec != prec_of<V>() || wt.pack != P) return;
+  const unsigned act =
+      sweep_members<acc64_prec(prec_of<V>())>(sts, gd, wt.prec, s0.smask, kSkSweep1, true);
+  MemberWalk w;
+  if (!member_walk(gd, act, lb, sts, w)) return;
+  const SlotDesc &sd = tab->slot[w.slot];
+  __shared__ EpiDscale<V, T> sh;
+  if (threadIdx.x == 0) sh = EpiDscale<V, T>{(const V *)s0.d, (T *)sd.t};
+  SharedEpi<EpiDscale<V, T>> epi{&sh};
+  srv_stream<P, stream_rmax<V>(), V>(wt, s0.L[kSkSweep1], (const double *)sd.vec[src], epi,
+                                     &sts[w.slot].k.timeout, w);
 }
 
+template <class V, class T, int P>
+__global__ void __launch_bounds__(kStreamThreads, kSrvStreamBlocks)
+    k_srv_stream_sweep2(const Table *tab, SlotState *sts, int dst) {
+  SRV_STREAM_PROLOGUE
+  const Mat &z = s0.z;
+  if (z.prec != prec_of<V>() || z.pack != P) return;
+  const unsigned act =
+      sweep_members<acc64_prec(prec_of<V>())>(sts, gd, z.prec, s0.smask, kSkSweep2, true);
+  MemberWalk w;
+  if (!member_walk(gd, act, lb, sts, w)) return;
+  const SlotDesc &sd = tab->slot[w.slot];
+  __shared__ EpiAxpby sh;
+  if (threadIdx.x == 0) sh = EpiAxpby{1.0, 0.0, sd.vec[dst]};
+  SharedEpi<EpiAxpby> epi{&sh};
+  srv_stream<P, stream_rmax<V>(), V>(z, s0.L[kSkSweep2], (const T *)sd.t, epi,
+                                     &sts[w.slot].k.timeout, w);
+}
+
+template <int MODE, int P>
+__global__ void __launch_bounds__(kStreamThreads, kSrvStreamBlocks)
+    k_srv_stream_spmv(const Table *tab, SlotState *sts) {
+  SRV_STREAM_PROLOGUE
+  const Mat &A = s0.A;
+  if (A.pack != P) return;
+  const unsigned act = spmv_members<MODE>(sts, gd, s0.smask, true);
+  MemberWalk w;
+  if (!member_walk(gd, act, lb, sts, w)) return;
+  const SlotDesc &sd = tab->slot[w.slot];
+  __shared__ EpiDots<MODE> sh;
+  if (threadIdx.x == 0) {
+    void *p[kMemberVecs];
+    spmv_vectors<MODE>(sd, p);
+    sh = EpiDots<MODE>{(double *)p[1], (const double *)p[0], (const double *)p[2], (double *)p[3],
+                       (const double *)p[4], {sd.sp, sd.ld, {}}};
+  }
+  SharedEpiDots<MODE> epi{&sh, {}};
+  void *p[kMemberVecs];
+  spmv_vectors<MODE>(sd, p);
+  srv_stream<P, 1, double>(A, s0.L[spmv_kind(MODE)], (const double *)p[0], epi,
+                           &sts[w.slot].k.timeout, w);
+}
+
+// ---- launch plan -----------------------------------------------------------------
 enum Family { kFamStd = 1, kFamAcc64 = 2 };
 
-void sweeps(const Table *tab, SlotState *sts, int grid, cudaStream_t s, int fam, int src,
-            int dst) {
-  if (fam & kFamStd) k_srv_sweep1<false><<<grid, kBlock, 0, s>>>(tab, sts, src);
-  if (fam & kFamAcc64) k_srv_sweep1<true><<<grid, kBlock, 0, s>>>(tab, sts, src);
-  if (fam & kFamStd) k_srv_sweep2<false><<<grid, kBlock, 0, s>>>(tab, sts, dst);
-  if (fam & kFamAcc64) k_srv_sweep2<true><<<grid, kBlock, 0, s>>>(tab, sts, dst);
+// What one batched iteration launches, from the registered operators: the
+// streamed kernel variants (precision and pack of W^T / Z, pack of A) with
+// their shared memory, and the chunk-walking kernels still needed.
+struct LaunchPlan {
+  std::vector<std::pair<int, int>> sw1, sw2;  // (prec, pack)
+  std::vector<int> spmv, strue;               // packs of A
+  size_t smem[kNumSk] = {0, 0, 0, 0};
+  int fb_sweep1 = 0, fb_sweep2 = 0;  // families of chunk-walked sweeps
+  bool fb_spmv = false, fb_true = false;
+  bool operator==(const LaunchPlan &o) const {
+    return sw1 == o.sw1 && sw2 == o.sw2 && spmv == o.spmv && strue == o.strue &&
+           std::equal(smem, smem + kNumSk, o.smem) && fb_sweep1 == o.fb_sweep1 &&
+           fb_sweep2 == o.fb_sweep2 && fb_spmv == o.fb_spmv && fb_true == o.fb_true;
+  }
+};
+
+// The streamed sweep kernel (WHICH = 1 or 2) of one value type and pack.
+template <int WHICH, class V, class T, int P>
+void *sweep_kernel_vp() {
+  return WHICH == 1 ? (void *)k_srv_stream_sweep1<V, T, P> : (void *)k_srv_stream_sweep2<V, T, P>;
+}
+template <int WHICH, class V, class T>
+void *sweep_kernel_p(int pack) {
+  switch (pack) {
+    case 1: return sweep_kernel_vp<WHICH, V, T, 1>();
+    case 2: if constexpr (pack_ok<V, 2>()) return sweep_kernel_vp<WHICH, V, T, 2>(); break;
+    case 4: if constexpr (pack_ok<V, 4>()) return sweep_kernel_vp<WHICH, V, T, 4>(); break;
+    case 8: if constexpr (pack_ok<V, 8>()) return sweep_kernel_vp<WHICH, V, T, 8>(); break;
+  }
+  return nullptr;
+}
+template <int WHICH>
+void *sweep_kernel(int prec, int pack) {
+  switch (prec) {
+    case AINV_PREC_FP64: return sweep_kernel_p<WHICH, double, double>(pack);
+    case AINV_PREC_FP32: return sweep_kernel_p<WHICH, float, float>(pack);
+    case AINV_PREC_BF16: return sweep_kernel_p<WHICH, __nv_bfloat16, float>(pack);
+    case AINV_PREC_FP32_ACC64: return sweep_kernel_p<WHICH, f32w, double>(pack);
+    case AINV_PREC_BF16_ACC64: return sweep_kernel_p<WHICH, b16w, double>(pack);
+  }
+  return nullptr;
+}
+template <int MODE>
+void *spmv_kernel(int pack) {
+  switch (pack) {
+    case 1: return (void *)k_srv_stream_spmv<MODE, 1>;
+    case 2: return (void *)k_srv_stream_spmv<MODE, 2>;
+  }
+  return nullptr;
 }
 
-// One batched iteration on stream s (11 launches over the whole grid, plus
-// the second family's two sweeps when both families are registered).
+// Grid of the streamed operator kernels: kSrvStreamBlocks blocks per SM.
+int stream_grid() { return std::min(kMaxGrid, kSrvStreamBlocks * sm_count()); }
+
+cudaError_t launch_raw(void *k, int grid, int threads, size_t smem, cudaStream_t s, void **args) {
+  return cudaLaunchKernel(k, dim3(grid), dim3(threads), args, smem, s);
+}
+
+void sweeps(const Table *tab, SlotState *sts, int grid, cudaStream_t s, const LaunchPlan &lp,
+            int src, int dst, int *count) {
+  const int gs = stream_grid();
+  for (const auto &v : lp.sw1) {
+    void *args[] = {(void *)&tab, (void *)&sts, (void *)&src};
+    launch_raw(sweep_kernel<1>(v.first, v.second), gs, kStreamThreads, lp.smem[kSkSweep1], s, args);
+    ++*count;
+  }
+  if (lp.fb_sweep1 & kFamStd) k_srv_sweep1<false><<<grid, kBlock, 0, s>>>(tab, sts, src), ++*count;
+  if (lp.fb_sweep1 & kFamAcc64) k_srv_sweep1<true><<<grid, kBlock, 0, s>>>(tab, sts, src), ++*count;
+  for (const auto &v : lp.sw2) {
+    void *args[] = {(void *)&tab, (void *)&sts, (void *)&dst};
+    launch_raw(sweep_kernel<2>(v.first, v.second), gs, kStreamThreads, lp.smem[kSkSweep2], s, args);
+    ++*count;
+  }
+  if (lp.fb_sweep2 & kFamStd) k_srv_sweep2<false><<<grid, kBlock, 0, s>>>(tab, sts, dst), ++*count;
+  if (lp.fb_sweep2 & kFamAcc64) k_srv_sweep2<true><<<grid, kBlock, 0, s>>>(tab, sts, dst), ++*count;
+}
+
+template <int MODE>
+void spmv(const Table *tab, SlotState *sts, int grid, cudaStream_t s, const LaunchPlan &lp,
+          int *count) {
+  const std::vector<int> &packs = MODE == kTrueRes ? lp.strue : lp.spmv;
+  for (int pk : packs) {
+    void *args[] = {(void *)&tab, (void *)&sts};
+    launch_raw(spmv_kernel<MODE>(pk), stream_grid(), kStreamThreads, lp.smem[spmv_kind(MODE)], s,
+               args);
+    ++*count;
+  }
+  if (MODE == kTrueRes ? lp.fb_true : lp.fb_spmv) {
+    k_srv_spmv<MODE><<<grid, kBlock, 0, s>>>(tab, sts);
+    ++*count;
+  }
+  k_srv_fold<dots_of(MODE), FinDotsSrv<MODE>><<<grid, kBlock, 0, s>>>(tab, sts, FinDotsSrv<MODE>{});
+  ++*count;
+}
+
+// Start of a graph launch: new slots' vectors and first scalars.
+void enqueue_init(const Table *tab, SlotState *sts, int grid, cudaStream_t s, int *count) {
+  k_srv_init<<<grid, kBlock, 0, s>>>(tab, sts);
+  k_srv_fold<1, FinInit><<<grid, kBlock, 0, s>>>(tab, sts, FinInit{});
+  *count += 2;
+}
+
+// One batched iteration on stream s, the single-solve BiCGSTAB sequence.
 cudaError_t enqueue_iteration(const Table *tab, SlotState *sts, int grid, cudaStream_t s,
-                              int fam) {
+                              const LaunchPlan &lp, int *count) {
   k_srv_p<<<grid, kBlock, 0, s>>>(tab, sts);
-  sweeps(tab, sts, grid, s, fam, VP, VF);
-  k_srv_spmv<kBicgSigma><<<grid, kBlock, 0, s>>>(tab, sts);
+  sweeps(tab, sts, grid, s, lp, VP, VF, count);
+  spmv<kBicgSigma>(tab, sts, grid, s, lp, count);
   k_srv_s<<<grid, kBlock, 0, s>>>(tab, sts);
-  sweeps(tab, sts, grid, s, fam, VS, VZ);
-  k_srv_spmv<kBicgOmega><<<grid, kBlock, 0, s>>>(tab, sts);
+  sweeps(tab, sts, grid, s, lp, VS, VZ, count);
+  spmv<kBicgOmega>(tab, sts, grid, s, lp, count);
   k_srv_xr<<<grid, kBlock, 0, s>>>(tab, sts);
-  k_srv_spmv<kTrueRes><<<grid, kBlock, 0, s>>>(tab, sts);
+  k_srv_fold<2, FinXr><<<grid, kBlock, 0, s>>>(tab, sts, FinXr{});
+  spmv<kTrueRes>(tab, sts, grid, s, lp, count);
   k_srv_replace<<<grid, kBlock, 0, s>>>(tab, sts);
+  *count += 5;
   return cudaGetLastError();
 }
-
-constexpr int kLaunchesPerIteration = 11;
 
 // ------------------------------------------------------------------ host --
 size_t round256(size_t b) { return (b + 255) / 256 * 256; }
 size_t vec_stride(int n) { return ((size_t)n + 31) / 32 * 32; }  // doubles
 int chunks_of(int n) { return (n + kChunkRows - 1) / kChunkRows; }
 
+// Sizes of a slot's canonical-order reduction buffers.
+struct FoldSizes {
+  int ns, ng, nr, ld, ldr;
+};
+FoldSizes fold_sizes(int n) {
+  FoldSizes z;
+  z.ns = (n + kSlice - 1) / kSlice;
+  z.ng = (z.ns + kGroupSlices - 1) / kGroupSlices;
+  z.nr = (z.ng + kFoldRange - 1) / kFoldRange;
+  z.ld = (z.ns + 31) / 32 * 32;
+  z.ldr = (z.nr + 31) / 32 * 32;
+  return z;
+}
+
 // Device bytes of one request's vectors: 11 FP64 vectors, the apply
-// intermediate and the chunk partials.
+// intermediate (<= 8 B per row), and the slice and range sums of 3 dots.
 size_t request_bytes(int n) {
   const size_t st = vec_stride(n) * sizeof(double);
-  return round256(kNumVec * st + st + 3 * sizeof(double) * (size_t)chunks_of(n));  // t: <= 8 B/row
+  const FoldSizes z = fold_sizes(n);
+  return round256((kNumVec + 1) * st + 3 * sizeof(double) * ((size_t)z.ld + (size_t)z.ldr));
 }
 
 // First-fit allocator over the server's device arena (offsets only).
@@ -676,7 +950,90 @@ class Arena {
 struct Operator {
   const ainv_csr *a = nullptr;
   const ainv_handle *h = nullptr;
+  // streamed operator kernels: layout and shared memory per kind, and
+  // which kinds stream (bit k)
+  StreamLayout L[kNumSk] = {};
+  size_t smem[kNumSk] = {0, 0, 0, 0};
+  unsigned smask = 0;
 };
+
+// The operator's streamed kinds: those whose matrix the streaming layout
+// takes (stream_plan) and whose kernel variant exists.  AINV_SERVER_STREAM=0
+// runs every kind chunk-walked (for comparison).
+void plan_operator(Operator &op) {
+  static const bool off = [] {
+    const char *e = std::getenv("AINV_SERVER_STREAM");
+    return e && e[0] == '0';
+  }();
+  const ainv_handle *h = op.h;
+  const int tsz = (h->prec == AINV_PREC_FP32 || h->prec == AINV_PREC_BF16) ? 4 : 8;
+  const struct {
+    const DevSell *m;
+    int xs, nrv;
+  } k[kNumSk] = {{&h->wt, 8, 1}, {&h->z, tsz, 0}, {&op.a->a, 8, 1}, {&op.a->a, 8, 3}};
+  op.smask = 0;
+  for (int q = 0; q < kNumSk && !off; q++) {
+    StreamLayout L;
+    size_t smem = 0;
+    if (stream_plan(*k[q].m, k[q].xs, k[q].nrv, L, smem) <= 0) continue;
+    const int prec = k[q].m->prec, pack = k[q].m->pack;
+    void *kern = q == kSkSweep1   ? sweep_kernel<1>(prec, pack)
+                 : q == kSkSweep2 ? sweep_kernel<2>(prec, pack)
+                 : q == kSkSpmv   ? spmv_kernel<kBicgSigma>(pack)
+                                  : spmv_kernel<kTrueRes>(pack);
+    if (!kern || (q >= kSkSpmv && prec != AINV_PREC_FP64)) continue;
+    op.L[q] = L;
+    op.smem[q] = smem;
+    op.smask |= 1u << q;
+  }
+}
+
+// Union of the registered operators' launch needs.
+LaunchPlan make_plan(const std::vector<Operator> &ops) {
+  LaunchPlan lp;
+  auto add = [](auto &v, auto x) {
+    if (std::find(v.begin(), v.end(), x) == v.end()) v.push_back(x);
+  };
+  for (const Operator &op : ops) {
+    const int fam = acc64_prec(op.h->prec) ? kFamAcc64 : kFamStd;
+    for (int q = 0; q < kNumSk; q++) {
+      const bool st = (op.smask >> q) & 1u;
+      if (st) lp.smem[q] = std::max(lp.smem[q], op.smem[q]);
+      switch (q) {
+        case kSkSweep1:
+          if (st) add(lp.sw1, std::make_pair(op.h->wt.prec, op.h->wt.pack));
+          else lp.fb_sweep1 |= fam;
+          break;
+        case kSkSweep2:
+          if (st) add(lp.sw2, std::make_pair(op.h->z.prec, op.h->z.pack));
+          else lp.fb_sweep2 |= fam;
+          break;
+        case kSkSpmv:
+          if (st) add(lp.spmv, op.a->a.pack);
+          else lp.fb_spmv = true;
+          break;
+        default:
+          if (st) add(lp.strue, op.a->a.pack);
+          else lp.fb_true = true;
+          break;
+      }
+    }
+  }
+  return lp;
+}
+
+// Allow every streamed kernel of the plan its shared memory.
+bool plan_smem(const LaunchPlan &lp) {
+  bool ok = true;
+  for (const auto &v : lp.sw1) ok = ok && set_smem_attr(sweep_kernel<1>(v.first, v.second), lp.smem[kSkSweep1]);
+  for (const auto &v : lp.sw2) ok = ok && set_smem_attr(sweep_kernel<2>(v.first, v.second), lp.smem[kSkSweep2]);
+  for (int pk : lp.spmv) {
+    ok = ok && set_smem_attr(spmv_kernel<kBicgSigma>(pk), lp.smem[kSkSpmv]);
+    ok = ok && set_smem_attr(spmv_kernel<kBicgOmega>(pk), lp.smem[kSkSpmv]);
+  }
+  for (int pk : lp.strue) ok = ok && set_smem_attr(spmv_kernel<kTrueRes>(pk), lp.smem[kSkTrue]);
+  return ok;
+}
 
 struct Request {
   long long id = 0;
@@ -707,7 +1064,8 @@ struct ainv_server {
   cudaGraphExec_t exec = nullptr;
   ainv::srv::Table *tab_d = nullptr, *tab_h = nullptr;
   ainv::srv::Table *tab_empty_d = nullptr;  // all blocks idle: settles new kernels
-  int fam = 0, graph_fam = 0;               // kernel families registered / in the graph
+  ainv::srv::LaunchPlan plan, graph_plan;   // launches the operators need / in the graph
+  int graph_kernels = 0;                    // kernel launches per graph launch
   ainv::srv::SlotState *st_d = nullptr, *st_h = nullptr;
   char *arena_d = nullptr;
   ainv::srv::Arena arena;
@@ -736,21 +1094,24 @@ namespace ainv {
 namespace srv {
 namespace {
 
-// Capture (or re-capture) the step graph for the kernel families `fam`: the
-// init kernel and `iters` batched iterations.  Every kernel of the graph is
+// Capture (or re-capture) the step graph for the launch plan `lp`: the
+// init kernels and `iters` batched iterations.  Every kernel of the graph is
 // first launched once on an all-idle table, so nothing loads during capture
 // and no admitted request is advanced.
-cudaError_t capture_graph(ainv_server *srv, int fam) {
-  k_srv_init<<<srv->grid, kBlock, 0, srv->s>>>(srv->tab_empty_d, srv->st_d);
-  cudaError_t e = enqueue_iteration(srv->tab_empty_d, srv->st_d, srv->grid, srv->s, fam);
+cudaError_t capture_graph(ainv_server *srv, const LaunchPlan &lp) {
+  if (!plan_smem(lp)) return cudaErrorInvalidConfiguration;
+  int count = 0;
+  enqueue_init(srv->tab_empty_d, srv->st_d, srv->grid, srv->s, &count);
+  cudaError_t e = enqueue_iteration(srv->tab_empty_d, srv->st_d, srv->grid, srv->s, lp, &count);
   if (e == cudaSuccess) e = cudaStreamSynchronize(srv->s);
   if (e != cudaSuccess) return e;
   e = cudaStreamBeginCapture(srv->s, cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) return e;
-  k_srv_init<<<srv->grid, kBlock, 0, srv->s>>>(srv->tab_d, srv->st_d);
+  count = 0;
+  enqueue_init(srv->tab_d, srv->st_d, srv->grid, srv->s, &count);
   cudaError_t ce = cudaGetLastError();
   for (int k = 0; k < srv->iters && ce == cudaSuccess; k++)
-    ce = enqueue_iteration(srv->tab_d, srv->st_d, srv->grid, srv->s, fam);
+    ce = enqueue_iteration(srv->tab_d, srv->st_d, srv->grid, srv->s, lp, &count);
   cudaGraph_t g = nullptr;
   e = cudaStreamEndCapture(srv->s, &g);
   if (ce != cudaSuccess || e != cudaSuccess) {
@@ -763,7 +1124,8 @@ cudaError_t capture_graph(ainv_server *srv, int fam) {
   if (e != cudaSuccess) return e;
   if (srv->exec) cudaGraphExecDestroy(srv->exec);
   srv->exec = exec;
-  srv->graph_fam = fam;
+  srv->graph_plan = lp;
+  srv->graph_kernels = count;
   return cudaSuccess;
 }
 
@@ -795,6 +1157,28 @@ int plan_weighted(int nslots, const long long *weight, const int *cap, int grid,
   }
   int at = 0;
   for (int k = 0; k < nslots; k++) {
+    b0[k] = at;
+    at += nb[k];
+  }
+  return AINV_SUCCESS;
+}
+
+// Streamed operator kernels: group k gets minb[k] blocks (its members) plus a
+// share of the rest in proportion to weight[k]; contiguous ranges.
+int plan_stream(int ng, const long long *weight, const int *minb, int grid, int *b0, int *nb) {
+  long long total = 0;
+  int fixed = 0;
+  for (int k = 0; k < ng; k++) {
+    total += std::max(1LL, weight[k]);
+    fixed += minb[k];
+  }
+  if (fixed > grid) {
+    set_error("server stream plan: %d members for a grid of %d blocks", fixed, grid);
+    return AINV_ERR_ARG;
+  }
+  int at = 0;
+  for (int k = 0; k < ng; k++) {
+    nb[k] = minb[k] + (int)((long long)(grid - fixed) * std::max(1LL, weight[k]) / std::max(1LL, total));
     b0[k] = at;
     at += nb[k];
   }
@@ -848,11 +1232,20 @@ void fill_slot(ainv_server *srv, int k, const Request *r, size_t off) {
   d.wt = mat_of(op.h->wt);
   d.z = mat_of(op.h->z);
   d.d = op.h->d;
+  for (int q = 0; q < kNumSk; q++) d.L[q] = op.L[q];
+  d.smask = op.smask;
   const size_t st = vec_stride(r->n);
   double *base = reinterpret_cast<double *>(srv->arena_d + off);
   for (int v = 0; v < kNumVec; v++) d.vec[v] = base + (size_t)v * st;
   d.t = base + (size_t)kNumVec * st;
-  d.partials = base + (size_t)(kNumVec + 1) * st;
+  const FoldSizes z = fold_sizes(r->n);
+  d.ns = z.ns;
+  d.ng = z.ng;
+  d.nr = z.nr;
+  d.ld = z.ld;
+  d.ldr = z.ldr;
+  d.sp = base + (size_t)(kNumVec + 1) * st;
+  d.rs = d.sp + 3 * (size_t)z.ld;
   SlotState &s = srv->st_h[k];
   std::memset(&s, 0, sizeof(s));
   s.k.eps = r->eps;
@@ -954,16 +1347,30 @@ void engine_loop(ainv_server *srv) {
         gd.nb = gnb[(size_t)g];
         for (int b = gd.b0; b < gd.b0 + gd.nb; b++) srv->tab_h->block_group[b] = (short)g;
       }
+      // the streamed grid: at least one block per member
+      for (int g = 0; g < ng; g++) gcap[(size_t)g] = srv->tab_h->group[g].nmem;
+      if (plan_stream(ng, gw.data(), gcap.data(), stream_grid(), gb0.data(), gnb.data()) !=
+          AINV_SUCCESS) {
+        fail_all(srv, AINV_ERR_INTERNAL, "server stream plan failed");
+        return;
+      }
+      std::fill(srv->tab_h->block_group_s, srv->tab_h->block_group_s + kMaxGrid, (short)-1);
+      for (int g = 0; g < ng; g++) {
+        GroupDesc &gd = srv->tab_h->group[g];
+        gd.bs0 = gb0[(size_t)g];
+        gd.nbs = gnb[(size_t)g];
+        for (int b = gd.bs0; b < gd.bs0 + gd.nbs; b++) srv->tab_h->block_group_s[b] = (short)g;
+      }
       ENG_TRY(cudaMemcpyAsync(srv->tab_d, srv->tab_h, sizeof(Table), cudaMemcpyHostToDevice,
                               srv->s));
       dirty = false;
     }
-    int fam;
+    LaunchPlan lp;
     {
       std::lock_guard<std::mutex> lk(srv->mu);
-      fam = srv->fam;
+      lp = srv->plan;
     }
-    if (fam != 0 && fam != srv->graph_fam) ENG_TRY(capture_graph(srv, fam));  // new family
+    if (!(lp == srv->graph_plan)) ENG_TRY(capture_graph(srv, lp));  // new operator kinds
     ENG_TRY(cudaGraphLaunch(srv->exec, srv->s));
     ENG_TRY(cudaMemcpyAsync(srv->st_h, srv->st_d, sizeof(SlotState) * (size_t)S,
                             cudaMemcpyDeviceToHost, srv->s));
@@ -972,7 +1379,8 @@ void engine_loop(ainv_server *srv) {
     std::vector<int> done;
     for (int k = 0; k < S; k++) {
       const SlotHost &sl = srv->slots[(size_t)k];
-      if (sl.req && srv->st_h[k].phase == kRun && srv->st_h[k].k.done) {
+      // finished, or a streamed kernel gave up a bounded wait for it
+      if (sl.req && ((srv->st_h[k].phase == kRun && srv->st_h[k].k.done) || srv->st_h[k].k.timeout)) {
         done.push_back(k);
         ENG_TRY(cudaMemcpyAsync(sl.req->x, srv->tab_h->slot[k].vec[VX],
                                 sizeof(double) * (size_t)sl.req->n, cudaMemcpyDeviceToHost,
@@ -990,7 +1398,7 @@ void engine_loop(ainv_server *srv) {
         Request *r = sl.req;
         r->iter = f.iter;
         r->err = sqrt(f.rn2) / f.bn2;
-        r->status = f.status;
+        r->status = f.timeout ? AINV_ERR_TIMEOUT : f.status;
         r->t_done = t;
         r->complete = true;
         srv->arena.release(sl.off, r->bytes);
@@ -1086,6 +1494,7 @@ int ainv_server_create(ainv_server **out, int max_slots, size_t hbm_bytes, int i
   std::memset(srv->tab_h, 0, sizeof(Table));
   std::fill(srv->tab_h->block_slot, srv->tab_h->block_slot + kMaxGrid, (short)-1);
   std::fill(srv->tab_h->block_group, srv->tab_h->block_group + kMaxGrid, (short)-1);
+  std::fill(srv->tab_h->block_group_s, srv->tab_h->block_group_s + kMaxGrid, (short)-1);
   std::memset(srv->st_h, 0, sizeof(SlotState) * (size_t)max_slots);
   e = cudaMemcpy(srv->tab_d, srv->tab_h, sizeof(Table), cudaMemcpyHostToDevice);
   if (e == cudaSuccess)
@@ -1095,7 +1504,7 @@ int ainv_server_create(ainv_server **out, int max_slots, size_t hbm_bytes, int i
   if ((e = cudaMalloc(&srv->tab_empty_d, sizeof(Table))) != cudaSuccess) return fail(e, "table");
   e = cudaMemcpy(srv->tab_empty_d, srv->tab_h, sizeof(Table), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return fail(e, "empty table");
-  if ((e = capture_graph(srv, kFamStd)) != cudaSuccess) return fail(e, "graph capture");
+  if ((e = capture_graph(srv, LaunchPlan{})) != cudaSuccess) return fail(e, "graph capture");
   srv->running = true;
   srv->engine = std::thread(engine_loop, srv);
   *out = srv;
@@ -1112,9 +1521,13 @@ int ainv_server_add_operator(ainv_server *srv, const ainv_csr *a, const ainv_han
     ainv::set_error("ainv_server_add_operator: operator size %d, factor size %d", a->n, h->n);
     return AINV_ERR_ARG;
   }
+  ainv::srv::Operator o;
+  o.a = a;
+  o.h = h;
+  ainv::srv::plan_operator(o);
   std::lock_guard<std::mutex> lk(srv->mu);
-  srv->fam |= ainv::srv::acc64_prec(h->prec) ? ainv::srv::kFamAcc64 : ainv::srv::kFamStd;
-  srv->ops.push_back(ainv::srv::Operator{a, h});
+  srv->ops.push_back(o);
+  srv->plan = ainv::srv::make_plan(srv->ops);
   *op = (int)srv->ops.size() - 1;
   return AINV_SUCCESS;
 }
@@ -1220,9 +1633,7 @@ int ainv_server_stats(ainv_server *srv, ainv_server_info *out) {
   out->submitted = srv->submitted;
   out->completed = srv->completed;
   out->graph_launches = srv->launches;
-  out->kernel_launches = srv->launches *
-      (1 + (long long)srv->iters *
-               (ainv::srv::kLaunchesPerIteration + (srv->graph_fam == 3 ? 4 : 0)));
+  out->kernel_launches = srv->launches * (long long)srv->graph_kernels;
   out->active = srv->active;
   out->queued = (int)srv->queue.size();
   out->peak_active = srv->peak_active;

@@ -2,7 +2,9 @@
 // asynchronous copies (cp.async.bulk, the TMA engine's linear mode) so the
 // bytes in flight do not occupy registers.
 //
-// Each block walks stages blockIdx.x, blockIdx.x + gridDim.x, ...  A stage
+// Each block walks stages j0, j0 + stride, ... (by default blockIdx.x and
+// gridDim.x; a caller that splits the grid among several vectors passes
+// its own walk).  A stage
 // (StageDesc) is m.stage_slices consecutive slices.  Its buffer receives, by
 // bulk copies: the descriptor, the stage's chunks of the slice pointers,
 // its values, its index words and -- for uniform stages, whose slices share
@@ -172,6 +174,22 @@ struct StagedRows {
     return reinterpret_cast<const T *>(p[i])[row];
   }
 };
+
+// Accumulation-type value of a staged operand element.
+template <class V>
+__device__ __forceinline__ typename Acc<V>::type to_acc(V v) { return v; }
+template <>
+__device__ __forceinline__ double to_acc<f32w>(f32w v) {
+  return (double)v.v;
+}
+template <>
+__device__ __forceinline__ double to_acc<b16w>(b16w v) {
+  return (double)__uint_as_float(((unsigned)v.v) << 16);
+}
+template <>
+__device__ __forceinline__ float to_acc<__nv_bfloat16>(__nv_bfloat16 v) {
+  return __uint_as_float(((unsigned)__bfloat16_as_ushort(v)) << 16);
+}
 
 // Element t of a small register array selected by a runtime index without
 // dynamic indexing (which would move the array to local memory).
@@ -486,21 +504,27 @@ __device__ __forceinline__ void slice_end(E &e, int s) { slice_end_impl(e, s, 0)
 // epi.post(r, acc, rows) with acc = (M x)[r] and `rows` the reader of the
 // staged row operands epi.row_vecs().  Must be called by all kStreamThreads
 // threads; the last warp produces, the others consume.  RMAX bounds L.R
-// (slices per consumer warp and stage).  Returns false (and sets *status)
-// if a wait ran past its limit.
+// (slices per consumer warp and stage).  The block takes stages j0,
+// j0 + jstride, ... (j0 < 0: blockIdx.x and gridDim.x).  Returns false (and
+// sets *status) if a wait ran past its limit.
 template <int P, int RMAX, class V, class X, class Epi>
 __device__ __forceinline__ bool stream_rows(const SellView<V> &m,
                                             const StageDesc *__restrict__ stages, int nstages,
                                             const X *__restrict__ x, const StreamLayout &L,
-                                            Epi &epi, int *status) {
+                                            Epi &epi, int *status, int j0 = -1,
+                                            int jstride = 0) {
   const RowVecs rv = epi.row_vecs();
   extern __shared__ __align__(128) unsigned char smem[];
   unsigned long long *full = reinterpret_cast<unsigned long long *>(smem);
   unsigned long long *empty = full + 8;
   unsigned char *base = smem + 128;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int G = gridDim.x;
-  const int mine = ((int)blockIdx.x < nstages) ? (nstages - (int)blockIdx.x + G - 1) / G : 0;
+  if (j0 < 0) {
+    j0 = (int)blockIdx.x;
+    jstride = (int)gridDim.x;
+  }
+  const int G = jstride;
+  const int mine = (j0 < nstages) ? (nstages - j0 + G - 1) / G : 0;
   const int stage_slices = kConsumerWarps * L.R;
   if (tid == 0) {
     for (int b = 0; b < L.D; b++) {
@@ -519,7 +543,7 @@ __device__ __forceinline__ bool stream_rows(const SellView<V> &m,
       int4 q0 = make_int4(0, 0, 0, 0), q1 = q0, q2 = q0, q3 = q0;
       const int jl = jb + lane;
       if (jl < mine) {
-        const int4 *src = reinterpret_cast<const int4 *>(stages + blockIdx.x + jl * G);
+        const int4 *src = reinterpret_cast<const int4 *>(stages + j0 + jl * G);
         q0 = __ldg(src);
         q1 = __ldg(src + 1);
         q2 = __ldg(src + 2);
@@ -538,7 +562,7 @@ __device__ __forceinline__ bool stream_rows(const SellView<V> &m,
           ok = false;
           break;
         }
-        issue_stage(m, stages, blockIdx.x + j * G, d, x, rv, L, base + (size_t)b * L.stage,
+        issue_stage(m, stages, j0 + j * G, d, x, rv, L, base + (size_t)b * L.stage,
                     &full[b]);
         j++;
       }
@@ -594,6 +618,35 @@ __device__ __forceinline__ bool stream_rows(const SellView<V> &m,
   __syncthreads();
   return ok;
 }
+
+// Epilogues of the apply's two sweeps: t = D^-1 .* acc (D staged as a row
+// operand) and y = alpha*acc + beta*y (y staged when beta != 0).
+template <class V, class T>
+struct EpiDscale {
+  const V *__restrict__ d;
+  T *__restrict__ t;
+  static constexpr int kRowVecs = 1;
+  __device__ __forceinline__ RowVecs row_vecs() const {
+    return RowVecs{{d, nullptr, nullptr}, {(int)sizeof(V), 0, 0}};
+  }
+  template <class A>
+  __device__ __forceinline__ void post(int row, A acc, const StagedRows &r) const {
+    t[row] = (T)(to_acc(r.get<V>(0, row)) * acc);
+  }
+};
+
+struct EpiAxpby {
+  double alpha, beta;
+  double *__restrict__ y;
+  static constexpr int kRowVecs = 1;
+  __device__ __forceinline__ RowVecs row_vecs() const {
+    return RowVecs{{beta == 0.0 ? nullptr : y, nullptr, nullptr}, {8, 0, 0}};
+  }
+  template <class A>
+  __device__ __forceinline__ void post(int row, A acc, const StagedRows &r) const {
+    y[row] = axpby_row(alpha, (double)acc, beta, beta == 0.0 ? 0.0 : r.get<double>(0, row));
+  }
+};
 
 // Shared-memory budgets (bytes): one stage buffer at most, per block target,
 // per block maximum (opt-in carve-out) and per SM.

@@ -1,14 +1,15 @@
 """Solve server on the GPU: continuous batching of BiCGSTAB solves against
 resident operators, through the ainv_server_* C-ABI.
 
-The central property: a request's result is the same alone and in a mix.
-The server's reductions are folded over fixed row chunks, so the iterates
-do not depend on the other requests, on how many blocks a request gets or
-on how many iterations a graph launch runs; the test asserts bit-identical
-solutions and iteration counts.  Converged results meet the FP64 relative
-residual on b - A x (tolerance 1e-8, as the serving workload asks), and
-with FP64 factors the iteration counts sit inside the oracle's
-rounding-level spread (+-5%).
+The central properties: a request's result is the same alone and in a mix,
+and it is the single-solve result.  The server sums every dot in the
+canonical order of the single-solve loop (slice sums folded in fixed
+groups and ranges), and its operator kernels compute each member's rows
+with the single-solve arithmetic, so the iterates depend neither on the
+other requests nor on the blocks a request gets: the tests assert
+bit-identical solutions and iteration counts, against a request's solo run
+and against ainv_gpu_solve.  Converged results meet the FP64 relative
+residual on b - A x (tolerance 1e-8, as the serving workload asks).
 """
 import numpy as np
 import pytest
@@ -202,3 +203,75 @@ def test_requests_on_one_operator_share_reads():
         assert r1[j].converged and r2[j].converged
         assert r1[j].iter == r2[j].iter and np.array_equal(x1[j], x2[j]), j
         assert _true_relres(ops[k]["csr"], x2[j], b) <= 1.05 * EPS
+
+
+@pytest.mark.parametrize("prec", ["FP64", "FP32_ACC64", "FP32", "BF16"])
+def test_served_equals_single_solve(prec):
+    """Six concurrent requests on two operators (groups of members that share
+    the operator's streamed reads): each solution and iteration count equals
+    ainv_gpu_solve's on the same right-hand side, bit for bit."""
+    ops = _operators(prec)[1:3]
+    reqs = _requests(ops, 6)
+    xs, res, st = _run(ops, reqs, max_slots=6, iters=3)
+    assert st["peak_active"] == 6
+    for j, (k, b) in enumerate(reqs):
+        bd = torch.tensor(b, device="cuda")
+        xd = torch.zeros_like(bd)
+        r = ops[k]["a"].solve(bd, xd, ops[k]["f"], eps=EPS, itmax=2000)
+        assert res[j].converged and r.info == 0
+        assert res[j].iter == r.iter, (j, res[j].iter, r.iter)
+        assert np.array_equal(xs[j], xd.cpu().numpy()), j
+
+
+def test_served_fp64_equals_oracle():
+    """With FP64 factors a served request's iterates are the oracle's
+    ordered-dot BiCGSTAB iterates: same count, same solution bits."""
+    ops = _operators("FP64")[1:2]
+    reqs = _requests(ops, 3)
+    xs, res, _ = _run(ops, reqs, max_slots=3, iters=4)
+    for j, (k, b) in enumerate(reqs):
+        x, it, err, rc = O.solve("BICGSTAB", ops[k]["csr"], oracle_factors(ops[k]["fac"]), b,
+                                 eps=EPS, itmax=2000, order="device")
+        assert rc == 0 and res[j].iter == it, (j, res[j].iter, it)
+        assert np.array_equal(xs[j], x), j
+
+
+_CHUNK_SCRIPT = """
+import sys, numpy as np, torch
+sys.path[:0] = {paths!r}
+import ainv
+from ainv import serve, workload
+from util import build_factors, device_factors
+irp, ja, val = ainv.pde.gen_pde3d(17, "convdiff", (8.0, -3.0, 5.0))
+f = build_factors(irp, ja, val)
+a = ainv.DeviceOperator(irp, ja, val)
+fd = device_factors(f, "FP32_ACC64")
+out = []
+with serve.SolveServer(max_slots=3, iters_per_launch=2) as srv:
+    op = srv.add_operator(a, fd)
+    bs = [workload.request_rhs(1000 + j, a.n) for j in range(3)]
+    xs = [np.zeros(a.n) for _ in bs]
+    ids = [srv.submit(op, b, x, 1e-8, 2000) for b, x in zip(bs, xs)]
+    res = [srv.wait(i) for i in ids]
+for b, x, r in zip(bs, xs, res):
+    bd = torch.tensor(b, device="cuda"); xd = torch.zeros_like(bd)
+    s = a.solve(bd, xd, fd, eps=1e-8, itmax=2000)
+    assert r.converged and r.iter == s.iter, (r.iter, s.iter)
+    assert np.array_equal(x, xd.cpu().numpy())
+print("OK")
+"""
+
+
+def test_chunk_walked_operator_kernels_equal_single_solve():
+    """With streaming switched off (AINV_SERVER_STREAM=0) the server's
+    chunk-walking operator kernels run instead and give the same bits."""
+    import os
+    import subprocess
+    import sys
+    here = os.path.dirname(os.path.abspath(__file__))
+    root = os.path.dirname(here)
+    paths = [here, root, os.path.join(root, "oracle"), os.path.join(root, "mld-ainv_b200")]
+    env = dict(os.environ, AINV_SERVER_STREAM="0")
+    out = subprocess.run([sys.executable, "-c", _CHUNK_SCRIPT.format(paths=paths)],
+                         env=env, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0 and "OK" in out.stdout, out.stderr[-3000:]
