@@ -72,10 +72,14 @@ constexpr int kMaxOffsets = 64;  // offset mode only for slices with <= 64 offse
 // words and, for uniform stages, the windows of the gathered vector.  A
 // stage is "uniform" when all its slices use offset mode with one identical
 // offset list of at most kStageMaxOffsets entries; its gathers then read
-// contiguous windows x[r0+o, r1+o) that are copied too.  Built on the host at
-// upload; consumed by the streaming kernels.
+// contiguous windows x[r0+o, r1+o) that are copied too.  Offsets (sorted)
+// within kWindowSpan elements of their cluster's first offset share one
+// window, x[r0+o_first, r1+o_last): a new cluster starts at the first offset
+// more than kWindowSpan past the current cluster's first offset.  Built on
+// the host at upload; consumed by the streaming kernels.
 constexpr int kConsumerSlices = 8;   // consumer warps per streaming block
 constexpr int kStageMaxOffsets = 8;
+constexpr int kWindowSpan = 16;
 constexpr int kMaxStageSlices = 32;
 struct alignas(16) StageDesc {
   int s0, s1;          // slice range [s0, s1)
@@ -83,7 +87,8 @@ struct alignas(16) StageDesc {
   int vbytes;          // value bytes (multiple of 16)
   long long ibyte0;    // first index byte copied (16-aligned)
   int ibytes;          // index bytes copied (multiple of 16)
-  int noff;            // uniform: number of offsets, else 0
+  int noff;            // uniform: number of offsets (bits 0-7, else 0) and the
+                       // offsets that start a window cluster (bit 8 + k)
   int off[kStageMaxOffsets];
 };
 static_assert(sizeof(StageDesc) == 64, "stage descriptor is one 64-byte copy");
@@ -105,6 +110,7 @@ struct DevSell {
   int nstages = 0;
   int stage_slices = 0;
   int stage_vmax = 0, stage_imax = 0, stage_noff_max = 0;
+  int stage_nwin_max = 0;  // windows (offset clusters) of a uniform stage
   StageDesc *stages = nullptr;
   // host copy: the largest column each slice reads (-1 for an empty slice);
   // a sweep over rows of a slice range needs its input only up to there

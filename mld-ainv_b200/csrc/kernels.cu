@@ -193,11 +193,12 @@ int stream_plan(const DevSell &m, int xs, int nrv, StreamLayout &L, size_t &smem
   L.R = m.stage_slices / kConsumerWarps;
   L.vb = r128(m.stage_vmax);
   L.ib = r128(m.stage_imax);
-  L.xw = (int)(((long long)m.stage_slices * kSlice * xs + 32 + 15) / 16 * 16);
-  L.noff = m.stage_noff_max;
+  // a window: the stage's rows, its offset cluster's span and granule slack
+  L.xw = (int)(((long long)(m.stage_slices * kSlice + kWindowSpan) * xs + 32 + 15) / 16 * 16);
+  L.nwin = m.stage_nwin_max;
   L.nrv = std::max(0, std::min(kMaxRowVecs, nrv));
   L.rw = (int)(((long long)m.stage_slices * kSlice * 8 + 15) / 16 * 16);
-  L.stage = r128((long long)kHeaderBytes + L.vb + L.ib + (long long)L.noff * L.xw +
+  L.stage = r128((long long)kHeaderBytes + L.vb + L.ib + (long long)L.nwin * L.xw +
                  (long long)L.nrv * L.rw);
   if (L.stage > kStreamStageMax) return 0;
   // shared memory per block (tunable: AINV_STREAM_SMEM_KB); a smaller budget

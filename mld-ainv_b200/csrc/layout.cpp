@@ -285,10 +285,19 @@ int upload_sell_t(const HostCsr &a, int prec, DevSell &out) {
       if (uni) {
         d.noff = u0;
         for (int k = 0; k < u0; k++) d.off[k] = o0[k];
+        // windows: clusters of offsets within kWindowSpan of their first
+        int nwin = 0, first = 0;
+        for (int k = 0; k < u0; k++)
+          if (k == 0 || o0[k] - first > kWindowSpan) {
+            nwin++;
+            first = o0[k];
+            d.noff |= 1 << (8 + k);
+          }
+        m.stage_nwin_max = std::max(m.stage_nwin_max, nwin);
       }
       m.stage_vmax = std::max(m.stage_vmax, d.vbytes);
       m.stage_imax = std::max(m.stage_imax, d.ibytes);
-      m.stage_noff_max = std::max(m.stage_noff_max, d.noff);
+      m.stage_noff_max = std::max(m.stage_noff_max, d.noff & 0xff);
     }
     m.nstages = nst;
     m.stage_slices = stage_slices;

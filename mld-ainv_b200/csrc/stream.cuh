@@ -111,14 +111,14 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned pari
 __device__ __forceinline__ int granule(int es) { return 16 / es; }
 
 // Shared-memory arrangement of one launch (bytes; computed on the host).
-// Buffer: [header | values (vb) | index words (ib) | noff windows of xw |
+// Buffer: [header | values (vb) | index words (ib) | nwin windows of xw |
 //          nrv row-operand areas of rw].
 struct StreamLayout {
   int D;      // stage buffers
   int vb;     // value area per buffer
   int ib;     // index area per buffer
   int xw;     // one gathered-vector window
-  int noff;   // windows per buffer
+  int nwin;   // windows per buffer (offset clusters)
   int rw;     // one row-operand area (the stage's rows of an epilogue vector)
   int nrv;    // row-operand areas per buffer
   int stage;  // bytes per buffer
@@ -282,12 +282,14 @@ struct SPack<b16w, P> {
   }
 };
 
-// Element range [a, e) of the window of offset o for rows [r0, r1) of an
-// n-element vector: the rows' columns, widened to whole 16-byte granules.
+// Element range [a, e) of the window of an offset cluster [o0, o1] for rows
+// [r0, r1) of an n-element vector: the rows' columns, widened to whole
+// 16-byte granules.
 template <class X>
-__device__ __forceinline__ void window_range(int r0, int r1, int o, int n, int &a, int &e) {
+__device__ __forceinline__ void window_range(int r0, int r1, int o0, int o1, int n, int &a,
+                                             int &e) {
   const int g = granule((int)sizeof(X));
-  int lo = r0 + o, hi = r1 + o;
+  int lo = r0 + o0, hi = r1 + o1;
   lo = lo < 0 ? 0 : lo;
   hi = hi > n ? n : hi;
   a = lo & ~(g - 1);
@@ -329,16 +331,28 @@ __device__ __forceinline__ void issue_stage(const SellView<V> &m,
     dst = buf + kHeaderBytes + L.vb;
     bytes = d.ibytes;
   } else if (lane < 5 + kStageMaxOffsets) {
+    // offset k's window cluster c (first offset o0, last o1); the cluster's
+    // first offset copies the window into area c
     const int k = lane - 5;
+    const int noff = d.noff & 0xff;
     int wofs = -r0;
-    if (k < d.noff) {
+    if (k < noff) {
+      // cluster leaders (bit q: offset q starts a cluster); k's cluster runs
+      // from the last leader <= k to before the next leader
+      const unsigned lead = ((unsigned)d.noff >> 8) & 0xffu;
+      const unsigned upto = lead & ((2u << k) - 1u);
+      const int kc = __popc(upto) - 1, k0 = 31 - __clz(upto);
+      const unsigned after = lead & ~((2u << k) - 1u);
+      const int k1 = after ? __ffs(after) - 2 : noff - 1;
+      const int o = pick(d.off, k), o0 = pick(d.off, k0), o1 = pick(d.off, k1);
       int a, e;
-      const int o = pick(d.off, k);
-      window_range<X>(r0, r1, o, m.n, a, e);
-      src = reinterpret_cast<const unsigned char *>(x + a);
-      dst = buf + kHeaderBytes + L.vb + L.ib + k * L.xw;
-      bytes = (e - a) * (int)sizeof(X);
-      wofs = k * (L.xw / (int)sizeof(X)) + o - a;
+      window_range<X>(r0, r1, o0, o1, m.n, a, e);
+      if (k == k0) {
+        src = reinterpret_cast<const unsigned char *>(x + a);
+        dst = buf + kHeaderBytes + L.vb + L.ib + kc * L.xw;
+        bytes = (e - a) * (int)sizeof(X);
+      }
+      wofs = kc * (L.xw / (int)sizeof(X)) + o - a;
     }
     dv->wofs[k] = wofs;
   } else if (lane < 5 + kStageMaxOffsets + kMaxRowVecs) {
@@ -349,7 +363,7 @@ __device__ __forceinline__ void issue_stage(const SellView<V> &m,
     if (i < L.nrv && p) {
       const int ce = row_copy_end(r0, r1, m.n, es);
       src = reinterpret_cast<const unsigned char *>(p) + (size_t)r0 * es;
-      dst = buf + kHeaderBytes + L.vb + L.ib + L.noff * L.xw + i * L.rw;
+      dst = buf + kHeaderBytes + L.vb + L.ib + L.nwin * L.xw + i * L.rw;
       bytes = (ce - r0) * es;
       nrows = ce - r0;
     }
@@ -401,7 +415,7 @@ struct UniformStage {
 };
 __device__ __forceinline__ void uniform_stage(const StageDesc &d, const StageDerived &dv,
                                               UniformStage &u) {
-  u.noff = d.noff;
+  u.noff = d.noff & 0xff;
   static_assert(kStageMaxOffsets == 8, "the offsets' shifts are read as two 16-byte words");
   const int4 a = *reinterpret_cast<const int4 *>(dv.wofs);
   const int4 b = *reinterpret_cast<const int4 *>(dv.wofs + 4);
@@ -588,7 +602,7 @@ __device__ __forceinline__ bool stream_rows(const SellView<V> &m,
       UniformStage u;
       uniform_stage(d, dv, u);
       StagedRows sr;
-      sr.area = buf + kHeaderBytes + L.vb + L.ib + L.noff * L.xw;
+      sr.area = buf + kHeaderBytes + L.vb + L.ib + L.nwin * L.xw;
       sr.rw = L.rw;
       sr.r0 = d.s0 * kSlice;
       {
