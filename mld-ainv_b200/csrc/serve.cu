@@ -138,49 +138,163 @@ __device__ __forceinline__ SellView<V> sview(const Mat &m) {
   return SellView<V>{m.n, m.nslices, m.sptr, m.iptr, m.idx, (const V *)m.val};
 }
 
-// Rows of chunk c of M (warp w takes slice group 8c + w): epi(row, acc) for
-// its rows, then end(s) (whole warp) for each of its slices.  Values and
-// indices stay cached (a group's members read them in turn).
-template <class V, int P, class X, class Epi, class End>
-__device__ __forceinline__ void chunk_rows_p(const Mat &mm, int c, const X *__restrict__ x,
-                                             Epi &epi, End &end) {
-  const SellView<V> m = sview<V>(mm);
-  const int g = c * kWarps + (threadIdx.x >> 5);
-  const int ngroups = (m.nslices + kGroupS - 1) / kGroupS;
-  if (g >= ngroups) return;  // warp-uniform
-  GroupCtx<kGroupS> ctx;
-  group_ctx(m, g, ctx);
-  typename Acc<V>::type acc[kGroupS];
-  group_dot<P, 4, true, false>(m, ctx, g, x, acc);
+// The members' vector pointers an operator kernel needs (up to 5 each),
+// staged once per block in shared memory; the operator (A, W^T, Z, D^-1)
+// is the same for every member and is read from member 0.
+constexpr int kMemberVecs = 5;
+struct MemberVecs {
+  void *p[kMaxMembers][kMemberVecs];
+};
+
+// ---- slice-shared operator walk ------------------------------------------------
+// The group's blocks walk the operator's slices warp by warp (lane = row;
+// block lb takes slices 8 lb + warp, then every 8 nb-th).  A slice's
+// values and columns are loaded once into registers and each active
+// member's rows are computed from them, two members at a time, so a member
+// adds only its own gathers and epilogue.  Slots run in order with the
+// products of zero slots adding zero, as group_slots forms them, so every
+// member gets the single-solve row sums.  Slices wider than kShareSlots
+// slots reload their values for each member, kShareSlots at a time.
+// body(i, row, acc) runs for each member i (index into the group; its
+// gathered vector is mv.p[i][0]) and row < n; end(i, s) then runs with the
+// whole warp.  ml: the M active members (shared memory).
+constexpr int kShareSlots = 8;
+
+// Slots [k0, k0 + kShareSlots) of the lane's row of a slice into registers
+// (zeros past w): values, and columns (offset mode: row + offset).
+template <bool EF, int P, class V>
+__device__ __forceinline__ void share_load(const SellView<V> &m, int w, int vb, int ib, bool om,
+                                           int row, int k0,
+                                           typename Acc<V>::type (&vv)[kShareSlots / P][P],
+                                           int (&col)[kShareSlots / P][P]) {
+  using A = typename Acc<V>::type;
   const int lane = threadIdx.x & 31;
 #pragma unroll
-  for (int q = 0; q < kGroupS; q++) {
-    const int s = g * kGroupS + q;
-    if (s < m.nslices) {
-      const int row = s * kSlice + lane;
-      if (row < m.n) epi(row, acc[q]);
-      end(s);
+  for (int j = 0; j < kShareSlots / P; j++) {
+    const int k = k0 + j * P;
+    const size_t pos = (size_t)(k / P) * (kSlice * P) + (size_t)lane * P;
+    if (k < w) {
+      Pack<V, P>::template load<EF>(m.val + vb + pos, vv[j]);
+      if (om) {
+        load_ints<P, false>(m.idx + ib + k, col[j]);
+#pragma unroll
+        for (int e = 0; e < P; e++) col[j][e] += row;
+      } else {
+        load_ints<P, EF>(m.idx + ib + pos, col[j]);
+      }
+    } else {
+#pragma unroll
+      for (int e = 0; e < P; e++) {
+        vv[j][e] = A(0);
+        col[j][e] = 0;
+      }
     }
   }
 }
 
-template <class V, class X, class Epi, class End>
-__device__ __forceinline__ void chunk_rows(const Mat &m, int c, const X *__restrict__ x, Epi &epi,
-                                           End &end) {
+// acc += the loaded slots dotted with x, in slot order (zero slots add 0).
+template <int P, class A, class X>
+__device__ __forceinline__ void share_dot(int n, const A (&vv)[kShareSlots / P][P],
+                                          const int (&col)[kShareSlots / P][P],
+                                          const X *__restrict__ x, A &acc) {
+  A xv[kShareSlots / P][P];
+#pragma unroll
+  for (int j = 0; j < kShareSlots / P; j++)
+#pragma unroll
+    for (int e = 0; e < P; e++)
+      xv[j][e] = (vv[j][e] != A(0) && (unsigned)col[j][e] < (unsigned)n) ? (A)__ldg(x + col[j][e])
+                                                                         : A(0);
+#pragma unroll
+  for (int j = 0; j < kShareSlots / P; j++)
+#pragma unroll
+    for (int e = 0; e < P; e++) acc = madd(vv[j][e], xv[j][e], acc);
+}
+
+template <class V, int P, class X, class Body, class End>
+__device__ __forceinline__ void shared_slices(const Mat &mm, int lb, int nb, const int *ml, int M,
+                                              const MemberVecs &mv, Body &body, End &end) {
+  using A = typename Acc<V>::type;
+  constexpr int J = kShareSlots / P;
+  const SellView<V> m = sview<V>(mm);
+  const int lane = threadIdx.x & 31;
+  for (int s = lb * kWarps + (int)(threadIdx.x >> 5); s < m.nslices; s += nb * kWarps) {
+    int sp = 0, ip = 0;
+    if (lane <= 1) {
+      sp = __ldg(m.sptr + s + lane);
+      ip = __ldg(m.iptr + s + lane);
+    }
+    const int vb = __shfl_sync(0xffffffffu, sp, 0), ve = __shfl_sync(0xffffffffu, sp, 1);
+    const int ib = __shfl_sync(0xffffffffu, ip, 0), ie = __shfl_sync(0xffffffffu, ip, 1);
+    const int w = (ve - vb) / kSlice;
+    const bool om = (ie - ib) == w;
+    const int row = s * kSlice + lane;
+    if (w <= kShareSlots) {
+      A vv[J][P];
+      int col[J][P];
+      share_load<true, P>(m, w, vb, ib, om, row, 0, vv, col);  // read once: evict-first
+      int q = 0;
+      for (; q + 1 < M; q += 2) {
+        const int i0 = ml[q], i1 = ml[q + 1];
+        A a0 = A(0), a1 = A(0);
+        share_dot<P>(m.n, vv, col, (const X *)mv.p[i0][0], a0);
+        share_dot<P>(m.n, vv, col, (const X *)mv.p[i1][0], a1);
+        if (row < m.n) body(i0, row, a0);
+        end(i0, s);
+        if (row < m.n) body(i1, row, a1);
+        end(i1, s);
+      }
+      if (q < M) {
+        const int i0 = ml[q];
+        A a0 = A(0);
+        share_dot<P>(m.n, vv, col, (const X *)mv.p[i0][0], a0);
+        if (row < m.n) body(i0, row, a0);
+        end(i0, s);
+      }
+    } else {
+      for (int q = 0; q < M; q++) {
+        const int i0 = ml[q];
+        A a0 = A(0);
+        for (int k0 = 0; k0 < w; k0 += kShareSlots) {
+          A vv[J][P];
+          int col[J][P];
+          share_load<false, P>(m, w, vb, ib, om, row, k0, vv, col);  // every member: cached
+          share_dot<P>(m.n, vv, col, (const X *)mv.p[i0][0], a0);
+        }
+        if (row < m.n) body(i0, row, a0);
+        end(i0, s);
+      }
+    }
+  }
+}
+
+// shared_slices for the operator's pack.
+template <class V, class X, class Body, class End>
+__device__ __forceinline__ void shared_slices_any(const Mat &m, int lb, int nb, const int *ml,
+                                                  int M, const MemberVecs &mv, Body &body,
+                                                  End &end) {
   if constexpr (pack_ok<V, 2>()) {
-    if (m.pack == 2) return chunk_rows_p<V, 2>(m, c, x, epi, end);
+    if (m.pack == 2) return shared_slices<V, 2, X>(m, lb, nb, ml, M, mv, body, end);
   }
   if constexpr (pack_ok<V, 4>()) {
-    if (m.pack == 4) return chunk_rows_p<V, 4>(m, c, x, epi, end);
+    if (m.pack == 4) return shared_slices<V, 4, X>(m, lb, nb, ml, M, mv, body, end);
   }
   if constexpr (pack_ok<V, 8>()) {
-    if (m.pack == 8) return chunk_rows_p<V, 8>(m, c, x, epi, end);
+    if (m.pack == 8) return shared_slices<V, 8, X>(m, lb, nb, ml, M, mv, body, end);
   }
-  chunk_rows_p<V, 1>(m, c, x, epi, end);
+  shared_slices<V, 1, X>(m, lb, nb, ml, M, mv, body, end);
+}
+
+// The active members (bits of act) as a list of group indices in shared
+// memory (thread 0 writes; the caller synchronises).
+__device__ __forceinline__ void member_list(unsigned act, int nmem, int *ml) {
+  if (threadIdx.x != 0) return;
+  int M = 0;
+  for (int i = 0; i < nmem; i++)
+    if ((act >> i) & 1u) ml[M++] = i;
 }
 
 struct NoEnd {
-  __device__ __forceinline__ void operator()(int) const {}
+  __device__ __forceinline__ void operator()(int, int) const {}
 };
 
 // Block prologue: the block's slot, or -1.  `need` decides from the slot's
@@ -209,13 +323,6 @@ struct NoEnd {
   const GroupDesc gd = tab->group[grp];                           \
   const int lb = blockIdx.x - gd.b0;
 
-// The members' vector pointers an operator kernel needs (up to 5 each),
-// staged once per block in shared memory; the operator (A, W^T, Z, D^-1)
-// is the same for every member and is read from member 0.
-constexpr int kMemberVecs = 5;
-struct MemberVecs {
-  void *p[kMaxMembers][kMemberVecs];
-};
 template <class F>
 __device__ __forceinline__ void stage_members(const Table *tab, const GroupDesc &gd,
                                               MemberVecs &mv, F &&pick) {
@@ -424,48 +531,50 @@ __device__ __forceinline__ unsigned sweep_members(const SlotState *sts, const Gr
   return act;
 }
 
-// Sweep 1 of the apply: t = D^-1 .* (W^T src), chunk by chunk, every
-// member in turn.
+// Sweep 1 of the apply: t = D^-1 .* (W^T src) for the members in ml.
 template <class V, class T>
 __device__ __forceinline__ void sweep1_group(const Mat &wt, const V *__restrict__ d,
                                              const GroupDesc &gd, const MemberVecs &mv,
-                                             unsigned act, int lb) {
+                                             const int *ml, int M, int lb) {
   NoEnd end;
-  for (int c = lb; c < gd.nchunks; c += gd.nb)
-    for (int i = 0; i < gd.nmem; i++) {
-      if (!((act >> i) & 1u)) continue;
-      const double *src = (const double *)mv.p[i][0];
-      T *__restrict__ t = (T *)mv.p[i][1];
-      auto epi = [&](int row, auto acc) { t[row] = (T)(ldd(d + row) * acc); };
-      chunk_rows<V>(wt, c, src, epi, end);
-    }
+  auto body = [&](int i, int row, auto acc) { ((T *)mv.p[i][1])[row] = (T)(ldd(d + row) * acc); };
+  shared_slices_any<V, double>(wt, lb, gd.nb, ml, M, mv, body, end);
 }
 
+// Slice-shared operator kernels, for groups whose kind does not stream:
+// the members' vectors and the active-member list go to shared memory once
+// per block.
+#define SRV_SHARED_MEMBERS(act, pick)                 \
+  __shared__ MemberVecs mv;                           \
+  __shared__ int ml[kMaxMembers];                     \
+  const int M = __popc(act);                          \
+  member_list(act, gd.nmem, ml);                      \
+  stage_members(tab, gd, mv, pick);
+
 template <bool ACC>
-__global__ void __launch_bounds__(kBlock) k_srv_sweep1(const Table *tab, SlotState *sts,
-                                                       int src) {
+__global__ void __launch_bounds__(kBlock, 3) k_srv_sweep1(const Table *tab, SlotState *sts,
+                                                          int src) {
   SRV_GROUP_PROLOGUE
   const SlotDesc &s0 = tab->slot[gd.mem[0]];
   const Mat wt = s0.wt;
   const void *d = s0.d;
   const unsigned act = sweep_members<ACC>(sts, gd, wt.prec, s0.smask, kSkSweep1, false);
   if (!act) return;
-  __shared__ MemberVecs mv;
-  stage_members(tab, gd, mv, [&](const SlotDesc &sd, void *(&p)[kMemberVecs]) {
-    p[0] = sd.vec[src];
-    p[1] = sd.t;
-  });
+  SRV_SHARED_MEMBERS(act, ([&](const SlotDesc &sd, void *(&p)[kMemberVecs]) {
+                       p[0] = sd.vec[src];
+                       p[1] = sd.t;
+                     }))
   if constexpr (ACC) {
     if (wt.prec == AINV_PREC_FP32_ACC64)
-      sweep1_group<f32w, double>(wt, (const f32w *)d, gd, mv, act, lb);
+      sweep1_group<f32w, double>(wt, (const f32w *)d, gd, mv, ml, M, lb);
     else
-      sweep1_group<b16w, double>(wt, (const b16w *)d, gd, mv, act, lb);
+      sweep1_group<b16w, double>(wt, (const b16w *)d, gd, mv, ml, M, lb);
   } else {
     switch (wt.prec) {
-      case AINV_PREC_FP64: sweep1_group<double, double>(wt, (const double *)d, gd, mv, act, lb); break;
-      case AINV_PREC_FP32: sweep1_group<float, float>(wt, (const float *)d, gd, mv, act, lb); break;
+      case AINV_PREC_FP64: sweep1_group<double, double>(wt, (const double *)d, gd, mv, ml, M, lb); break;
+      case AINV_PREC_FP32: sweep1_group<float, float>(wt, (const float *)d, gd, mv, ml, M, lb); break;
       default:
-        sweep1_group<__nv_bfloat16, float>(wt, (const __nv_bfloat16 *)d, gd, mv, act, lb);
+        sweep1_group<__nv_bfloat16, float>(wt, (const __nv_bfloat16 *)d, gd, mv, ml, M, lb);
         break;
     }
   }
@@ -474,41 +583,36 @@ __global__ void __launch_bounds__(kBlock) k_srv_sweep1(const Table *tab, SlotSta
 // Sweep 2 of the apply: dst = Z t (alpha = 1, beta = 0).
 template <class V, class T>
 __device__ __forceinline__ void sweep2_group(const Mat &z, const GroupDesc &gd,
-                                             const MemberVecs &mv, unsigned act, int lb) {
+                                             const MemberVecs &mv, const int *ml, int M, int lb) {
   NoEnd end;
-  for (int c = lb; c < gd.nchunks; c += gd.nb)
-    for (int i = 0; i < gd.nmem; i++) {
-      if (!((act >> i) & 1u)) continue;
-      const T *t = (const T *)mv.p[i][0];
-      double *__restrict__ y = (double *)mv.p[i][1];
-      auto epi = [&](int row, auto acc) { y[row] = axpby_row(1.0, (double)acc, 0.0, 0.0); };
-      chunk_rows<V>(z, c, t, epi, end);
-    }
+  auto body = [&](int i, int row, auto acc) {
+    ((double *)mv.p[i][1])[row] = axpby_row(1.0, (double)acc, 0.0, 0.0);
+  };
+  shared_slices_any<V, T>(z, lb, gd.nb, ml, M, mv, body, end);
 }
 
 template <bool ACC>
-__global__ void __launch_bounds__(kBlock) k_srv_sweep2(const Table *tab, SlotState *sts,
-                                                       int dst) {
+__global__ void __launch_bounds__(kBlock, 3) k_srv_sweep2(const Table *tab, SlotState *sts,
+                                                          int dst) {
   SRV_GROUP_PROLOGUE
   const SlotDesc &s0 = tab->slot[gd.mem[0]];
   const Mat z = s0.z;
   const unsigned act = sweep_members<ACC>(sts, gd, z.prec, s0.smask, kSkSweep2, false);
   if (!act) return;
-  __shared__ MemberVecs mv;
-  stage_members(tab, gd, mv, [&](const SlotDesc &sd, void *(&p)[kMemberVecs]) {
-    p[0] = sd.t;
-    p[1] = sd.vec[dst];
-  });
+  SRV_SHARED_MEMBERS(act, ([&](const SlotDesc &sd, void *(&p)[kMemberVecs]) {
+                       p[0] = sd.t;
+                       p[1] = sd.vec[dst];
+                     }))
   if constexpr (ACC) {
     if (z.prec == AINV_PREC_FP32_ACC64)
-      sweep2_group<f32w, double>(z, gd, mv, act, lb);
+      sweep2_group<f32w, double>(z, gd, mv, ml, M, lb);
     else
-      sweep2_group<b16w, double>(z, gd, mv, act, lb);
+      sweep2_group<b16w, double>(z, gd, mv, ml, M, lb);
   } else {
     switch (z.prec) {
-      case AINV_PREC_FP64: sweep2_group<double, double>(z, gd, mv, act, lb); break;
-      case AINV_PREC_FP32: sweep2_group<float, float>(z, gd, mv, act, lb); break;
-      default: sweep2_group<__nv_bfloat16, float>(z, gd, mv, act, lb); break;
+      case AINV_PREC_FP64: sweep2_group<double, double>(z, gd, mv, ml, M, lb); break;
+      case AINV_PREC_FP32: sweep2_group<float, float>(z, gd, mv, ml, M, lb); break;
+      default: sweep2_group<__nv_bfloat16, float>(z, gd, mv, ml, M, lb); break;
     }
   }
 }
@@ -554,33 +658,31 @@ __device__ __forceinline__ unsigned spmv_members(const SlotState *sts, const Gro
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(kBlock, 4) k_srv_spmv(const Table *tab, SlotState *sts) {
+__global__ void __launch_bounds__(kBlock, 3) k_srv_spmv(const Table *tab, SlotState *sts) {
   SRV_GROUP_PROLOGUE
   const SlotDesc &s0 = tab->slot[gd.mem[0]];
   const unsigned act = spmv_members<MODE>(sts, gd, s0.smask, false);
   if (!act) return;
   const Mat A = s0.A;
-  __shared__ MemberVecs mv;
   __shared__ double *msp[kMaxMembers];
   __shared__ int mld[kMaxMembers];
-  stage_members(tab, gd, mv, [&](const SlotDesc &sd, void *(&p)[kMemberVecs]) {
-    spmv_vectors<MODE>(sd, p);
-    msp[threadIdx.x] = sd.sp;
-    mld[threadIdx.x] = sd.ld;
-  });
-  for (int c = lb; c < gd.nchunks; c += gd.nb)
-    for (int m = 0; m < gd.nmem; m++) {
-      if (!((act >> m) & 1u)) continue;
-      const double *x = (const double *)mv.p[m][0];
-      double *y = (double *)mv.p[m][1];
-      const double *w1 = (const double *)mv.p[m][2];
-      double *w2 = (double *)mv.p[m][3];
-      const double *w3 = (const double *)mv.p[m][4];
-      SliceSums<dots_of(MODE)> sums{msp[m], mld[m], {}};
-      auto epi = [&](int i, double acc) { dots_row<MODE>(i, acc, x, y, w1, w2, w3, sums); };
-      auto end = [&](int s) { sums.end(s); };
-      chunk_rows<double>(A, c, x, epi, end);
-    }
+  SRV_SHARED_MEMBERS(act, ([&](const SlotDesc &sd, void *(&p)[kMemberVecs]) {
+                       spmv_vectors<MODE>(sd, p);
+                       msp[threadIdx.x] = sd.sp;
+                       mld[threadIdx.x] = sd.ld;
+                     }))
+  SliceSums<dots_of(MODE)> cur{nullptr, 0, {}};
+  auto body = [&](int i, int row, double acc) {
+    dots_row<MODE>(row, acc, (const double *)mv.p[i][0], (double *)mv.p[i][1],
+                   (const double *)mv.p[i][2], (double *)mv.p[i][3], (const double *)mv.p[i][4],
+                   cur);
+  };
+  auto end = [&](int i, int s) {
+    cur.sp = msp[i];
+    cur.ld = mld[i];
+    cur.end(s);
+  };
+  shared_slices_any<double, double>(A, lb, gd.nb, ml, M, mv, body, end);
 }
 
 // ---- streamed operator kernels -----------------------------------------------
@@ -958,12 +1060,13 @@ struct Operator {
 };
 
 // The operator's streamed kinds: those whose matrix the streaming layout
-// takes (stream_plan) and whose kernel variant exists.  AINV_SERVER_STREAM=0
-// runs every kind chunk-walked (for comparison).
+// takes (stream_plan) and whose kernel variant exists; the others run
+// slice-shared.  AINV_SERVER_STREAM=<mask> restricts streaming to the kinds
+// of the mask (bit k: StreamKind k; 0 = none), for comparison.
 void plan_operator(Operator &op) {
-  static const bool off = [] {
+  static const unsigned allow = [] {
     const char *e = std::getenv("AINV_SERVER_STREAM");
-    return e && e[0] == '0';
+    return e ? (unsigned)std::strtoul(e, nullptr, 0) : 0xfu;
   }();
   const ainv_handle *h = op.h;
   const int tsz = (h->prec == AINV_PREC_FP32 || h->prec == AINV_PREC_BF16) ? 4 : 8;
@@ -972,7 +1075,8 @@ void plan_operator(Operator &op) {
     int xs, nrv;
   } k[kNumSk] = {{&h->wt, 8, 1}, {&h->z, tsz, 0}, {&op.a->a, 8, 1}, {&op.a->a, 8, 3}};
   op.smask = 0;
-  for (int q = 0; q < kNumSk && !off; q++) {
+  for (int q = 0; q < kNumSk; q++) {
+    if (!((allow >> q) & 1u)) continue;
     StreamLayout L;
     size_t smem = 0;
     if (stream_plan(*k[q].m, k[q].xs, k[q].nrv, L, smem) <= 0) continue;

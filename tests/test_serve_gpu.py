@@ -262,9 +262,9 @@ print("OK")
 """
 
 
-def test_chunk_walked_operator_kernels_equal_single_solve():
+def test_slice_shared_operator_kernels_equal_single_solve():
     """With streaming switched off (AINV_SERVER_STREAM=0) the server's
-    chunk-walking operator kernels run instead and give the same bits."""
+    slice-shared operator kernels run instead and give the same bits."""
     import os
     import subprocess
     import sys
