@@ -383,8 +383,9 @@ __global__ void __launch_bounds__(kBlock) k_srv_s(const Table *tab, SlotState *s
   for (int i = lb * kBlock + threadIdx.x; i < n; i += nb * kBlock) s[i] = r[i] - alpha * v[i];
 }
 
-// x += alpha f + omega z, r = s - omega t; slice sums of r.r and rt.r.
-__global__ void __launch_bounds__(kBlock) k_srv_xr(const Table *tab, SlotState *sts) {
+// x += alpha f + omega z, r = s - omega t; slice sums of r.r and rt.r.  Capped
+// at 32 registers so that the grid's 8 blocks per SM are resident at once.
+__global__ void __launch_bounds__(kBlock, 8) k_srv_xr(const Table *tab, SlotState *sts) {
   SRV_PROLOGUE(SRV_RUNNING)
   const double *f = sd.vec[VF], *z = sd.vec[VZ], *s = sd.vec[VS], *t = sd.vec[VT],
                *rt = sd.vec[VRT];
