@@ -22,13 +22,13 @@
 //
 // Requests on the same operator share its reads.  Active slots are grouped
 // by operator (up to kMaxMembers per group).  The kernels that read A or
-// the factors (the two sweeps and the three A products) run streamed where
-// the layout allows: the stream.cuh pipeline (a producer warp feeding
-// stages by bulk copies), with each of the group's blocks working for one
-// member and the members' blocks walking the same stages side by side, so
-// a stage's values come from HBM once and from L2 for the other members.
-// Otherwise the group's blocks walk its chunks of 512 rows and compute
-// each chunk for every member in turn.
+// the factors (the two sweeps and the three A products) walk the
+// operator's slices warp by warp, load each slice's values and columns
+// once into registers and compute every member's rows from them, so the
+// operator comes from HBM once per group and a member adds only its own
+// gathers and epilogue.  A streamed form (the stream.cuh pipeline, each
+// block working for one member, the members' blocks walking the same
+// stages side by side) can be selected per kernel kind.
 //
 // The host side is an engine thread: requests queue on submit, are admitted
 // first-come first-served while a slot is free and their vectors fit in the
@@ -74,6 +74,19 @@ static_assert(kBlock == kFoldThreads, "the fold runs on the server's blocks");
 #define AINV_SRV_STREAM_BLOCKS 3
 #endif
 constexpr int kSrvStreamBlocks = AINV_SRV_STREAM_BLOCKS;
+// Slice-shared operator kernels: resident blocks per SM (their register
+// cap and grid) and members computed per step from one slice's registers.
+// They are latency-bound: 5 blocks per SM (48 registers, a few spills)
+// served the 200^3 batch 8% faster than 4 and 18% faster than 3; 6 was
+// within 2%, and 7 or 8 (40, 32 registers) lost 19% to spills.
+#ifndef AINV_SRV_SHARE_BLOCKS
+#define AINV_SRV_SHARE_BLOCKS 5
+#endif
+#ifndef AINV_SRV_SHARE_UNROLL
+#define AINV_SRV_SHARE_UNROLL 2
+#endif
+constexpr int kSrvShareBlocks = AINV_SRV_SHARE_BLOCKS;
+constexpr int kShareUnroll = AINV_SRV_SHARE_UNROLL;
 
 enum Vec { VX = 0, VB, VR, VRT, VP, VV, VF, VS, VZ, VT, VRTRUE, kNumVec };
 enum Phase { kIdle = 0, kInitPhase = 1, kRun = 2 };
@@ -108,7 +121,7 @@ struct SlotDesc {
 
 // Slots on one operator, served together by the operator kernels.
 struct GroupDesc {
-  int b0, nb;    // chunk-walking operator kernels: blocks [b0, b0 + nb)
+  int b0, nb;    // slice-shared operator kernels: blocks [b0, b0 + nb)
   int bs0, nbs;  // streamed operator kernels: blocks [bs0, bs0 + nbs) (nbs >= nmem)
   int nchunks, nmem;
   short mem[kMaxMembers];
@@ -118,7 +131,7 @@ struct Table {
   SlotDesc slot[kMaxSlots];
   GroupDesc group[kMaxSlots];
   short block_slot[kMaxGrid];     // vector kernels and folds: the block's slot, -1 idle
-  short block_group[kMaxGrid];    // chunk-walking operator kernels: the block's group
+  short block_group[kMaxGrid];    // slice-shared operator kernels: the block's group
   short block_group_s[kMaxGrid];  // streamed operator kernels: the block's group
 };
 
@@ -150,8 +163,9 @@ struct MemberVecs {
 // The group's blocks walk the operator's slices warp by warp (lane = row;
 // block lb takes slices 8 lb + warp, then every 8 nb-th).  A slice's
 // values and columns are loaded once into registers and each active
-// member's rows are computed from them, two members at a time, so a member
-// adds only its own gathers and epilogue.  Slots run in order with the
+// member's rows are computed from them, kShareUnroll members at a time (their
+// gathers in flight together), so a member adds only its own gathers and
+// epilogue.  Slots run in order with the
 // products of zero slots adding zero, as group_slots forms them, so every
 // member gets the single-solve row sums.  Slices wider than kShareSlots
 // slots reload their values for each member, kShareSlots at a time.
@@ -232,23 +246,21 @@ __device__ __forceinline__ void shared_slices(const Mat &mm, int lb, int nb, con
       A vv[J][P];
       int col[J][P];
       share_load<true, P>(m, w, vb, ib, om, row, 0, vv, col);  // read once: evict-first
-      int q = 0;
-      for (; q + 1 < M; q += 2) {
-        const int i0 = ml[q], i1 = ml[q + 1];
-        A a0 = A(0), a1 = A(0);
-        share_dot<P>(m.n, vv, col, (const X *)mv.p[i0][0], a0);
-        share_dot<P>(m.n, vv, col, (const X *)mv.p[i1][0], a1);
-        if (row < m.n) body(i0, row, a0);
-        end(i0, s);
-        if (row < m.n) body(i1, row, a1);
-        end(i1, s);
-      }
-      if (q < M) {
-        const int i0 = ml[q];
-        A a0 = A(0);
-        share_dot<P>(m.n, vv, col, (const X *)mv.p[i0][0], a0);
-        if (row < m.n) body(i0, row, a0);
-        end(i0, s);
+      for (int q = 0; q < M; q += kShareUnroll) {
+        A a[kShareUnroll];
+        int iu[kShareUnroll];
+#pragma unroll
+        for (int u = 0; u < kShareUnroll; u++) {
+          iu[u] = q + u < M ? ml[q + u] : -1;
+          a[u] = A(0);
+          if (iu[u] >= 0) share_dot<P>(m.n, vv, col, (const X *)mv.p[iu[u]][0], a[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < kShareUnroll; u++)
+          if (iu[u] >= 0) {
+            if (row < m.n) body(iu[u], row, a[u]);
+            end(iu[u], s);
+          }
       }
     } else {
       for (int q = 0; q < M; q++) {
@@ -314,7 +326,7 @@ struct NoEnd {
 
 #define SRV_RUNNING (ss->phase == kRun && !st->done)
 
-// Prologue of the chunk-walking operator kernels: the block's group (copied
+// Prologue of the slice-shared operator kernels: the block's group (copied
 // out of the table, so that the stores of the inner loops cannot force
 // reloads), or return.
 #define SRV_GROUP_PROLOGUE                                         \
@@ -553,7 +565,7 @@ __device__ __forceinline__ void sweep1_group(const Mat &wt, const V *__restrict_
   stage_members(tab, gd, mv, pick);
 
 template <bool ACC>
-__global__ void __launch_bounds__(kBlock, 3) k_srv_sweep1(const Table *tab, SlotState *sts,
+__global__ void __launch_bounds__(kBlock, kSrvShareBlocks) k_srv_sweep1(const Table *tab, SlotState *sts,
                                                           int src) {
   SRV_GROUP_PROLOGUE
   const SlotDesc &s0 = tab->slot[gd.mem[0]];
@@ -593,7 +605,7 @@ __device__ __forceinline__ void sweep2_group(const Mat &z, const GroupDesc &gd,
 }
 
 template <bool ACC>
-__global__ void __launch_bounds__(kBlock, 3) k_srv_sweep2(const Table *tab, SlotState *sts,
+__global__ void __launch_bounds__(kBlock, kSrvShareBlocks) k_srv_sweep2(const Table *tab, SlotState *sts,
                                                           int dst) {
   SRV_GROUP_PROLOGUE
   const SlotDesc &s0 = tab->slot[gd.mem[0]];
@@ -659,7 +671,7 @@ __device__ __forceinline__ unsigned spmv_members(const SlotState *sts, const Gro
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(kBlock, 3) k_srv_spmv(const Table *tab, SlotState *sts) {
+__global__ void __launch_bounds__(kBlock, kSrvShareBlocks) k_srv_spmv(const Table *tab, SlotState *sts) {
   SRV_GROUP_PROLOGUE
   const SlotDesc &s0 = tab->slot[gd.mem[0]];
   const unsigned act = spmv_members<MODE>(sts, gd, s0.smask, false);
@@ -907,8 +919,10 @@ void *spmv_kernel(int pack) {
   return nullptr;
 }
 
-// Grid of the streamed operator kernels: kSrvStreamBlocks blocks per SM.
+// Grids of the streamed and slice-shared operator kernels: one resident
+// wave each.
 int stream_grid() { return std::min(kMaxGrid, kSrvStreamBlocks * sm_count()); }
+int share_grid() { return std::min(kMaxGrid, kSrvShareBlocks * sm_count()); }
 
 cudaError_t launch_raw(void *k, int grid, int threads, size_t smem, cudaStream_t s, void **args) {
   return cudaLaunchKernel(k, dim3(grid), dim3(threads), args, smem, s);
@@ -922,15 +936,16 @@ void sweeps(const Table *tab, SlotState *sts, int grid, cudaStream_t s, const La
     launch_raw(sweep_kernel<1>(v.first, v.second), gs, kStreamThreads, lp.smem[kSkSweep1], s, args);
     ++*count;
   }
-  if (lp.fb_sweep1 & kFamStd) k_srv_sweep1<false><<<grid, kBlock, 0, s>>>(tab, sts, src), ++*count;
-  if (lp.fb_sweep1 & kFamAcc64) k_srv_sweep1<true><<<grid, kBlock, 0, s>>>(tab, sts, src), ++*count;
+  const int gh = share_grid();
+  if (lp.fb_sweep1 & kFamStd) k_srv_sweep1<false><<<gh, kBlock, 0, s>>>(tab, sts, src), ++*count;
+  if (lp.fb_sweep1 & kFamAcc64) k_srv_sweep1<true><<<gh, kBlock, 0, s>>>(tab, sts, src), ++*count;
   for (const auto &v : lp.sw2) {
     void *args[] = {(void *)&tab, (void *)&sts, (void *)&dst};
     launch_raw(sweep_kernel<2>(v.first, v.second), gs, kStreamThreads, lp.smem[kSkSweep2], s, args);
     ++*count;
   }
-  if (lp.fb_sweep2 & kFamStd) k_srv_sweep2<false><<<grid, kBlock, 0, s>>>(tab, sts, dst), ++*count;
-  if (lp.fb_sweep2 & kFamAcc64) k_srv_sweep2<true><<<grid, kBlock, 0, s>>>(tab, sts, dst), ++*count;
+  if (lp.fb_sweep2 & kFamStd) k_srv_sweep2<false><<<gh, kBlock, 0, s>>>(tab, sts, dst), ++*count;
+  if (lp.fb_sweep2 & kFamAcc64) k_srv_sweep2<true><<<gh, kBlock, 0, s>>>(tab, sts, dst), ++*count;
 }
 
 template <int MODE>
@@ -944,7 +959,7 @@ void spmv(const Table *tab, SlotState *sts, int grid, cudaStream_t s, const Laun
     ++*count;
   }
   if (MODE == kTrueRes ? lp.fb_true : lp.fb_spmv) {
-    k_srv_spmv<MODE><<<grid, kBlock, 0, s>>>(tab, sts);
+    k_srv_spmv<MODE><<<share_grid(), kBlock, 0, s>>>(tab, sts);
     ++*count;
   }
   k_srv_fold<dots_of(MODE), FinDotsSrv<MODE>><<<grid, kBlock, 0, s>>>(tab, sts, FinDotsSrv<MODE>{});
@@ -1060,14 +1075,16 @@ struct Operator {
   unsigned smask = 0;
 };
 
-// The operator's streamed kinds: those whose matrix the streaming layout
-// takes (stream_plan) and whose kernel variant exists; the others run
-// slice-shared.  AINV_SERVER_STREAM=<mask> restricts streaming to the kinds
-// of the mask (bit k: StreamKind k; 0 = none), for comparison.
+// The operator's streamed kinds.  By default every kind runs slice-shared:
+// at 5 blocks per SM it served the 200^3 batch 1.26x faster than the
+// streamed kernels (whose shared memory holds them to 3 blocks per SM).
+// AINV_SERVER_STREAM=<mask> streams the kinds of the mask (bit k:
+// StreamKind k) whose matrix the streaming layout takes and whose kernel
+// variant exists.
 void plan_operator(Operator &op) {
   static const unsigned allow = [] {
     const char *e = std::getenv("AINV_SERVER_STREAM");
-    return e ? (unsigned)std::strtoul(e, nullptr, 0) : 0xfu;
+    return e ? (unsigned)std::strtoul(e, nullptr, 0) : 0u;
   }();
   const ainv_handle *h = op.h;
   const int tsz = (h->prec == AINV_PREC_FP32 || h->prec == AINV_PREC_BF16) ? 4 : 8;
@@ -1440,7 +1457,7 @@ void engine_loop(ainv_server *srv) {
         gw[(size_t)g] = (long long)srv->tab_h->group[g].nchunks * srv->tab_h->group[g].nmem;
         gcap[(size_t)g] = srv->tab_h->group[g].nchunks;
       }
-      if (plan_weighted(ng, gw.data(), gcap.data(), srv->grid, gb0.data(), gnb.data()) !=
+      if (plan_weighted(ng, gw.data(), gcap.data(), share_grid(), gb0.data(), gnb.data()) !=
           AINV_SUCCESS) {
         fail_all(srv, AINV_ERR_INTERNAL, "server group plan failed");
         return;

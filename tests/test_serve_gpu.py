@@ -208,7 +208,7 @@ def test_requests_on_one_operator_share_reads():
 @pytest.mark.parametrize("prec", ["FP64", "FP32_ACC64", "FP32", "BF16"])
 def test_served_equals_single_solve(prec):
     """Six concurrent requests on two operators (groups of members that share
-    the operator's streamed reads): each solution and iteration count equals
+    the operator's reads): each solution and iteration count equals
     ainv_gpu_solve's on the same right-hand side, bit for bit."""
     ops = _operators(prec)[1:3]
     reqs = _requests(ops, 6)
@@ -262,16 +262,17 @@ print("OK")
 """
 
 
-def test_slice_shared_operator_kernels_equal_single_solve():
-    """With streaming switched off (AINV_SERVER_STREAM=0) the server's
-    slice-shared operator kernels run instead and give the same bits."""
+def test_streamed_operator_kernels_equal_single_solve():
+    """With streaming selected for every kind (AINV_SERVER_STREAM=15) the
+    server's streamed operator kernels run instead of the slice-shared ones
+    and give the same bits."""
     import os
     import subprocess
     import sys
     here = os.path.dirname(os.path.abspath(__file__))
     root = os.path.dirname(here)
     paths = [here, root, os.path.join(root, "oracle"), os.path.join(root, "mld-ainv_b200")]
-    env = dict(os.environ, AINV_SERVER_STREAM="0")
+    env = dict(os.environ, AINV_SERVER_STREAM="15")
     out = subprocess.run([sys.executable, "-c", _CHUNK_SCRIPT.format(paths=paths)],
                          env=env, capture_output=True, text=True, timeout=600)
     assert out.returncode == 0 and "OK" in out.stdout, out.stderr[-3000:]
