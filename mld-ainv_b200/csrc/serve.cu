@@ -104,7 +104,8 @@ struct Mat {
 };
 
 struct SlotDesc {
-  int b0, nb;  // launch blocks [b0, b0 + nb) of the vector kernels and the fold
+  int b0, nb;    // launch blocks [b0, b0 + nb) of the vector kernels
+  int fb0, fnb;  // fold blocks [fb0, fb0 + fnb), at most one per range
   int n, nchunks;
   Mat A, wt, z;
   const void *d;  // D^-1 in the factors' precision
@@ -130,7 +131,8 @@ struct GroupDesc {
 struct Table {
   SlotDesc slot[kMaxSlots];
   GroupDesc group[kMaxSlots];
-  short block_slot[kMaxGrid];     // vector kernels and folds: the block's slot, -1 idle
+  short block_slot[kMaxGrid];     // vector kernels: the block's slot, -1 idle
+  short block_slot_f[kMaxGrid];   // folds: the block's slot, -1 idle
   short block_group[kMaxGrid];    // slice-shared operator kernels: the block's group
   short block_group_s[kMaxGrid];  // streamed operator kernels: the block's group
 };
@@ -375,15 +377,25 @@ __global__ void __launch_bounds__(kBlock) k_srv_init(const Table *tab, SlotState
   }
 }
 
-// p = r (first iteration) or p = r + beta (p - omega v).
+// p = r (first iteration) or p = r + beta (p - omega v).  When the last
+// true-residual check asked for it, r := b - A x first (the single solve's
+// replacement before its next p update; nothing reads r in between).
 __global__ void __launch_bounds__(kBlock) k_srv_p(const Table *tab, SlotState *sts) {
   SRV_PROLOGUE(SRV_RUNNING)
-  const double *r = sd.vec[VR], *v = sd.vec[VV];
-  double *p = sd.vec[VP];
-  const bool first = st->iter == 0;
+  const double *rtrue = sd.vec[VRTRUE], *v = sd.vec[VV];
+  double *r = sd.vec[VR], *p = sd.vec[VP];
+  const bool first = st->iter == 0, repl = st->replace != 0;
   const double beta = st->beta, omega = st->omega;
-  for (int i = lb * kBlock + threadIdx.x; i < n; i += nb * kBlock)
-    p[i] = first ? r[i] : r[i] + beta * (p[i] - omega * v[i]);
+  for (int i = lb * kBlock + threadIdx.x; i < n; i += nb * kBlock) {
+    double ri;
+    if (repl) {
+      ri = rtrue[i];
+      r[i] = ri;
+    } else {
+      ri = r[i];
+    }
+    p[i] = first ? ri : ri + beta * (p[i] - omega * v[i]);
+  }
 }
 
 // s = r - alpha v.
@@ -418,29 +430,21 @@ __global__ void __launch_bounds__(kBlock, 8) k_srv_xr(const Table *tab, SlotStat
   }
 }
 
-// r := b - A x when the last true-residual check asked for it.
-__global__ void __launch_bounds__(kBlock) k_srv_replace(const Table *tab, SlotState *sts) {
-  SRV_PROLOGUE(ss->phase == kRun && st->replace)
-  const double *rtrue = sd.vec[VRTRUE];
-  double *r = sd.vec[VR];
-  for (int i = lb * kBlock + threadIdx.x; i < n; i += nb * kBlock) r[i] = rtrue[i];
-}
-
 // ---- the fold ------------------------------------------------------------------
-// The slot's blocks fold its slice sums in the canonical order (the single-
-// solve fold's steps): block lb takes ranges lb, lb + np, ... (np = the
-// slot's blocks, at most one per range); the last block to finish (atomic
+// The slot's fold blocks (their own small grid) fold its slice sums in the
+// canonical order (the single-solve fold's steps): block lb takes ranges
+// lb, lb + np, ... (np = the slot's fold blocks); the last block to finish (atomic
 // ticket, no waiting) folds the range sums and runs fin.  fin.need(ss) is
 // the producing kernel's test, so a reduction that did not run is not
 // folded.
 template <int NV, class Fin>
 __global__ void __launch_bounds__(kBlock) k_srv_fold(const Table *tab, SlotState *sts, Fin fin) {
-  const int slot = tab->block_slot[blockIdx.x];
+  const int slot = tab->block_slot_f[blockIdx.x];
   if (slot < 0) return;
   SlotState *ss = sts + slot;
   if (!fin.need(ss)) return;
   const SlotDesc &sd = tab->slot[slot];
-  const int lb = blockIdx.x - sd.b0, np = min(sd.nb, sd.nr);
+  const int lb = blockIdx.x - sd.fb0, np = min(sd.fnb, sd.nr);
   if (lb >= np) return;
   __shared__ bool is_last;
   double v[NV];
@@ -919,10 +923,12 @@ void *spmv_kernel(int pack) {
   return nullptr;
 }
 
-// Grids of the streamed and slice-shared operator kernels: one resident
-// wave each.
+// Grids of the streamed and slice-shared operator kernels (one resident
+// wave each) and of the folds (2 blocks per SM: a fold has one block per
+// 256-group range, 123 for a 200^3 slot).
 int stream_grid() { return std::min(kMaxGrid, kSrvStreamBlocks * sm_count()); }
 int share_grid() { return std::min(kMaxGrid, kSrvShareBlocks * sm_count()); }
+int fold_grid() { return std::min(kMaxGrid, std::max(kMaxSlots, 2 * sm_count())); }
 
 cudaError_t launch_raw(void *k, int grid, int threads, size_t smem, cudaStream_t s, void **args) {
   return cudaLaunchKernel(k, dim3(grid), dim3(threads), args, smem, s);
@@ -962,14 +968,14 @@ void spmv(const Table *tab, SlotState *sts, int grid, cudaStream_t s, const Laun
     k_srv_spmv<MODE><<<share_grid(), kBlock, 0, s>>>(tab, sts);
     ++*count;
   }
-  k_srv_fold<dots_of(MODE), FinDotsSrv<MODE>><<<grid, kBlock, 0, s>>>(tab, sts, FinDotsSrv<MODE>{});
+  k_srv_fold<dots_of(MODE), FinDotsSrv<MODE>><<<fold_grid(), kBlock, 0, s>>>(tab, sts, FinDotsSrv<MODE>{});
   ++*count;
 }
 
 // Start of a graph launch: new slots' vectors and first scalars.
 void enqueue_init(const Table *tab, SlotState *sts, int grid, cudaStream_t s, int *count) {
   k_srv_init<<<grid, kBlock, 0, s>>>(tab, sts);
-  k_srv_fold<1, FinInit><<<grid, kBlock, 0, s>>>(tab, sts, FinInit{});
+  k_srv_fold<1, FinInit><<<fold_grid(), kBlock, 0, s>>>(tab, sts, FinInit{});
   *count += 2;
 }
 
@@ -983,10 +989,9 @@ cudaError_t enqueue_iteration(const Table *tab, SlotState *sts, int grid, cudaSt
   sweeps(tab, sts, grid, s, lp, VS, VZ, count);
   spmv<kBicgOmega>(tab, sts, grid, s, lp, count);
   k_srv_xr<<<grid, kBlock, 0, s>>>(tab, sts);
-  k_srv_fold<2, FinXr><<<grid, kBlock, 0, s>>>(tab, sts, FinXr{});
+  k_srv_fold<2, FinXr><<<fold_grid(), kBlock, 0, s>>>(tab, sts, FinXr{});
   spmv<kTrueRes>(tab, sts, grid, s, lp, count);
-  k_srv_replace<<<grid, kBlock, 0, s>>>(tab, sts);
-  *count += 5;
+  *count += 4;
   return cudaGetLastError();
 }
 
@@ -1433,6 +1438,26 @@ void engine_loop(ainv_server *srv) {
         d.nb = nb[q];
         for (int b = d.b0; b < d.b0 + d.nb; b++) srv->tab_h->block_slot[b] = (short)order[q];
       }
+      // fold blocks: shares of the fold grid in proportion to the ranges
+      {
+        std::vector<long long> fw(order.size());
+        std::vector<int> fcap(order.size()), fb0(order.size()), fnb(order.size());
+        for (size_t q = 0; q < order.size(); q++) {
+          fw[q] = fcap[q] = srv->tab_h->slot[order[q]].nr;
+        }
+        if (plan_weighted((int)order.size(), fw.data(), fcap.data(), fold_grid(), fb0.data(),
+                          fnb.data()) != AINV_SUCCESS) {
+          fail_all(srv, AINV_ERR_INTERNAL, "server fold plan failed");
+          return;
+        }
+        std::fill(srv->tab_h->block_slot_f, srv->tab_h->block_slot_f + kMaxGrid, (short)-1);
+        for (size_t q = 0; q < order.size(); q++) {
+          SlotDesc &d = srv->tab_h->slot[order[q]];
+          d.fb0 = fb0[q];
+          d.fnb = fnb[q];
+          for (int b = d.fb0; b < d.fb0 + d.fnb; b++) srv->tab_h->block_slot_f[b] = (short)order[q];
+        }
+      }
       // operator groups: active slots on one operator, in slot order, up to
       // kMaxMembers each; blocks in proportion to chunks x members
       int ng = 0;
@@ -1615,6 +1640,7 @@ int ainv_server_create(ainv_server **out, int max_slots, size_t hbm_bytes, int i
     return fail(e, "stream");
   std::memset(srv->tab_h, 0, sizeof(Table));
   std::fill(srv->tab_h->block_slot, srv->tab_h->block_slot + kMaxGrid, (short)-1);
+  std::fill(srv->tab_h->block_slot_f, srv->tab_h->block_slot_f + kMaxGrid, (short)-1);
   std::fill(srv->tab_h->block_group, srv->tab_h->block_group + kMaxGrid, (short)-1);
   std::fill(srv->tab_h->block_group_s, srv->tab_h->block_group_s + kMaxGrid, (short)-1);
   std::memset(srv->st_h, 0, sizeof(SlotState) * (size_t)max_slots);
