@@ -83,6 +83,16 @@ __device__ __forceinline__ void st4(double *p, const double (&v)[4]) {
 __device__ __forceinline__ void st4(float *p, const float (&v)[4]) {
   *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
 }
+// Evict-first stores for the products' multivector outputs (Q, T, Z): they
+// are larger than L2 and read back only by a later kernel, so they should
+// not displace the gathered input's rows that the next slices reuse.
+__device__ __forceinline__ void st4cs(double *p, const double (&v)[4]) {
+  __stcs(reinterpret_cast<double2 *>(p), make_double2(v[0], v[1]));
+  __stcs(reinterpret_cast<double2 *>(p) + 1, make_double2(v[2], v[3]));
+}
+__device__ __forceinline__ void st4cs(float *p, const float (&v)[4]) {
+  __stcs(reinterpret_cast<float4 *>(p), make_float4(v[0], v[1], v[2], v[3]));
+}
 
 // acc[e] = row `row` (slice-local rs) of M times column c0 + e of x.  Slots
 // are taken kSlotBatch at a time: their values and index words load
@@ -298,7 +308,7 @@ __global__ void __launch_bounds__(kBlock)
     T t[kColsPerLane];
 #pragma unroll
     for (int e = 0; e < kColsPerLane; e++) t[e] = (T)(dr * acc[e]);
-    st4(Tm + (size_t)row * kCols + c0, t);
+    st4cs(Tm + (size_t)row * kCols + c0, t);
   });
 }
 
@@ -320,7 +330,7 @@ __global__ void __launch_bounds__(kBlock)
       z[e] = (double)acc[e];
       pr[0][e] += r[e] * z[e];
     }
-    st4(Zv + e0, z);
+    st4cs(Zv + e0, z);
   });
   double tot[1];
   if (col_sum4<1>(pr, tot, partials, &ms->ticket) && threadIdx.x < 32) {
@@ -375,7 +385,7 @@ __global__ void __launch_bounds__(kBlock)
     ldg4(P + e0, p);
 #pragma unroll
     for (int e = 0; e < kColsPerLane; e++) pr[0][e] += p[e] * acc[e];
-    st4(Q + e0, acc);
+    st4cs(Q + e0, acc);
   });
   double tot[1];
   if (col_sum4<1>(pr, tot, partials, &ms->ticket) && threadIdx.x < 32) {
