@@ -36,6 +36,14 @@ using namespace kstate;
 constexpr int kCols = 32;    // multivector stride (columns per row)
 constexpr int kChunk = 8;    // iterations per captured graph launch
 constexpr int kRecheck = 50; // true-residual period for FP32/BF16 factors
+// Resident blocks per SM asked of the gathering kernels (SpMM and sweeps):
+// 4 (64 registers) measured 0.489 s per 128^3 x 32 block solve, 5 (48
+// registers, a few spills) 0.500 s, 6 (40) and an uncapped build (72-96
+// registers) 0.54 s.
+#ifndef AINV_MRHS_BLOCKS
+#define AINV_MRHS_BLOCKS 4
+#endif
+constexpr int kGatherBlocks = AINV_MRHS_BLOCKS;
 
 struct MState {
   KState col[kCols];
@@ -298,7 +306,7 @@ __global__ void __launch_bounds__(kBlock)
 
 // Sweep 1 of the apply on all columns: T = D^-1 .* (W^T R).
 template <class V, class T>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, kGatherBlocks)
     k_mv_sweep1(SellView<V> m, int pack, const double *__restrict__ R, const V *__restrict__ d,
                 T *__restrict__ Tm, const MState *ms) {
   if (ms->alldone) return;
@@ -314,7 +322,7 @@ __global__ void __launch_bounds__(kBlock)
 
 // Sweep 2 on all columns: Zv = Z T, with rho_l = r_l . z_l and beta_l.
 template <class V, class T>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, kGatherBlocks)
     k_mv_sweep2(SellView<V> m, int pack, const T *__restrict__ Tm, const double *__restrict__ R,
                 double *__restrict__ Zv, MState *ms, double *partials) {
   if (ms->alldone) return;
@@ -373,7 +381,7 @@ __global__ void __launch_bounds__(kBlock)
 }
 
 // Q = A P with sigma_l = p_l . q_l, alpha_l = rho_l / sigma_l.
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, kGatherBlocks)
     k_mv_spmm_sigma(SellView<double> a, int apack, const double *__restrict__ P,
                     double *__restrict__ Q, MState *ms, double *partials) {
   if (ms->alldone) return;
