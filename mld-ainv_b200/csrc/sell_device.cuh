@@ -613,37 +613,5 @@ __device__ __forceinline__ void fold_total(const double *rs, int ldr, int nr, do
   block_sum<NV>(v);
 }
 
-// Grid-wide deterministic sum: every block stores its partials, the last
-// block to arrive (atomic ticket, no waiting) folds all partials in block
-// order.  Returns true in the last block, where thread 0 holds the totals in
-// v.  The ticket is reset by the last block so the slot can be reused by the
-// next launch.
-template <int NV>
-__device__ __forceinline__ bool grid_sum(double (&v)[NV], double *__restrict__ partials,
-                                         unsigned *__restrict__ ticket) {
-  __shared__ bool is_last;
-  block_sum<NV>(v);
-  const int G = gridDim.x;
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int i = 0; i < NV; i++) partials[i * G + blockIdx.x] = v[i];
-    __threadfence();
-    const unsigned t = atomicAdd(ticket, 1u);
-    is_last = (t == (unsigned)G - 1);
-  }
-  __syncthreads();
-  if (!is_last) return false;
-  __threadfence();
-#pragma unroll
-  for (int i = 0; i < NV; i++) {
-    double s = 0.0;
-    for (int b = threadIdx.x; b < G; b += blockDim.x) s += __ldcg(partials + i * G + b);
-    v[i] = s;
-  }
-  block_sum<NV>(v);
-  if (threadIdx.x == 0) *ticket = 0u;
-  return true;
-}
-
 }  // namespace dev
 }  // namespace ainv
