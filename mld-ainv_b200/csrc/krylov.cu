@@ -11,7 +11,8 @@
 // and the host inspects the state once per chunk.
 //
 // Reproducible iterates.  Every dot is summed in the canonical order of
-// sell_device.cuh (slice trees, then 1024-slice ranges, then the ranges),
+// sell_device.cuh (slice trees, groups of 8 slices, ranges of 256 groups,
+// then the ranges),
 // which does not depend on the grid, the kernel that computes the products
 // or the device: the producing kernel stores one sum per 32-row slice and a
 // small fold kernel (k_fold) reduces them.  The library is compiled without
