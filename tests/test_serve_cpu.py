@@ -35,8 +35,18 @@ def test_plan_rejects_more_slots_than_blocks():
 
 
 def test_request_bytes():
-    for n in (1, 1000, 13824, 2097152):
+    """A request's device bytes: 11 FP64 vectors and the apply intermediate
+    (rows rounded up to 32), then the slice sums of 3 dots (one per 32-row
+    slice, rounded up to 32) and their range sums (one per 256 groups of 8
+    slices, rounded up to 32), the whole rounded up to 256 bytes."""
+    def up(x, m):
+        return -(-x // m) * m
+    for n in (1, 31, 33, 1000, 13824, 2097152, 8000000):
+        ns = -(-n // 32)
+        nr = -(-(-(-ns // 8)) // 256)
+        want = up((12 * up(n, 32) + 3 * (up(ns, 32) + up(nr, 32))) * 8, 256)
         b = serve.request_bytes(n)
+        assert b == want, (n, b, want)
         assert b % 256 == 0 and b >= 12 * 8 * n
     assert serve.request_bytes(2097152) > serve.request_bytes(13824)
 
