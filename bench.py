@@ -575,7 +575,13 @@ def run_extras(ainv, torch, dev, irp, ja, val, f, sv, flush, stream, fp64_ms):
                       "true_relres_seed0": out["solve"][p]["true_relres"],
                       "max_err_vs_xstar_seed0": out["solve"][p]["max_err_vs_xstar"]}
                   for p in seeds},
-        "served": served}
+        "served": served,
+        # reduced-precision modes whose served solve meets the target: every
+        # request converged, every final FP64 residual <= 1e-9, >= 1.5x
+        "target_met_by": sorted(
+            m for m, r in served["served"].items()
+            if m != "FP64" and r["vs_plain_fp64"] is not None and r["vs_plain_fp64"] >= 1.5
+            and r["converged"] == served["requests"] and r["max_final_fp64_relres"] <= 1e-9)}
     return out
 
 
